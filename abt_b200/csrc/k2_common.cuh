@@ -1,0 +1,35 @@
+// k2_common.cuh -- record layout and device helpers of the batched FP32 path.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pbt {
+
+// One triangular aperture prepared for the FP32 far-field sum.  A polygon
+// facet becomes nv-2 records (a fan from its first vertex) that share the
+// facet's centre of mass and aperture frame, so their sum is the polygon's
+// contour integral.  176 bytes, a multiple of 16 for 1-D bulk copies.
+struct __align__(16) K2Rec {
+    double kc[3];    // k * com (lab frame), FP64: the far-field phase k r.c
+    float eps[3];    // com / R
+    float b;         // |com|^2 / R^2
+    float R[9];      // lab -> aperture frame rotation, row-major
+    float ea[3];     // R * com / R
+    float kp[2];     // k * prop2 (x, y)
+    float hkz_cf;    // -0.5 Kz / sqrt(1 - Ky^2)
+    float hicf;      // 0.5 sqrt(1 - Ky^2)
+    float hkxky_cf;  // 0.5 Kx Ky / sqrt(1 - Ky^2)
+    float inc[3];    // incidence direction (0,0,-1) in the aperture frame
+    float vx[3];     // triangle vertices (aperture frame, relative to com)
+    float vy[3];
+    float amp[8];    // (2 i A / lambda) * sign * ampl, (1,1),(2,1),(1,2),(2,2) re/im
+};
+static_assert(sizeof(K2Rec) == 176, "K2Rec must be 176 bytes");
+
+// Per-record field-of-view test data (is_fast_diff only): prop0 and cos(fov).
+struct __align__(16) K2Fov {
+    float p0[3];
+    float cos_fov;
+};
+
+}  // namespace pbt

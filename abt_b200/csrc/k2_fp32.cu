@@ -1,0 +1,1033 @@
+// k2_fp32.cu -- batched far-field sum in FP32 with the phase formed in FP64.
+//
+// Pipeline for a batch of orientations (all on the GPU, no host round trip):
+//   1. k2_count / CUB scan / k2_setup: one thread per outgoing facet forms the
+//      facet's aperture frame in FP64 (frame.h, the reference's set-up of
+//      src/diff_mod.f90:515-574) and writes nv-2 K2Rec triangle records.
+//   2. k2_plan: per (orientation, beam|external) segment, the number of
+//      work items = facet splits x bin tiles.
+//   3. k2_main: a persistent kernel; each CTA claims work items with an
+//      atomic counter, streams the item's facet records through shared memory
+//      with 1-D bulk copies (cp.async.bulk + mbarrier, bounded waits), and
+//      accumulates for each of its bins the 2x2 complex amplitude in FP32
+//      (chunk sums carried in FP64), then adds it to the orientation's
+//      amplitude workspace.
+//   4. k2_epi: FP64 epilogue per bin over the orientations of the batch:
+//      T(phi) rotation, Mueller matrix (ampl_to_mueller, src/outputs_mod.f90:
+//      473-549), running orientation sum, and per-orientation weighted sums
+//      that equal the reference's simpne phi/theta integrals of M11.
+//   5. k2_final / k2_average: per-orientation parameters (finalise,
+//      src/outputs_mod.f90:133-245) and the orientation average
+//      (summation + divide_by_num_orientations).
+//
+// Per facet x bin arithmetic.  The reference evaluates, per edge, a contour
+// term with a 1/(kxx kyy) coordinate singularity (src/diff_mod.f90:408-420).
+// Summed over a triangle's edges it equals (-i/lambda) e^{iK} times the
+// aperture integral, which for a triangle is -2A g[d1,d2,d3]: the second
+// divided difference of e^{ix} at the three vertex phases.  That form has no
+// coordinate singularity; it is evaluated from edge-midpoint phases and
+// sinc((d_b - d_a)/2) (stable for every pair gap), with a Taylor series when
+// all three phases lie within 0.25 rad.  The far-field phase
+// k(|X - c| - |X|) = -k u.c + k(|c|^2 - (u.c)^2)(1 + u.c/R)/(2R) is formed
+// with k u.c in FP64 and reduced mod 2 pi before the FP32 work; the common
+// e^{ik|X|} is applied per bin only when amplitudes are returned.
+#include <cub/device/device_scan.cuh>
+
+#include "frame.h"
+#include "k2_common.cuh"
+#include "pbt_internal.h"
+
+namespace pbt {
+
+namespace {
+
+constexpr int K2_THREADS = 128;
+constexpr int K2_CH = 32;   // records per shared-memory stage
+constexpr int K2_NST = 3;   // stages
+constexpr double kTwoPi = 6.283185307179586;
+constexpr double kInv2Pi = 0.15915494309189535;
+constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52, round-to-integer constant
+
+struct BinDev {
+    double ux, uy, uz;  // unit bin direction, FP64
+    float fx, fy, fz;   // same, FP32
+    float hx, hy, hz;   // direction of the (phi_i, theta_i) bin used by the forward bodge
+};
+
+// ---------------------------------------------------------------- set-up
+
+struct RefSrc {
+    const pbt_outbeam *beam;
+    const pbt_outbeam *ext;
+    const int64_t *beam_off;  // device copies, norient+1
+    const int64_t *ext_off;
+    const int64_t *refbase;   // beam_off[o] + ext_off[o]
+    int64_t norient;
+};
+
+__device__ __forceinline__ int64_t find_orient(const int64_t *base, int64_t n, int64_t g) {
+    int64_t lo = 0, hi = n;  // largest o in [0, n) with base[o] <= g
+    while (hi - lo > 1) {
+        int64_t mid = (lo + hi) >> 1;
+        if (base[mid] <= g)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ const pbt_outbeam *ref_lookup(const RefSrc &S, int64_t g, int64_t &o,
+                                                         int &kind) {
+    o = find_orient(S.refbase, S.norient, g);
+    const int64_t local = g - S.refbase[o];
+    const int64_t nb = S.beam_off[o + 1] - S.beam_off[o];
+    if (local < nb) {
+        kind = 0;
+        return S.beam + S.beam_off[o] + local;
+    }
+    kind = 1;
+    return S.ext + S.ext_off[o] + (local - nb);
+}
+
+__global__ void k2_count_kernel(RefSrc S, int64_t nrefs, const int64_t *__restrict__ face_off,
+                                int64_t nfaces, int64_t *__restrict__ cnt, int *__restrict__ err) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g > nrefs) return;
+    if (g == nrefs) {
+        cnt[g] = 0;
+        return;
+    }
+    int64_t o;
+    int kind;
+    const pbt_outbeam *ob = ref_lookup(S, g, o, kind);
+    const int64_t fi = ob->fi;
+    if (fi < 1 || fi > nfaces) {
+        atomicOr(err, 1);
+        cnt[g] = 0;
+        return;
+    }
+    cnt[g] = face_off[fi] - face_off[fi - 1] - 2;
+}
+
+__global__ void k2_setup_kernel(RefSrc S, int64_t nrefs, const double *__restrict__ verts,
+                                int64_t nverts, const int64_t *__restrict__ face_off,
+                                const int64_t *__restrict__ face_vi, const int64_t *__restrict__ start,
+                                double waveno, double lambda, int fast_diff,
+                                K2Rec *__restrict__ recs, K2Fov *__restrict__ fovs,
+                                int *__restrict__ err) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nrefs) return;
+    int64_t o;
+    int kind;
+    const pbt_outbeam *ob = ref_lookup(S, g, o, kind);
+    const int64_t fi = ob->fi;
+    if (fi < 1) return;  // reported by the count kernel
+    const int64_t fb = face_off[fi - 1];
+    const int nv = (int)(face_off[fi] - fb);
+    const double *V = verts + o * 3 * nverts;
+    constexpr int NVS = 16;  // vertices held in registers; larger faces re-read
+    double vx[NVS], vy[NVS], vz[NVS];
+    double prop0[3] = {ob->prop_out[0], ob->prop_out[1], ob->prop_out[2]};
+    double perp0[3] = {ob->vk7[0], ob->vk7[1], ob->vk7[2]};
+    if (nv > NVS) {
+        atomicOr(err, 2);  // faces above 16 vertices are not supported in FP32
+        return;
+    }
+    for (int i = 0; i < nv; i++) {
+        const int64_t vi = face_vi[fb + i] - 1;
+        vx[i] = V[vi];
+        vy[i] = V[vi + nverts];
+        vz[i] = V[vi + 2 * nverts];
+    }
+    FacetFrame fr;
+    facet_frame(vx, vy, vz, nv, prop0, perp0, fr, nullptr, nullptr, nullptr);
+    const double sign = fr.sign;
+    const double *com = fr.com;
+    const double R = kFarR;
+    const double Ky = fr.prop2[1];
+    const double cf = 1.0 / sqrt(1.0 - Ky * Ky);
+    double ea[3];
+    mv33(fr.R, com, ea);
+    const int64_t r0 = start[g];
+    for (int t = 0; t < nv - 2; t++) {
+        const int iv[3] = {0, t + 1, t + 2};
+        double xa[3], ya[3];
+        for (int q = 0; q < 3; q++) {
+            const double d[3] = {vx[iv[q]] - com[0], vy[iv[q]] - com[1], vz[iv[q]] - com[2]};
+            double rr[3];
+            mv33(fr.R, d, rr);
+            xa[q] = rr[0];
+            ya[q] = rr[1];
+        }
+        const double As = 0.5 * ((xa[1] - xa[0]) * (ya[2] - ya[0]) - (xa[2] - xa[0]) * (ya[1] - ya[0]));
+        const double cpre = 2.0 * As / lambda * sign;  // amp' = i * cpre * ampl
+        K2Rec rec;
+        for (int c = 0; c < 3; c++) {
+            rec.kc[c] = waveno * com[c];
+            rec.eps[c] = (float)(com[c] / R);
+            rec.ea[c] = (float)(ea[c] / R);
+            rec.inc[c] = (float)fr.inc2[c];
+            rec.vx[c] = (float)xa[c];
+            rec.vy[c] = (float)ya[c];
+        }
+        rec.b = (float)((com[0] * com[0] + com[1] * com[1] + com[2] * com[2]) / (R * R));
+        for (int q = 0; q < 9; q++) rec.R[q] = (float)fr.R.m[q / 3][q % 3];
+        rec.kp[0] = (float)(waveno * fr.prop2[0]);
+        rec.kp[1] = (float)(waveno * fr.prop2[1]);
+        rec.hkz_cf = (float)(-0.5 * fr.prop2[2] * cf);
+        rec.hicf = (float)(0.5 / cf);
+        rec.hkxky_cf = (float)(0.5 * fr.prop2[0] * Ky * cf);
+        for (int q = 0; q < 4; q++) {
+            rec.amp[2 * q] = (float)(-cpre * ob->ampl[2 * q + 1]);
+            rec.amp[2 * q + 1] = (float)(cpre * ob->ampl[2 * q]);
+        }
+        recs[r0 + t] = rec;
+        if (fast_diff) {
+            K2Fov fv;
+            const double fov = kind ? kPiRef / 2.0 : ob->fov;
+            fv.p0[0] = (float)prop0[0];
+            fv.p0[1] = (float)prop0[1];
+            fv.p0[2] = (float)prop0[2];
+            fv.cos_fov = (float)cos(fov);
+            fovs[r0 + t] = fv;
+        }
+    }
+}
+
+// Per orientation chunk [o0, o0+no): segment records and work-item prefix.
+__global__ void k2_plan_kernel(const int64_t *__restrict__ start, const int64_t *__restrict__ refbase,
+                               const int64_t *__restrict__ beam_off, int64_t o0, int64_t no,
+                               int64_t rpi, int64_t ntiles, int64_t *__restrict__ seg_rec,
+                               int64_t *__restrict__ item_pre, unsigned long long *__restrict__ counter) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int64_t q = 0; q < no; q++) {
+        const int64_t o = o0 + q;
+        const int64_t nbo = beam_off[o + 1] - beam_off[o];
+        seg_rec[2 * q] = start[refbase[o]];
+        seg_rec[2 * q + 1] = start[refbase[o] + nbo];
+    }
+    seg_rec[2 * no] = start[refbase[o0 + no]];
+    int64_t p = 0;
+    for (int64_t s = 0; s < 2 * no; s++) {
+        item_pre[s] = p;
+        const int64_t n = seg_rec[s + 1] - seg_rec[s];
+        p += ((n + rpi - 1) / rpi) * ntiles;
+    }
+    item_pre[2 * no] = p;
+    *counter = 0ull;
+}
+
+// ------------------------------------------------------------ main kernel
+
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// sin(h)/h for h >= 0: Taylor series below 0.5, MUFU sine above
+__device__ __forceinline__ float sinc_pos(float h) {
+    const float h2 = h * h;
+    const float p = fmaf(h2, fmaf(h2, fmaf(h2, fmaf(h2, 2.7557319e-6f, -1.9841270e-4f), 8.3333333e-3f),
+                                  -1.6666667e-1f),
+                         1.0f);
+    const float q = __sinf(h) * rcp_approx(h);
+    return h < 0.5f ? p : q;
+}
+
+// Second divided difference of e^{ix} at t1, t2, t3 (symmetric in its arguments).
+__device__ __forceinline__ float2 tri_dd(float t1, float t2, float t3) {
+    float lo = fminf(t1, t2), hi = fmaxf(t1, t2);
+    const float mid = fmaxf(lo, fminf(hi, t3));
+    lo = fminf(lo, t3);
+    hi = fmaxf(hi, t3);
+    const float D = hi - lo;
+    float2 g;
+    if (D >= 0.25f) {
+        const float h1 = 0.5f * (mid - lo), h2 = 0.5f * (hi - mid);
+        float s1, c1, s2, c2;
+        __sincosf(lo + h1, &s1, &c1);
+        __sincosf(mid + h2, &s2, &c2);
+        const float sc1 = sinc_pos(h1), sc2 = sinc_pos(h2);
+        const float iD = rcp_approx(D);
+        g.x = (sc1 * s1 - sc2 * s2) * iD;
+        g.y = (sc2 * c2 - sc1 * c1) * iD;
+    } else {
+        // e^{i mid} * sum_n i^(n+2)/(n+2)! h_n(ya, yc), h_n complete homogeneous
+        const float ya = lo - mid, yc = hi - mid;
+        const float h1 = ya + yc;
+        const float ya2 = ya * ya;
+        const float h2 = fmaf(yc, h1, ya2);
+        const float ya3 = ya2 * ya;
+        const float h3 = fmaf(yc, h2, ya3);
+        const float ya4 = ya3 * ya;
+        const float h4 = fmaf(yc, h3, ya4);
+        const float h5 = fmaf(yc, h4, ya4 * ya);
+        const float h6 = fmaf(yc, h5, ya4 * ya2);
+        const float re = -0.5f + h2 * (1.0f / 24.0f) - h4 * (1.0f / 720.0f) + h6 * (1.0f / 40320.0f);
+        const float im = -h1 * (1.0f / 6.0f) + h3 * (1.0f / 120.0f) - h5 * (1.0f / 5040.0f);
+        float sm, cm;
+        __sincosf(mid, &sm, &cm);
+        g.x = cm * re - sm * im;
+        g.y = cm * im + sm * re;
+    }
+    return g;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+// Bounded wait on an mbarrier phase: false after ~2 s.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    uint64_t t0 = 0;
+    for (uint32_t it = 0;; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (it == 0) t0 = gtimer();
+        else if ((it & 255) == 0 && gtimer() - t0 > 2000000000ull) return false;
+    }
+}
+
+struct K2MainArgs {
+    const K2Rec *recs;
+    const K2Fov *fovs;
+    const int64_t *seg_rec;
+    const int64_t *item_pre;
+    int64_t nseg;
+    int64_t rpi;
+    int64_t ntiles;
+    const double *xyz;
+    int64_t nb, nphi;
+    int64_t theta_i;
+    float k;      // wavenumber
+    float hkR;    // k R / 2
+    float *ws;    // [seg][8][nb]
+    unsigned long long *counter;
+    int *err;
+};
+
+template <int BPT, bool FAST>
+__device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const BinDev (&bd)[BPT],
+                                          const bool (&valid)[BPT], float (&acc)[BPT][8], float k,
+                                          float hkR) {
+    const double kc0 = r.kc[0], kc1 = r.kc[1], kc2 = r.kc[2];
+#pragma unroll
+    for (int q = 0; q < BPT; q++) {
+        const BinDev &B = bd[q];
+        // far-field phase: FP64 k u.c, reduced mod 2 pi
+        const double ka = fma(B.uz, kc2, fma(B.uy, kc1, B.ux * kc0));
+        const double nq = fma(ka, kInv2Pi, kMagic) - kMagic;
+        const float rf = (float)fma(-nq, kTwoPi, ka);
+        const float a = fmaf(B.fz, r.eps[2], fmaf(B.fy, r.eps[1], B.fx * r.eps[0]));
+        const float ph = fmaf(hkR * fmaf(-a, a, r.b), 1.0f + a, -rf);
+        // bin direction from the facet centre, in the aperture frame
+        const float opa = 1.0f + a;
+        const float w0 = fmaf(r.R[2], B.fz, fmaf(r.R[1], B.fy, r.R[0] * B.fx));
+        const float w1 = fmaf(r.R[5], B.fz, fmaf(r.R[4], B.fy, r.R[3] * B.fx));
+        const float w2 = fmaf(r.R[8], B.fz, fmaf(r.R[7], B.fy, r.R[6] * B.fx));
+        const float kx = fmaf(w0, opa, -r.ea[0]);
+        const float ky = fmaf(w1, opa, -r.ea[1]);
+        const float kz = fmaf(w2, opa, -r.ea[2]);
+        bool use = valid[q];
+        if (FAST) {
+            // lab-frame direction from the centre: u - eps + u a
+            const float dx = fmaf(B.fx, opa, -r.eps[0]);
+            const float dy = fmaf(B.fy, opa, -r.eps[1]);
+            const float dz = fmaf(B.fz, opa, -r.eps[2]);
+            const float dp = fmaf(dz, fv->p0[2], fmaf(dy, fv->p0[1], dx * fv->p0[0]));
+            use = use && !(dp < fv->cos_fov);
+        }
+        // aperture integral
+        const float kxx = fmaf(-k, kx, r.kp[0]);
+        const float kyy = fmaf(-k, ky, r.kp[1]);
+        const float t1 = fmaf(kyy, r.vy[0], fmaf(kxx, r.vx[0], ph));
+        const float t2 = fmaf(kyy, r.vy[1], fmaf(kxx, r.vx[1], ph));
+        const float t3 = fmaf(kyy, r.vy[2], fmaf(kxx, r.vx[2], ph));
+        const float2 g = tri_dd(t1, t2, t3);
+        // Karczewski-Wolf polarisation matrix [[d, e], [-e, d]]
+        const float kyc = fminf(fmaxf(ky, -0.999999f), 0.999999f);
+        const float tt = fmaf(-kyc, kyc, 1.0f);
+        const float rs = rsqrtf(tt);
+        const float s = tt * rs;
+        const float kyrs = kyc * rs;
+        const float m0 = -kx * kyrs, m1 = s, m2 = -kz * kyrs;
+        const float d = fmaf(r.hkz_cf, s, -(kz * rs) * r.hicf);
+        const float e = fmaf(r.hkxky_cf, s, -(kx * kyrs) * r.hicf);
+        // vector perpendicular to the scattering plane (forward bodge near the poles)
+        float qx = kx, qy = kyc, qz = kz;
+        const float dinc = fmaf(r.inc[2], kz, fmaf(r.inc[1], kyc, r.inc[0] * kx));
+        if (!(fabsf(dinc) < 0.999f)) {
+            const float ah = fmaf(B.hz, r.eps[2], fmaf(B.hy, r.eps[1], B.hx * r.eps[0]));
+            const float oh = 1.0f + ah;
+            qx = fmaf(fmaf(r.R[2], B.hz, fmaf(r.R[1], B.hy, r.R[0] * B.hx)), oh, -r.ea[0]);
+            qy = fmaf(fmaf(r.R[5], B.hz, fmaf(r.R[4], B.hy, r.R[3] * B.hx)), oh, -r.ea[1]);
+            qz = fmaf(fmaf(r.R[8], B.hz, fmaf(r.R[7], B.hy, r.R[6] * B.hx)), oh, -r.ea[2]);
+        }
+        float hx = fmaf(r.inc[1], qz, -r.inc[2] * qy);
+        float hy = fmaf(r.inc[2], qx, -r.inc[0] * qz);
+        float hz = fmaf(r.inc[0], qy, -r.inc[1] * qx);
+        const float hn = rsqrtf(fmaf(hz, hz, fmaf(hy, hy, hx * hx)));
+        hx *= hn;
+        hy *= hn;
+        hz *= hn;
+        const float ex = fmaf(kyc, m2, -kz * m1);
+        const float ey = fmaf(kz, m0, -kx * m2);
+        const float ez = fmaf(kx, m1, -kyc * m0);
+        const float p = fmaf(hz, m2, fmaf(hy, m1, hx * m0));
+        const float rr = fmaf(hz, ez, fmaf(hy, ey, hx * ex));
+        const float A = fmaf(p, d, rr * e);
+        const float Bc = fmaf(p, e, -rr * d);
+        // G = [[A, B], [-B, A]] . amp ; acc += g * G
+        const float gx = use ? g.x : 0.0f, gy = use ? g.y : 0.0f;
+        float G[8];
+        G[0] = fmaf(A, r.amp[0], Bc * r.amp[2]);
+        G[1] = fmaf(A, r.amp[1], Bc * r.amp[3]);
+        G[2] = fmaf(A, r.amp[2], -Bc * r.amp[0]);
+        G[3] = fmaf(A, r.amp[3], -Bc * r.amp[1]);
+        G[4] = fmaf(A, r.amp[4], Bc * r.amp[6]);
+        G[5] = fmaf(A, r.amp[5], Bc * r.amp[7]);
+        G[6] = fmaf(A, r.amp[6], -Bc * r.amp[4]);
+        G[7] = fmaf(A, r.amp[7], -Bc * r.amp[5]);
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            acc[q][2 * c] = fmaf(gx, G[2 * c], fmaf(-gy, G[2 * c + 1], acc[q][2 * c]));
+            acc[q][2 * c + 1] = fmaf(gx, G[2 * c + 1], fmaf(gy, G[2 * c], acc[q][2 * c + 1]));
+        }
+    }
+}
+
+template <int BPT, bool FAST>
+__global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
+    __shared__ __align__(128) K2Rec sbuf[K2_NST][K2_CH];
+    __shared__ __align__(8) uint64_t bars[K2_NST];
+    __shared__ long long s_item;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < K2_NST; s++) mbar_init(smem_u32(&bars[s]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t parity[K2_NST] = {0, 0, 0};
+    const int64_t total = P.item_pre[P.nseg];
+    constexpr int64_t TILE = (int64_t)K2_THREADS * BPT;
+    for (;;) {
+        if (tid == 0) s_item = (long long)atomicAdd(P.counter, 1ull);
+        __syncthreads();
+        const int64_t item = s_item;
+        if (item >= total) break;
+        // decode item -> (segment, split, tile)
+        int64_t lo = 0, hi = P.nseg;
+        while (hi - lo > 1) {
+            const int64_t m = (lo + hi) >> 1;
+            if (P.item_pre[m] <= item)
+                lo = m;
+            else
+                hi = m;
+        }
+        const int64_t seg = lo;
+        const int64_t local = item - P.item_pre[seg];
+        const int64_t split = local / P.ntiles, tile = local % P.ntiles;
+        const int64_t rbeg = P.seg_rec[seg] + split * P.rpi;
+        const int64_t rend = min(rbeg + P.rpi, P.seg_rec[seg + 1]);
+        // bins of this thread
+        BinDev bd[BPT];
+        bool valid[BPT];
+        int64_t bin[BPT];
+#pragma unroll
+        for (int q = 0; q < BPT; q++) {
+            bin[q] = tile * TILE + q * K2_THREADS + tid;
+            valid[q] = bin[q] < P.nb;
+            const int64_t o = valid[q] ? bin[q] : 0;
+            const double X = P.xyz[o], Y = P.xyz[P.nb + o], Zc = P.xyz[2 * P.nb + o];
+            const double ir = 1.0 / sqrt(X * X + Y * Y + Zc * Zc);
+            bd[q].ux = X * ir;
+            bd[q].uy = Y * ir;
+            bd[q].uz = Zc * ir;
+            bd[q].fx = (float)bd[q].ux;
+            bd[q].fy = (float)bd[q].uy;
+            bd[q].fz = (float)bd[q].uz;
+            const int64_t oh = (o % P.nphi) + P.nphi * P.theta_i;
+            const double Xh = P.xyz[oh], Yh = P.xyz[P.nb + oh], Zh = P.xyz[2 * P.nb + oh];
+            const double irh = 1.0 / sqrt(Xh * Xh + Yh * Yh + Zh * Zh);
+            bd[q].hx = (float)(Xh * irh);
+            bd[q].hy = (float)(Yh * irh);
+            bd[q].hz = (float)(Zh * irh);
+        }
+        double acc64[BPT][8];
+#pragma unroll
+        for (int q = 0; q < BPT; q++)
+#pragma unroll
+            for (int c = 0; c < 8; c++) acc64[q][c] = 0.0;
+        const int64_t nrec = rend - rbeg;
+        const int64_t nchunk = (nrec + K2_CH - 1) / K2_CH;
+        if (tid == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            for (int64_t c = 0; c < nchunk && c < K2_NST; c++) {
+                const int64_t n = min((int64_t)K2_CH, nrec - c * K2_CH);
+                bulk_load(smem_u32(&sbuf[c][0]), P.recs + rbeg + c * K2_CH,
+                          (uint32_t)(n * sizeof(K2Rec)), smem_u32(&bars[c]));
+            }
+        }
+        bool timed_out = false;
+        for (int64_t c = 0; c < nchunk; c++) {
+            const int st = (int)(c % K2_NST);
+            const bool ok = mbar_wait(smem_u32(&bars[st]), parity[st]);
+            parity[st] ^= 1u;
+            if (__syncthreads_or(!ok)) {
+                timed_out = true;
+                break;
+            }
+            const int n = (int)min((int64_t)K2_CH, nrec - c * K2_CH);
+            float acc[BPT][8];
+#pragma unroll
+            for (int q = 0; q < BPT; q++)
+#pragma unroll
+                for (int cc = 0; cc < 8; cc++) acc[q][cc] = 0.0f;
+            const K2Fov *fv = FAST ? P.fovs + rbeg + c * K2_CH : nullptr;
+            for (int j = 0; j < n; j++)
+                k2_record<BPT, FAST>(sbuf[st][j], FAST ? fv + j : nullptr, bd, valid, acc, P.k,
+                                     P.hkR);
+#pragma unroll
+            for (int q = 0; q < BPT; q++)
+#pragma unroll
+                for (int cc = 0; cc < 8; cc++) acc64[q][cc] += (double)acc[q][cc];
+            __syncthreads();  // every thread is done with stage st
+            if (tid == 0 && c + K2_NST < nchunk) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                const int64_t c2 = c + K2_NST;
+                const int64_t n2 = min((int64_t)K2_CH, nrec - c2 * K2_CH);
+                bulk_load(smem_u32(&sbuf[st][0]), P.recs + rbeg + c2 * K2_CH,
+                          (uint32_t)(n2 * sizeof(K2Rec)), smem_u32(&bars[st]));
+            }
+        }
+        if (timed_out) {
+            if (tid == 0) atomicOr(P.err, 4);
+            return;
+        }
+        float *out = P.ws + seg * 8 * P.nb;
+#pragma unroll
+        for (int q = 0; q < BPT; q++)
+            if (valid[q])
+#pragma unroll
+                for (int cc = 0; cc < 8; cc++) atomicAdd(out + cc * P.nb + bin[q], (float)acc64[q][cc]);
+    }
+}
+
+// --------------------------------------------------------------- epilogue
+
+struct Zd {
+    double re, im;
+};
+__device__ __forceinline__ double re_mc(Zd a, Zd b) { return a.re * b.re + a.im * b.im; }
+__device__ __forceinline__ double im_mc(Zd a, Zd b) { return a.im * b.re - a.re * b.im; }
+
+__device__ __forceinline__ void mueller16d(const Zd *S, double mu[16]) {
+    const Zd a11 = S[0], a21 = S[1], a12 = S[2], a22 = S[3];
+    const double p11 = re_mc(a11, a11), p12 = re_mc(a12, a12), p21 = re_mc(a21, a21),
+                 p22 = re_mc(a22, a22);
+    mu[0] = 0.5 * (p11 + p12 + p21 + p22);
+    mu[1] = 0.5 * (p11 - p12 + p21 - p22);
+    mu[2] = re_mc(a11, a12) + re_mc(a22, a21);
+    mu[3] = im_mc(a11, a12) - im_mc(a22, a21);
+    mu[4] = 0.5 * (p11 + p12 - p21 - p22);
+    mu[5] = 0.5 * (p11 - p12 - p21 + p22);
+    mu[6] = re_mc(a11, a12) - re_mc(a22, a21);
+    mu[7] = im_mc(a11, a12) + im_mc(a22, a21);
+    mu[8] = re_mc(a11, a21) + re_mc(a22, a12);
+    mu[9] = re_mc(a11, a21) - re_mc(a22, a12);
+    mu[10] = re_mc(a11, a22) + re_mc(a12, a21);
+    mu[11] = im_mc(a11, a22) + im_mc(a21, a12);
+    mu[12] = im_mc(a21, a11) + im_mc(a22, a12);
+    mu[13] = im_mc(a21, a11) - im_mc(a22, a12);
+    mu[14] = im_mc(a22, a11) - im_mc(a12, a21);
+    mu[15] = re_mc(a22, a11) - re_mc(a12, a21);
+}
+
+// Amplitude of segment seg at bin o as reference-layout complex 2x2 (with
+// T(phi) applied and scaled by sc), common phase e^{ik|X|} omitted.
+__device__ __forceinline__ void ws_ampl(const float *ws, int64_t seg, int64_t nb, int64_t o, double cp,
+                                        double sp, double sc, Zd S[4]) {
+    const float *w = ws + seg * 8 * nb + o;
+    Zd a[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        a[c].re = (double)w[(2 * c) * nb];
+        a[c].im = (double)w[(2 * c + 1) * nb];
+    }
+    // (S T)(a,b) = S(a,1) T(1,b) + S(a,2) T(2,b); T = [[-s, -c], [c, -s]]
+    // order (1,1),(2,1),(1,2),(2,2): a[0]=S11 a[1]=S21 a[2]=S12 a[3]=S22
+    const double T11 = -sp, T12 = -cp, T21 = cp, T22 = -sp;
+    S[0] = {(a[0].re * T11 + a[2].re * T21) * sc, (a[0].im * T11 + a[2].im * T21) * sc};
+    S[1] = {(a[1].re * T11 + a[3].re * T21) * sc, (a[1].im * T11 + a[3].im * T21) * sc};
+    S[2] = {(a[0].re * T12 + a[2].re * T22) * sc, (a[0].im * T12 + a[2].im * T22) * sc};
+    S[3] = {(a[1].re * T12 + a[3].re * T22) * sc, (a[1].im * T12 + a[3].im * T22) * sc};
+}
+
+__device__ __forceinline__ double block_sum(double v, double *red) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += red[i];
+    __syncthreads();
+    return s;
+}
+
+// Pre-pass of -scaling: per-orientation scatt_beam / scatt_ext sums.
+__global__ void k2_scatt_be_kernel(const float *__restrict__ ws, int64_t no, int64_t o0, int64_t nb,
+                                   int64_t nphi, const double *__restrict__ phitab, double waveno,
+                                   const double *__restrict__ wbin, double *__restrict__ sums) {
+    __shared__ double red[32];
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = o < nb;
+    const int64_t oo = in ? o : 0;
+    const double cp = phitab[oo % nphi], sp = phitab[nphi + oo % nphi];
+    const double W = in ? wbin[oo] / (waveno * waveno) : 0.0;
+    for (int64_t q = 0; q < no; q++) {
+        Zd Sb[4], Se[4];
+        ws_ampl(ws, 2 * q, nb, oo, cp, sp, waveno, Sb);
+        ws_ampl(ws, 2 * q + 1, nb, oo, cp, sp, waveno, Se);
+        double mb[16], me[16];
+        mueller16d(Sb, mb);
+        mueller16d(Se, me);
+        const double vb = block_sum(W * mb[0], red);
+        const double ve = block_sum(W * me[0], red);
+        if (threadIdx.x == 0) {
+            atomicAdd(&sums[2 * (o0 + q)], vb);
+            atomicAdd(&sums[2 * (o0 + q) + 1], ve);
+        }
+    }
+}
+
+// sqrt(scatt_part / energy_part) per orientation (src/outputs_mod.f90:151,154)
+__global__ void k2_scale_kernel(double *__restrict__ scale, const pbt_output_params *__restrict__ pin,
+                                int64_t o0, int64_t no) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= no) return;
+    const int64_t o = o0 + q;
+    scale[2 * o] = sqrt(scale[2 * o] / pin[o].beam_energy_out);
+    scale[2 * o + 1] = sqrt(scale[2 * o + 1] / pin[o].ext_energy_out);
+}
+
+// Main epilogue: Mueller sum over the chunk's orientations and per-orientation
+// weighted sums  red[o] = {scatt, scatt_beam, scatt_ext, g_num, g_num_beam, g_num_ext}.
+__global__ void k2_epi_kernel(const float *__restrict__ ws, int64_t no, int64_t o0, int64_t nb,
+                              int64_t nphi, const double *__restrict__ phitab,
+                              const double *__restrict__ cth, double waveno,
+                              const double *__restrict__ wbin, int64_t back_bin,
+                              const double *__restrict__ scale, double *__restrict__ mu_sum,
+                              double *__restrict__ redo, double *__restrict__ bs) {
+    __shared__ double red[32];
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = o < nb;
+    const int64_t oo = in ? o : 0;
+    const int64_t i = oo % nphi, j = oo / nphi;
+    const double cp = phitab[i], sp = phitab[nphi + i];
+    const double W = in ? wbin[oo] / (waveno * waveno) : 0.0;
+    const double ct = cth[j];
+    double acc[16];
+#pragma unroll
+    for (int e = 0; e < 16; e++) acc[e] = 0.0;
+    for (int64_t q = 0; q < no; q++) {
+        const int64_t og = o0 + q;
+        const double sb = scale ? 1.0 / scale[2 * og] : 1.0;
+        const double se = scale ? 1.0 / scale[2 * og + 1] : 1.0;
+        Zd Sb[4], Se[4], St[4];
+        ws_ampl(ws, 2 * q, nb, oo, cp, sp, waveno * sb, Sb);
+        ws_ampl(ws, 2 * q + 1, nb, oo, cp, sp, waveno * se, Se);
+#pragma unroll
+        for (int c = 0; c < 4; c++) St[c] = {Sb[c].re + Se[c].re, Sb[c].im + Se[c].im};
+        double m[16];
+        mueller16d(St, m);
+#pragma unroll
+        for (int e = 0; e < 16; e++) acc[e] += m[e];
+        const double mb = 0.5 * (re_mc(Sb[0], Sb[0]) + re_mc(Sb[2], Sb[2]) + re_mc(Sb[1], Sb[1]) +
+                                 re_mc(Sb[3], Sb[3]));
+        const double me = 0.5 * (re_mc(Se[0], Se[0]) + re_mc(Se[2], Se[2]) + re_mc(Se[1], Se[1]) +
+                                 re_mc(Se[3], Se[3]));
+        double v[6] = {W * m[0], W * mb, W * me, W * ct * m[0], W * ct * mb, W * ct * me};
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const double s = block_sum(v[k], red);
+            if (threadIdx.x == 0) atomicAdd(&redo[6 * og + k], s);
+        }
+        if (in && o == back_bin) bs[og] = m[0] * 4.0 * kPiRef / (waveno * waveno);
+    }
+    if (in)
+#pragma unroll
+        for (int e = 0; e < 16; e++) mu_sum[e * nb + o] += acc[e];
+}
+
+__global__ void k2_final_kernel(const double *__restrict__ redo, const double *__restrict__ bs,
+                                const pbt_output_params *__restrict__ pin, int64_t norient,
+                                pbt_output_params *__restrict__ pout) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= norient) return;
+    const double *r = redo + 6 * o;
+    pbt_output_params p = pin[o];
+    const double scatt = r[0], scatt_b = r[1], scatt_e = r[2];
+    p.scatt = scatt;
+    p.ext = p.abs + scatt;
+    p.albedo = 1 - (p.ext - scatt) / p.ext;
+    p.asymmetry = r[3] / scatt;
+    p.abs_eff = p.abs / p.geo_cross_sec;
+    p.scatt_eff = scatt / p.geo_cross_sec;
+    p.ext_eff = p.ext / p.geo_cross_sec;
+    p.back_scatt = bs[o];
+    p.scatt_beam = scatt_b;
+    p.scatt_ext_diff = scatt_e;
+    p.asymmetry_beam = r[4] / scatt_b;
+    p.asymmetry_ext_diff = r[5] / scatt_e;
+    p.scatt_eff_beam = scatt_b / p.geo_cross_sec;
+    p.scatt_eff_ext_diff = scatt_e / p.geo_cross_sec;
+    pout[o] = p;
+}
+
+// Orientation average of the parameters (summation then divide), one thread per field.
+__global__ void k2_param_avg_kernel(const pbt_output_params *__restrict__ per, int64_t norient,
+                                    pbt_output_params *__restrict__ avg) {
+    const int f = threadIdx.x;
+    if (f >= 18) return;
+    const double *src = reinterpret_cast<const double *>(per);
+    double s = 0.0;
+    for (int64_t o = 0; o < norient; o++) s = s + src[18 * o + f];
+    // beam_energy_out / ext_energy_out are not summed by the reference
+    reinterpret_cast<double *>(avg)[f] = (f == 10 || f == 11) ? 0.0 : s / (double)norient;
+}
+
+__global__ void k2_mu_avg_kernel(const double *__restrict__ mu_sum, int64_t n, double inv_n,
+                                 double norient, double *__restrict__ mu_avg) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) mu_avg[q] = mu_sum[q] / norient;
+    (void)inv_n;
+}
+
+__global__ void k2_phi_int_kernel(const double *__restrict__ mu, const double *__restrict__ wphi,
+                                  int64_t nphi, int64_t ntheta, double *__restrict__ m1d) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 16 * ntheta) return;
+    const int64_t j = t % ntheta, e = t / ntheta;
+    const double *src = mu + e * nphi * ntheta + nphi * j;
+    double s = 0.0;
+    for (int64_t i = 0; i < nphi; i++) s += wphi[i] * src[i];
+    m1d[j + ntheta * e] = s;
+}
+
+// FP32 diff_main output: reference-layout complex(8) grids, e^{ik|X|} S' T(phi).
+__global__ void k2_ampl_out_kernel(const float *__restrict__ ws, int64_t nb, int64_t nphi,
+                                   const double *__restrict__ phitab, const double *__restrict__ xyz,
+                                   double waveno, double *__restrict__ afb, double *__restrict__ afe) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nb) return;
+    const double cp = phitab[o % nphi], sp = phitab[nphi + o % nphi];
+    const double X = xyz[o], Y = xyz[nb + o], Zc = xyz[2 * nb + o];
+    double sK, cK;
+    sincos(waveno * sqrt(X * X + Y * Y + Zc * Zc), &sK, &cK);
+    for (int kind = 0; kind < 2; kind++) {
+        Zd S[4];
+        ws_ampl(ws, kind, nb, o, cp, sp, 1.0, S);
+        double *dst = kind ? afe : afb;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            dst[2 * (o + nb * c)] = S[c].re * cK - S[c].im * sK;
+            dst[2 * (o + nb * c) + 1] = S[c].re * sK + S[c].im * cK;
+        }
+    }
+}
+
+}  // namespace
+
+// --------------------------------------------------------------- host side
+
+namespace {
+
+struct K2Plan {
+    int bpt = 2;
+    int64_t rpi = 2048;  // facet records per work item
+};
+
+// Device-side set-up shared by the batched and single-orientation entry points.
+struct K2Setup {
+    K2Rec *recs = nullptr;
+    K2Fov *fovs = nullptr;
+    int64_t *start = nullptr;
+    int64_t *refbase = nullptr;
+    int64_t *beam_off = nullptr;
+    int64_t *ext_off = nullptr;
+    int *err = nullptr;
+};
+
+size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam *d_beam,
+               const int64_t *h_beam_off, const pbt_outbeam *d_ext, const int64_t *h_ext_off,
+               const double *d_verts, int64_t nverts, const int64_t *d_face_off,
+               const int64_t *d_face_vi, int64_t nfaces, int64_t max_nv, double lambda,
+               int fast_diff, K2Setup &S) {
+    const int64_t nrefs = h_beam_off[norient] + h_ext_off[norient];
+    const int64_t max_recs = std::max<int64_t>(1, nrefs * std::max<int64_t>(1, max_nv - 2));
+    // scan temp size
+    size_t scan_tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (int64_t *)nullptr, (int64_t *)nullptr,
+                                  (int)(nrefs + 1), st);
+    // d_in: cnt | start | refbase | beam_off | ext_off | err | scan tmp
+    const size_t o_cnt = 0, o_start = align_up(o_cnt + (nrefs + 1) * 8),
+                 o_rb = align_up(o_start + (nrefs + 1) * 8),
+                 o_bo = align_up(o_rb + (norient + 1) * 8), o_eo = align_up(o_bo + (norient + 1) * 8),
+                 o_err = align_up(o_eo + (norient + 1) * 8), o_tmp = align_up(o_err + 64),
+                 o_end = align_up(o_tmp + scan_tmp);
+    PBT_TRY(ctx->d_scan.ensure(o_end));
+    char *base = ctx->d_scan.as<char>();
+    int64_t *cnt = (int64_t *)(base + o_cnt);
+    S.start = (int64_t *)(base + o_start);
+    S.refbase = (int64_t *)(base + o_rb);
+    S.beam_off = (int64_t *)(base + o_bo);
+    S.ext_off = (int64_t *)(base + o_eo);
+    S.err = (int *)(base + o_err);
+    void *tmp = base + o_tmp;
+    PBT_TRY(ctx->d_rec.ensure(align_up(max_recs * sizeof(K2Rec)) +
+                              (fast_diff ? max_recs * sizeof(K2Fov) : 0)));
+    S.recs = ctx->d_rec.as<K2Rec>();
+    S.fovs = fast_diff ? (K2Fov *)(ctx->d_rec.as<char>() + align_up(max_recs * sizeof(K2Rec))) : nullptr;
+    // host-side offsets -> device (pinned staging; the previous call's copy
+    // out of the staging buffer must have run before it is overwritten)
+    if (ctx->stage_pending) {
+        PBT_CUDA_TRY(cudaEventSynchronize(ctx->stage_ev));
+        ctx->stage_pending = false;
+    }
+    if (!ctx->stage_ev) PBT_CUDA_TRY(cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming));
+    PBT_TRY(ctx->h_stage.ensure(3 * (norient + 1) * 8));
+    int64_t *hs = ctx->h_stage.as<int64_t>();
+    for (int64_t o = 0; o <= norient; o++) {
+        hs[o] = h_beam_off[o] + h_ext_off[o];
+        hs[norient + 1 + o] = h_beam_off[o];
+        hs[2 * (norient + 1) + o] = h_ext_off[o];
+    }
+    PBT_CUDA_TRY(cudaMemcpyAsync(S.refbase, hs, (norient + 1) * 8, cudaMemcpyHostToDevice, st));
+    PBT_CUDA_TRY(cudaMemcpyAsync(S.beam_off, hs + norient + 1, (norient + 1) * 8,
+                                 cudaMemcpyHostToDevice, st));
+    PBT_CUDA_TRY(cudaMemcpyAsync(S.ext_off, hs + 2 * (norient + 1), (norient + 1) * 8,
+                                 cudaMemcpyHostToDevice, st));
+    PBT_CUDA_TRY(cudaEventRecord(ctx->stage_ev, st));
+    ctx->stage_pending = true;
+    PBT_CUDA_TRY(cudaMemsetAsync(S.err, 0, sizeof(int), st));
+    RefSrc src{d_beam, d_ext, S.beam_off, S.ext_off, S.refbase, norient};
+    const int th = 256;
+    k2_count_kernel<<<(unsigned)((nrefs + 1 + th - 1) / th), th, 0, st>>>(src, nrefs, d_face_off,
+                                                                          nfaces, cnt, S.err);
+    PBT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, scan_tmp, cnt, S.start, (int)(nrefs + 1), st));
+    const double waveno = 2.0 * kPiRef / lambda;
+    if (nrefs > 0)
+        k2_setup_kernel<<<(unsigned)((nrefs + th - 1) / th), th, 0, st>>>(
+            src, nrefs, d_verts, nverts, d_face_off, d_face_vi, S.start, waveno, lambda, fast_diff,
+            S.recs, S.fovs, S.err);
+    ctx->launches += 3;
+    PBT_CUDA_TRY(cudaGetLastError());
+    return PBT_OK;
+}
+
+template <int BPT, bool FAST>
+int k2_launch_main(pbt_ctx *ctx, cudaStream_t st, const K2MainArgs &A) {
+    static int occ = -1;
+    if (occ < 0) {
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k2_main_kernel<BPT, FAST>, K2_THREADS, 0);
+        occ = n > 0 ? n : 1;
+    }
+    const int grid = ctx->sm_count * occ;
+    timing_begin(ctx, st);
+    k2_main_kernel<BPT, FAST><<<grid, K2_THREADS, 0, st>>>(A);
+    timing_end(ctx, st);
+    ctx->launches++;
+    PBT_CUDA_TRY(cudaGetLastError());
+    return PBT_OK;
+}
+
+int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, int64_t no,
+                 double lambda, int fast_diff, const K2Plan &plan, float *ws, int64_t *seg_rec,
+                 int64_t *item_pre, unsigned long long *counter) {
+    const GridCache &g = ctx->grid;
+    const int64_t tile = (int64_t)K2_THREADS * plan.bpt;
+    const int64_t ntiles = (g.nb + tile - 1) / tile;
+    k2_plan_kernel<<<1, 32, 0, st>>>(S.start, S.refbase, S.beam_off, o0, no, plan.rpi, ntiles,
+                                     seg_rec, item_pre, counter);
+    ctx->launches++;
+    PBT_CUDA_TRY(cudaMemsetAsync(ws, 0, (size_t)2 * no * 8 * g.nb * sizeof(float), st));
+    const double waveno = 2.0 * kPiRef / lambda;
+    K2MainArgs A;
+    A.recs = S.recs;
+    A.fovs = S.fovs;
+    A.seg_rec = seg_rec;
+    A.item_pre = item_pre;
+    A.nseg = 2 * no;
+    A.rpi = plan.rpi;
+    A.ntiles = ntiles;
+    A.xyz = g.xyz.as<double>();
+    A.nb = g.nb;
+    A.nphi = (int64_t)g.phi.size();
+    A.theta_i = g.theta_i;
+    A.k = (float)waveno;
+    A.hkR = (float)(0.5 * waveno * kFarR);
+    A.ws = ws;
+    A.counter = counter;
+    A.err = S.err;
+    if (plan.bpt == 1)
+        return fast_diff ? k2_launch_main<1, true>(ctx, st, A) : k2_launch_main<1, false>(ctx, st, A);
+    return fast_diff ? k2_launch_main<2, true>(ctx, st, A) : k2_launch_main<2, false>(ctx, st, A);
+}
+
+int64_t max_face_nv(const int64_t *h_face_off, int64_t nfaces) {
+    int64_t m = 3;
+    for (int64_t f = 0; f < nfaces; f++) m = std::max(m, h_face_off[f + 1] - h_face_off[f]);
+    return m;
+}
+
+}  // namespace
+
+int k2_check_err(pbt_ctx *ctx, cudaStream_t st, const int *d_err) {
+    int h = 0;
+    PBT_CUDA_TRY(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PBT_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h & 1) {
+        set_error("an outbeam face index fi is out of range");
+        return PBT_EINVAL;
+    }
+    if (h & 2) {
+        set_error("the FP32 path supports faces of up to 16 vertices");
+        return PBT_EINVAL;
+    }
+    if (h & 4) {
+        set_error("a bounded device wait timed out in the far-field kernel");
+        return PBT_ETIMEOUT;
+    }
+    return PBT_OK;
+}
+
+// Batched FP32 orientation average.  h_beam_off / h_ext_off / h_face_off are
+// host arrays; every other array is device memory.
+int k2_batch_impl(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam *d_beam,
+                  const int64_t *h_beam_off, const pbt_outbeam *d_ext, const int64_t *h_ext_off,
+                  const double *d_verts, int64_t nverts, const int64_t *h_face_off,
+                  const int64_t *d_face_off, const int64_t *d_face_vi, int64_t nfaces,
+                  double lambda, int fast_diff, int scaling, const pbt_output_params *d_params_in,
+                  double *d_mueller_avg, double *d_m1d_avg, pbt_output_params *d_params_avg,
+                  pbt_output_params *d_params_per, int check_errors) {
+    const GridCache &g = ctx->grid;
+    const int64_t nb = g.nb, nphi = (int64_t)g.phi.size(), ntheta = (int64_t)g.theta.size();
+    K2Plan plan;
+    K2Setup S;
+    PBT_TRY(k2_prepare(ctx, st, norient, d_beam, h_beam_off, d_ext, h_ext_off, d_verts, nverts,
+                       d_face_off, d_face_vi, nfaces, max_face_nv(h_face_off, nfaces), lambda,
+                       fast_diff, S));
+    // orientation chunks sized to a workspace cap
+    const size_t per_orient = (size_t)2 * 8 * nb * sizeof(float);
+    const size_t cap = (size_t)8 << 30;
+    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(norient, (int64_t)(cap / per_orient)));
+    // d_ws: workspace | mu_sum | per-orient red (6) | bs | scale (2) | per-orient params | seg/items
+    const size_t o_ws = 0, o_mu = align_up(o_ws + chunk * per_orient),
+                 o_red = align_up(o_mu + 16 * nb * 8), o_bs = align_up(o_red + 6 * norient * 8),
+                 o_sc = align_up(o_bs + norient * 8), o_pp = align_up(o_sc + 2 * norient * 8),
+                 o_seg = align_up(o_pp + norient * sizeof(pbt_output_params)),
+                 o_it = align_up(o_seg + (2 * chunk + 1) * 8), o_cnt = align_up(o_it + (2 * chunk + 1) * 8),
+                 o_end = align_up(o_cnt + 64);
+    PBT_TRY(ctx->d_ws.ensure(o_end));
+    char *base = ctx->d_ws.as<char>();
+    float *ws = (float *)(base + o_ws);
+    double *mu_sum = (double *)(base + o_mu), *redo = (double *)(base + o_red),
+           *bs = (double *)(base + o_bs), *scale = (double *)(base + o_sc);
+    pbt_output_params *pp = d_params_per ? d_params_per : (pbt_output_params *)(base + o_pp);
+    int64_t *seg_rec = (int64_t *)(base + o_seg), *item_pre = (int64_t *)(base + o_it);
+    unsigned long long *counter = (unsigned long long *)(base + o_cnt);
+    PBT_CUDA_TRY(cudaMemsetAsync(mu_sum, 0, 16 * nb * 8, st));
+    PBT_CUDA_TRY(cudaMemsetAsync(redo, 0, 6 * norient * 8, st));
+    PBT_CUDA_TRY(cudaMemsetAsync(bs, 0, norient * 8, st));
+    PBT_CUDA_TRY(cudaMemsetAsync(scale, 0, 2 * norient * 8, st));
+    const double waveno = 2.0 * kPiRef / lambda;
+    const double *phitab = g.phitab.as<double>(), *sth = g.thtab.as<double>(), *cth = sth + ntheta;
+    const int64_t back_bin = 0 + nphi * g.back_i;
+    const int eb = 256;
+    const unsigned egrid = (unsigned)((nb + eb - 1) / eb);
+    for (int64_t o0 = 0; o0 < norient; o0 += chunk) {
+        const int64_t no = std::min(chunk, norient - o0);
+        PBT_TRY(k2_run_chunk(ctx, st, S, o0, no, lambda, fast_diff, plan, ws, seg_rec, item_pre,
+                             counter));
+        if (scaling) {
+            k2_scatt_be_kernel<<<egrid, eb, 0, st>>>(ws, no, o0, nb, nphi, phitab, waveno,
+                                                     g.wbin.as<double>(), scale);
+            k2_scale_kernel<<<(unsigned)((no + 127) / 128), 128, 0, st>>>(scale, d_params_in, o0, no);
+            ctx->launches += 2;
+        }
+        k2_epi_kernel<<<egrid, eb, 0, st>>>(ws, no, o0, nb, nphi, phitab, cth, waveno,
+                                            g.wbin.as<double>(), back_bin, scaling ? scale : nullptr,
+                                            mu_sum, redo, bs);
+        ctx->launches++;
+        PBT_CUDA_TRY(cudaGetLastError());
+    }
+    k2_final_kernel<<<(unsigned)((norient + 127) / 128), 128, 0, st>>>(redo, bs, d_params_in,
+                                                                       norient, pp);
+    k2_param_avg_kernel<<<1, 32, 0, st>>>(pp, norient, d_params_avg);
+    k2_mu_avg_kernel<<<(unsigned)((16 * nb + 255) / 256), 256, 0, st>>>(
+        mu_sum, 16 * nb, 1.0 / (double)norient, (double)norient, d_mueller_avg);
+    k2_phi_int_kernel<<<(unsigned)((16 * ntheta + 127) / 128), 128, 0, st>>>(
+        d_mueller_avg, g.wphi.as<double>(), nphi, ntheta, d_m1d_avg);
+    ctx->launches += 4;
+    PBT_CUDA_TRY(cudaGetLastError());
+    if (check_errors) PBT_TRY(k2_check_err(ctx, st, S.err));
+    return PBT_OK;
+}
+
+// FP32 diff_main: one orientation, amplitude grids in the reference layout.
+int k2_diff_main_impl(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *d_beam, int64_t nbeam,
+                      const pbt_outbeam *d_ext, int64_t next, const double *d_verts, int64_t nverts,
+                      const int64_t *h_face_off, const int64_t *d_face_off,
+                      const int64_t *d_face_vi, int64_t nfaces, double lambda, int fast_diff,
+                      double *d_afb, double *d_afe) {
+    const GridCache &g = ctx->grid;
+    const int64_t nb = g.nb;
+    K2Plan plan;
+    K2Setup S;
+    const int64_t hbo[2] = {0, nbeam}, heo[2] = {0, next};
+    PBT_TRY(k2_prepare(ctx, st, 1, d_beam, hbo, d_ext, heo, d_verts, nverts, d_face_off, d_face_vi,
+                       nfaces, max_face_nv(h_face_off, nfaces), lambda, fast_diff, S));
+    const size_t o_ws = 0, o_seg = align_up(o_ws + (size_t)2 * 8 * nb * sizeof(float)),
+                 o_it = align_up(o_seg + 3 * 8), o_cnt = align_up(o_it + 3 * 8), o_end = align_up(o_cnt + 64);
+    PBT_TRY(ctx->d_ws.ensure(o_end));
+    char *base = ctx->d_ws.as<char>();
+    float *ws = (float *)(base + o_ws);
+    PBT_TRY(k2_run_chunk(ctx, st, S, 0, 1, lambda, fast_diff, plan, ws, (int64_t *)(base + o_seg),
+                         (int64_t *)(base + o_it), (unsigned long long *)(base + o_cnt)));
+    const double waveno = 2.0 * kPiRef / lambda;
+    k2_ampl_out_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, st>>>(
+        ws, nb, (int64_t)g.phi.size(), g.phitab.as<double>(), g.xyz.as<double>(), waveno, d_afb,
+        d_afe);
+    ctx->launches++;
+    PBT_CUDA_TRY(cudaGetLastError());
+    return k2_check_err(ctx, st, S.err);
+}
+
+}  // namespace pbt

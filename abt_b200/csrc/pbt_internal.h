@@ -1,0 +1,179 @@
+// pbt_internal.h -- shared declarations of the library's host and device code.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pbt_diff.h"
+
+namespace pbt {
+
+// ------------------------------------------------------------------ errors
+void set_error(const char *fmt, ...);
+void clear_error();
+const char *last_error();
+
+#define PBT_CUDA_TRY(call)                                                                  \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            ::pbt::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),        \
+                             __FILE__, __LINE__);                                           \
+            return e_ == cudaErrorMemoryAllocation ? PBT_ENOMEM : PBT_ECUDA;                \
+        }                                                                                   \
+    } while (0)
+
+#define PBT_TRY(call)                     \
+    do {                                  \
+        int rc_ = (call);                 \
+        if (rc_ != PBT_OK) return rc_;    \
+    } while (0)
+
+// ------------------------------------------------------------ device memory
+// Grow-only device buffer owned by a context.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes);
+    void release();
+    template <class T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+// Grow-only pinned host staging buffer.
+struct HostBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes);
+    void release();
+    template <class T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+// ------------------------------------------- reference-exact FP64 records
+// One outgoing facet, prepared for the FP64 kernel (all values formed in the
+// reference's operation order).  272 bytes.
+struct K1Facet {
+    double com[3];
+    double R[9];      // matmul(rot2, rot), row-major
+    double prop2[3];
+    double inc2[3];
+    double kinc[2];   // prop2(1:2) * waveno  (src/diff_mod.f90:336)
+    double ampl[8];   // amplitude after the anti-parallel flip: (1,1),(2,1),(1,2),(2,2) re/im
+    double prop0[3];  // lab-frame propagation (field-of-view test)
+    double cos_fov;
+    int64_t edge_off;
+    int64_t nv;
+};
+static_assert(sizeof(K1Facet) == 272, "K1Facet layout");
+
+// One aperture edge after the slope clamps of src/diff_mod.f90:379-393.
+struct K1Edge {
+    double xj, yj, mj, nj, dx, dy;
+};
+
+// Far-field bin grid cached per (theta, phi) list.
+struct GridCache {
+    std::vector<double> theta, phi;  // radians, as given
+    int64_t nb = 0;
+    int64_t theta_i = -1;            // first theta above 1 degree (0-based), -1 if none
+    int64_t back_i = 0;              // minloc(|theta - 2 pi|)
+    DevBuf xyz;                      // xfar | yfar | zfar  (nb each), libm values
+    DevBuf phitab;                   // cos(phi) | sin(phi)  (nphi each), libm values
+    DevBuf thtab;                    // sin(theta) | cos(theta) (ntheta each), libm values
+    DevBuf wbin;                     // simpne weights w_phi(i) * w_theta(j) * sin(theta_j)  (nb)
+    DevBuf wphi;                     // simpne weights over phi (nphi)
+    bool valid = false;
+};
+
+// Device running totals of summation (src/outputs_mod.f90:407-471).
+struct DevTotals {
+    DevBuf mu, m1, par;  // (nphi,ntheta,16) | (ntheta,16) | 18 params
+    int64_t ntheta = 0, nphi = 0, count = 0;
+    void release() {
+        mu.release();
+        m1.release();
+        par.release();
+    }
+};
+
+}  // namespace pbt
+
+struct pbt_ctx {
+    int device = 0;
+    std::mutex mu;
+    cudaStream_t stream = nullptr;   // internal stream of the host-pointer entry points
+    pbt::GridCache grid;
+    // scratch (grow-only)
+    pbt::DevBuf d_fac, d_edge, d_out, d_mu, d_m1, d_misc, d_in, d_rec, d_ws, d_scan, d_items;
+    pbt::HostBuf h_stage;
+    cudaEvent_t stage_ev = nullptr;  // last copy out of h_stage (wait before reuse)
+    bool stage_pending = false;
+    pbt::DevTotals tot;    // user-visible totals (pbt_summation_c / pbt_finalise_c accumulate)
+    pbt::DevTotals btot;   // totals of the FP64 batch path
+    int64_t launches = 0;            // kernel launches of the last compute call
+    int sm_count = 0;
+    // CUDA-event timing of the far-field kernels
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;  // start/stop pairs
+    size_t ev_used = 0;
+};
+
+namespace pbt {
+
+// ----------------------------------------------------------- host helpers
+int validate_geometry(const double *verts, int64_t nverts, const int64_t *face_off,
+                      const int64_t *face_vi, int64_t nfaces);
+int validate_angles(const double *theta, int64_t ntheta, const double *phi, int64_t nphi);
+int grid_prepare(pbt_ctx *ctx, const double *theta, int64_t ntheta, const double *phi,
+                 int64_t nphi, cudaStream_t st);
+
+// Reference-exact facet set-up on the host (libm).  Appends to fac/edges.
+int k1_build_facets(const pbt_outbeam *obs, int64_t n, double fov_override, const double *verts,
+                    int64_t nverts, const int64_t *face_off, const int64_t *face_vi,
+                    int64_t nfaces, double lambda, std::vector<K1Facet> &fac,
+                    std::vector<K1Edge> &edges);
+
+// FP64 far-field sum of nf facets into a complex (nphi,ntheta,2,2) grid (overwritten).
+int k1_launch(pbt_ctx *ctx, cudaStream_t st, const K1Facet *d_fac, int64_t nf,
+              const K1Edge *d_edges, double lambda, int fast_diff, double *d_grid);
+
+// Reference-exact finalise on device grids.  Writes mueller (nb*16),
+// mueller_1d (ntheta*16) and params (18 doubles) to device memory; adds to the
+// context totals when accumulate.
+int k3_finalise(pbt_ctx *ctx, cudaStream_t st, const double *d_afb, const double *d_afe,
+                double lambda, int scaling, const pbt_output_params *h_params_in,
+                double *d_mueller, double *d_m1d, double *d_params, DevTotals *acc);
+int totals_ensure(DevTotals &T, int64_t ntheta, int64_t nphi, cudaStream_t st);
+int totals_reset(DevTotals &T, cudaStream_t st);
+int totals_add_device(pbt_ctx *ctx, DevTotals &T, cudaStream_t st, const double *d_mueller,
+                      const double *d_m1d, const double *d_params);
+
+// Batched FP32 path.  h_beam_off / h_ext_off / h_face_off are host arrays,
+// every other pointer is device memory.
+int k2_batch_impl(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam *d_beam,
+                  const int64_t *h_beam_off, const pbt_outbeam *d_ext, const int64_t *h_ext_off,
+                  const double *d_verts, int64_t nverts, const int64_t *h_face_off,
+                  const int64_t *d_face_off, const int64_t *d_face_vi, int64_t nfaces,
+                  double lambda, int fast_diff, int scaling, const pbt_output_params *d_params_in,
+                  double *d_mueller_avg, double *d_m1d_avg, pbt_output_params *d_params_avg,
+                  pbt_output_params *d_params_per, int check_errors);
+
+// FP32 single-orientation amplitude grids (the fast diff_main).
+int k2_diff_main_impl(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *d_beam, int64_t nbeam,
+                      const pbt_outbeam *d_ext, int64_t next, const double *d_verts, int64_t nverts,
+                      const int64_t *h_face_off, const int64_t *d_face_off,
+                      const int64_t *d_face_vi, int64_t nfaces, double lambda, int fast_diff,
+                      double *d_afb, double *d_afe);
+int k2_check_err(pbt_ctx *ctx, cudaStream_t st, const int *d_err);
+int totals_divide_device(pbt_ctx *ctx, DevTotals &T, cudaStream_t st, int64_t num_orients,
+                         double *d_mu, double *d_m1, double *d_p);
+int validate_outbeams(const pbt_outbeam *obs, int64_t n, int64_t nfaces, const char *what);
+// Bracket a far-field kernel launch with timing events (no-op unless enabled).
+void timing_begin(pbt_ctx *ctx, cudaStream_t st);
+void timing_end(pbt_ctx *ctx, cudaStream_t st);
+
+}  // namespace pbt

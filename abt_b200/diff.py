@@ -1,0 +1,256 @@
+"""Host-side mirror of PBT's far-field interface over the C ABI.
+
+Names, argument meanings and layouts follow the reference's Fortran routines
+(src/diff_mod.f90 diff_main / diffraction / make_far_field_bins,
+src/outputs_mod.f90 finalise / summation / divide_by_num_orientations,
+src/input_mod.f90 make_angles), so that tests read like the reference's own
+call sites.  Every compute call runs on the GPU through libpbt_b200.so.
+
+Arrays:
+  geometry           dict(verts=(nverts,3) float64, face_off=(nfaces+1,) int64
+                     0-based CSR offsets, face_vi=1-based vertex indices)
+  outbeams           numpy arrays of OUTBEAM_DTYPE
+  amplitude grids    complex128 (nphi, ntheta, 2, 2), Fortran order
+  Mueller grids      float64 (nphi, ntheta, 16) / (ntheta, 16), Fortran order
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import OUTBEAM_DTYPE, PARAMS_DTYPE, PARAM_NAMES, PBT_PREC_FP32, PBT_PREC_FP64, check, ptr
+
+# src/misc_submod.f90:12 -- a default-real literal widened to real(8)
+PI_REF = float(np.float32(3.14159265358979))
+
+_PREC = {"fp64": PBT_PREC_FP64, "fp32": PBT_PREC_FP32}
+
+
+def make_angles(vals_deg, splits_deg):
+    """make_angles (src/input_mod.f90:114-196) then the degree-to-radian step
+    theta_vals*pi/180d0 (src/input_mod.f90:742): a piecewise grid given as
+    values v1 s1 v2 s2 ... vn; interior segment ends are dropped."""
+    v = [float(x) for x in vals_deg]
+    s = [float(x) for x in splits_deg]
+    if len(v) < 2 or len(s) < len(v) - 1:
+        raise ValueError("need n values and n-1 splits")
+    out = []
+    n = len(v)
+    for i in range(n - 1):
+        q = (v[i + 1] - v[i]) / s[i]
+        jmax = int(np.floor(abs(q) + 0.5)) * (1 if q >= 0 else -1)
+        fr = np.fmod(q, 1.0)
+        if float(np.float32(1e-3)) < fr < float(np.float32(1.0) - np.float32(1e-3)):
+            raise ValueError("bad angle choice on segment %d: %g is not close to an integer"
+                             % (i + 1, q))
+        for j in range(jmax + 1):
+            if i != n - 2 and j == jmax:
+                continue
+            out.append(v[i] + j * s[i])
+    a = np.array(out, dtype=np.float64)
+    return a * PI_REF / 180.0
+
+
+def make_geometry(verts, faces):
+    """Geometry dict from (nverts,3) vertices and a list of 1-based vertex index lists."""
+    verts = np.asarray(verts, dtype=np.float64)
+    off = np.zeros(len(faces) + 1, dtype=np.int64)
+    off[1:] = np.cumsum([len(f) for f in faces])
+    vi = np.concatenate([np.asarray(f, dtype=np.int64) for f in faces])
+    return dict(verts=verts, face_off=off, face_vi=vi)
+
+
+def params(abs=0.0, geo_cross_sec=1.0, beam_energy_out=1.0, ext_energy_out=1.0):
+    """The inputs of finalise carried in output_parameters_type."""
+    p = np.zeros((), dtype=PARAMS_DTYPE)
+    p["abs"] = abs
+    p["geo_cross_sec"] = geo_cross_sec
+    p["beam_energy_out"] = beam_energy_out
+    p["ext_energy_out"] = ext_energy_out
+    return p
+
+
+def _geo(geometry):
+    v = np.asfortranarray(geometry["verts"], dtype=np.float64)
+    fo = np.ascontiguousarray(geometry["face_off"], dtype=np.int64)
+    fv = np.ascontiguousarray(geometry["face_vi"], dtype=np.int64)
+    return v, fo, fv
+
+
+def _ob(a):
+    return np.ascontiguousarray(np.atleast_1d(a) if a is not None else np.zeros(0, OUTBEAM_DTYPE),
+                                dtype=OUTBEAM_DTYPE)
+
+
+class Context:
+    """A library context on one CUDA device (pbt_ctx_create / pbt_ctx_destroy)."""
+
+    def __init__(self, device=0):
+        L = _lib.lib()
+        h = ctypes.c_void_p()
+        check(L.pbt_ctx_create(int(device), ctypes.byref(h)))
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            _lib.lib().pbt_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def last_launch_count(self):
+        return int(_lib.lib().pbt_last_launch_count(self._h))
+
+    def set_kernel_timing(self, enable=True):
+        check(_lib.lib().pbt_set_kernel_timing(self._h, int(bool(enable))))
+
+    def kernel_time_ms(self):
+        """(total ms, launches) of the far-field kernels timed since the last call."""
+        t = ctypes.c_double()
+        n = ctypes.c_int64()
+        check(_lib.lib().pbt_kernel_time_ms(self._h, ctypes.byref(t), ctypes.byref(n)))
+        return t.value, n.value
+
+    # ------------------------------------------------------------ diff_mod
+    def diff_main(self, beam, ext, geometry, theta, phi, lam, is_fast_diff=False,
+                  precision="fp64"):
+        """diff_main (src/diff_mod.f90:674-825) -> (ampl_far_beam, ampl_far_ext_diff)."""
+        beam, ext = _ob(beam), _ob(ext)
+        v, fo, fv = _geo(geometry)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        shape = (len(phi), len(theta), 2, 2)
+        afb = np.zeros(shape, dtype=np.complex128, order="F")
+        afe = np.zeros(shape, dtype=np.complex128, order="F")
+        check(_lib.lib().pbt_diff_main_c(self._h, ptr(beam), len(beam), ptr(ext), len(ext),
+                                         ptr(v), v.shape[0], ptr(fo), ptr(fv), len(fo) - 1,
+                                         ptr(theta), len(theta), ptr(phi), len(phi), float(lam),
+                                         int(bool(is_fast_diff)), _PREC[precision],
+                                         afb.ctypes.data, afe.ctypes.data))
+        return afb, afe
+
+    def diffraction(self, outbeam, geometry, theta, phi, lam, is_fast_diff=False):
+        """diffraction (src/diff_mod.f90:446-672) for one outbeam -> amplC."""
+        ob = _ob(outbeam)[:1]
+        v, fo, fv = _geo(geometry)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        out = np.zeros((len(phi), len(theta), 2, 2), dtype=np.complex128, order="F")
+        check(_lib.lib().pbt_diffraction_c(self._h, ptr(ob), ptr(v), v.shape[0], ptr(fo), ptr(fv),
+                                           len(fo) - 1, ptr(theta), len(theta), ptr(phi),
+                                           len(phi), float(lam), int(bool(is_fast_diff)),
+                                           out.ctypes.data))
+        return out
+
+    # --------------------------------------------------------- outputs_mod
+    def finalise(self, ampl_far_beam, ampl_far_ext_diff, theta, phi, lam, params_in,
+                 scaling=False, accumulate=False):
+        """finalise (src/outputs_mod.f90:63-278) -> (mueller, mueller_1d, params)."""
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        afb = np.asfortranarray(ampl_far_beam, dtype=np.complex128)
+        afe = np.asfortranarray(ampl_far_ext_diff, dtype=np.complex128)
+        p = np.array(params_in, dtype=PARAMS_DTYPE).copy()
+        mu = np.zeros((len(phi), len(theta), 16), order="F")
+        mu1 = np.zeros((len(theta), 16), order="F")
+        check(_lib.lib().pbt_finalise_c(self._h, afb.ctypes.data, afe.ctypes.data, ptr(theta),
+                                        len(theta), ptr(phi), len(phi), float(lam),
+                                        int(bool(scaling)), p.ctypes.data, mu.ctypes.data,
+                                        mu1.ctypes.data, int(bool(accumulate))))
+        return mu, mu1, p
+
+    def summation(self, mueller, mueller_1d, params_in):
+        """summation (src/outputs_mod.f90:407-471) into the context's device totals."""
+        mu = np.asfortranarray(mueller, dtype=np.float64)
+        mu1 = np.asfortranarray(mueller_1d, dtype=np.float64)
+        p = np.array(params_in, dtype=PARAMS_DTYPE)
+        check(_lib.lib().pbt_summation_c(self._h, mu.ctypes.data, mu1.ctypes.data, p.ctypes.data,
+                                         mu.shape[1], mu.shape[0]))
+
+    def divide_by_num_orientations(self, num_orients, ntheta, nphi):
+        """divide_by_num_orientations (src/outputs_mod.f90:13-43) of the device totals."""
+        mu = np.zeros((nphi, ntheta, 16), order="F")
+        mu1 = np.zeros((ntheta, 16), order="F")
+        p = np.zeros((), dtype=PARAMS_DTYPE)
+        check(_lib.lib().pbt_divide_by_num_orientations_c(self._h, int(num_orients),
+                                                          mu.ctypes.data, mu1.ctypes.data,
+                                                          p.ctypes.data))
+        return mu, mu1, p
+
+    def totals_reset(self):
+        check(_lib.lib().pbt_totals_reset_c(self._h))
+
+    # ------------------------------------------------------------ batched
+    def diff_batch(self, beams, exts, verts_per_orient, geometry, theta, phi, lam,
+                   params_in, is_fast_diff=False, scaling=False, precision="fp32"):
+        """Orientation average of norient orientations in one call.
+
+        beams / exts: lists (one per orientation) of outbeam arrays.
+        verts_per_orient: list of (nverts,3) rotated vertex arrays (topology from geometry).
+        params_in: PARAMS_DTYPE array of length norient.
+        Returns (mueller_avg, mueller_1d_avg, params_avg, params_per_orient)."""
+        norient = len(beams)
+        # a single orientation is passed without a copy (keeps pinned buffers pinned)
+        beam = _ob(beams[0] if norient == 1 else np.concatenate(beams))
+        ext = _ob(exts[0] if norient == 1 else np.concatenate(exts))
+        boff = np.zeros(norient + 1, dtype=np.int64)
+        boff[1:] = np.cumsum([len(b) for b in beams])
+        eoff = np.zeros(norient + 1, dtype=np.int64)
+        eoff[1:] = np.cumsum([len(e) for e in exts])
+        _, fo, fv = _geo(geometry)
+        nverts = np.asarray(verts_per_orient[0]).shape[0]
+        flat = [np.asfortranarray(v, dtype=np.float64).ravel(order="F") for v in verts_per_orient]
+        V = flat[0] if norient == 1 else np.concatenate(flat)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        pin = np.ascontiguousarray(params_in, dtype=PARAMS_DTYPE)
+        mu = np.zeros((len(phi), len(theta), 16), order="F")
+        mu1 = np.zeros((len(theta), 16), order="F")
+        pav = np.zeros((), dtype=PARAMS_DTYPE)
+        pper = np.zeros(norient, dtype=PARAMS_DTYPE)
+        check(_lib.lib().pbt_diff_batch_c(self._h, norient, ptr(beam), ptr(boff), ptr(ext),
+                                          ptr(eoff), ptr(V), nverts, ptr(fo), ptr(fv), len(fo) - 1,
+                                          ptr(theta), len(theta), ptr(phi), len(phi), float(lam),
+                                          int(bool(is_fast_diff)), int(bool(scaling)),
+                                          _PREC[precision], ptr(pin), mu.ctypes.data,
+                                          mu1.ctypes.data, pav.ctypes.data, pper.ctypes.data))
+        return mu, mu1, pav, pper
+
+
+def params_dict(p):
+    return {n: float(p[n]) for n in PARAM_NAMES}
+
+
+def diff_batch_dev(ctx, stream, norient, d_beam, beam_off, d_ext, ext_off, d_verts, nverts,
+                   face_off, d_face_vi, theta, phi, lam, d_params_in, d_mueller_avg, d_m1d_avg,
+                   d_params_avg, d_params_per=None, is_fast_diff=False, scaling=False):
+    """pbt_diff_batch_dev_c: the FP32 batched average on device-resident arrays.
+    d_* are device pointers (ints) or torch CUDA tensors; beam_off, ext_off,
+    face_off, theta and phi are host numpy arrays.  stream: a cudaStream_t
+    handle (int), e.g. torch.cuda.current_stream().cuda_stream."""
+    boff = np.ascontiguousarray(beam_off, dtype=np.int64)
+    eoff = np.ascontiguousarray(ext_off, dtype=np.int64)
+    fo = np.ascontiguousarray(face_off, dtype=np.int64)
+    theta = np.ascontiguousarray(theta, dtype=np.float64)
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    check(_lib.lib().pbt_diff_batch_dev_c(
+        ctx.handle, stream, int(norient), ptr(d_beam), ptr(boff), ptr(d_ext), ptr(eoff),
+        ptr(d_verts), int(nverts), ptr(fo), ptr(d_face_vi), len(fo) - 1, ptr(theta), len(theta),
+        ptr(phi), len(phi), float(lam), int(bool(is_fast_diff)), int(bool(scaling)),
+        PBT_PREC_FP32, ptr(d_params_in), ptr(d_mueller_avg), ptr(d_m1d_avg), ptr(d_params_avg),
+        ptr(d_params_per)))

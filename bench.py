@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark of the far-field diffraction hot path on B200.
+
+Workload (the precision-study configuration): a synthetic beam list of
+200,000 outgoing triangular facets in 2,000 beams (vertices in a 100 um cube,
+edges 0.3-1.5 um, log-normal amplitudes), lambda = 0.532 um, far field
+721 theta x 360 phi = 259,560 bins: 5.19e10 facet x bin evaluations per step.
+
+One step = the batched FP32 far-field sum with FP64 phase plus its FP64
+epilogue (Mueller matrix, phi/theta integrals, cross sections), inputs
+resident in HBM.  Metric: facet x bin evaluations per second (whole job).
+
+Also reported: the same metric end to end through the host C ABI
+(pbt_diff_batch_c, pinned host buffers, copies inside the timed region), the
+reference-exact FP64 drop-in's rate, the FP32-vs-FP64 Mueller error on the
+full workload, the roofline of the dominant kernel and a CPU baseline (the
+C FP64 restatement of the reference, all host cores, bounded sample).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "facet·bin evals/s & orientations/s: batched FP32 vs plain FP64 GPU @1e-4 err"
+UNIT = "facet·bin/s"
+LAM = 0.532
+# algorithmic work per triangle facet x bin (fixed counting convention)
+W_FP32 = 170.0   # FP32 flops (FMA = 2)
+W_SFU = 20.0     # special-function ops
+FP32_PER_SM_CLK = 128 * 2   # FP32 lanes x 2 flops
+SFU_PER_SM_CLK = 16
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--beams", type=int, default=2000)
+    ap.add_argument("--facets-per-beam", type=int, default=100)
+    ap.add_argument("--fp64-facets", type=int, default=4000,
+                    help="facets of the FP64 drop-in rate sample (0 = skip)")
+    ap.add_argument("--no-error-check", action="store_true",
+                    help="skip the full-workload FP64 run used for the FP32 error")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu_index),
+                                       "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def workload(args):
+    from abt_b200 import workloads as W
+    geo, beam, ext = W.synthetic_beam_list(n_beams=args.beams, facets_per_beam=args.facets_per_beam,
+                                           seed=2024)
+    th, ph = W.grid_precision_study()
+    return geo, beam, ext, th, ph
+
+
+def cpu_baseline(geo, beam, th, ph, seconds, nthreads):
+    """The oracle (C FP64 restatement of diff_mod, the reference's OpenMP loop
+    shape) on a bounded sample of the workload: the first n facets over the
+    full far-field grid, n sized to about `seconds` of work."""
+    from oracle import oracle as O
+    nb = len(th) * len(ph)
+    ext = np.zeros(0, dtype=O.OUTBEAM_DTYPE)
+    n = max(nthreads, 2)
+    t0 = time.perf_counter()
+    O.diff_main(th, ph, LAM, geo, beam[:n], ext, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    n2 = int(min(len(beam), max(n, n * seconds / max(dt, 1e-3))))
+    n2 = max(nthreads, (n2 // nthreads) * nthreads)
+    t0 = time.perf_counter()
+    O.diff_main(th, ph, LAM, geo, beam[:n2], ext, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return {"value": n2 * nb / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": "%d facets x %d bins (first facets of the workload), %.1f s" % (n2, nb, dt)}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    geo, beam, ext, th, ph = workload(args)
+    nthreads = os.cpu_count() or 1
+    nb = len(th) * len(ph)
+    per_step = max(1.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_baseline(geo, beam, th, ph, 1.0, nthreads)
+    vals = []
+    last = None
+    for _ in range(args.steps):
+        last = cpu_baseline(geo, beam, th, ph, per_step, nthreads)
+        vals.append(last["value"])
+    value = statistics.mean(vals)
+    ms = len(beam) * nb / value * 1e3
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "precision-study beam list, 200000 facets x 721x360 bins",
+                       "facets": int(len(beam)), "bins": nb},
+            "cpu_baseline": dict(last, value=value),
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local, dist = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import torch
+
+    import abt_b200
+    from abt_b200.diff import diff_batch_dev
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    geo, beam, ext, th, ph = workload(args)
+    nf = len(beam)
+    nb = len(th) * len(ph)
+    nverts = geo["verts"].shape[0]
+    work = float(nf) * nb  # facet x bin evaluations per step (one orientation)
+
+    ctx = abt_b200.Context(local)
+    # device-resident inputs
+    d_beam = torch.from_numpy(beam.view(np.uint8).copy()).to(dev)
+    d_ext = torch.empty(128, dtype=torch.uint8, device=dev)
+    d_verts = torch.from_numpy(np.asfortranarray(geo["verts"]).ravel(order="F").copy()).to(dev)
+    d_fvi = torch.from_numpy(geo["face_vi"].copy()).to(dev)
+    pin = np.zeros(1, dtype=abt_b200.PARAMS_DTYPE)
+    pin["geo_cross_sec"] = 1.0
+    pin["beam_energy_out"] = 1.0
+    pin["ext_energy_out"] = 1.0
+    d_pin = torch.from_numpy(pin.view(np.uint8).copy()).to(dev)
+    d_mu = torch.empty(16 * nb, dtype=torch.float64, device=dev)
+    d_m1 = torch.empty(16 * len(th), dtype=torch.float64, device=dev)
+    d_pav = torch.empty(18, dtype=torch.float64, device=dev)
+    d_pper = torch.empty(18, dtype=torch.float64, device=dev)
+    boff = np.array([0, nf], dtype=np.int64)
+    eoff = np.array([0, 0], dtype=np.int64)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        diff_batch_dev(ctx, stream.cuda_stream, 1, d_beam, boff, d_ext, eoff, d_verts, nverts,
+                       geo["face_off"], d_fvi, th, ph, LAM, d_pin, d_mu, d_m1, d_pav, d_pper)
+
+    for _ in range(max(3, args.warmup)):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ctx.set_kernel_timing(True)
+    ctx.kernel_time_ms()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches = 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        flush.zero_()
+        step()
+        launches += ctx.last_launch_count()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms_total = e0.elapsed_time(e1)
+    kern_ms, kern_n = ctx.kernel_time_ms()
+    ctx.set_kernel_timing(False)
+    if dist is not None:
+        t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = world * work / (ms_step / 1e3)
+
+    extra = {}
+    # end to end through the host C ABI with pinned host buffers
+    pinned_beam = torch.from_numpy(beam.view(np.uint8).copy()).pin_memory()
+    pb = pinned_beam.numpy().view(abt_b200.OUTBEAM_DTYPE)
+    pverts = torch.from_numpy(np.asfortranarray(geo["verts"]).copy()).pin_memory().numpy()
+    pverts = np.asfortranarray(pverts.reshape(geo["verts"].shape))
+    geo_p = dict(geo, verts=pverts)
+    out = ctx.diff_batch([pb], [np.zeros(0, abt_b200.OUTBEAM_DTYPE)], [pverts], geo_p, th, ph, LAM,
+                         pin, precision="fp32")
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        out = ctx.diff_batch([pb], [np.zeros(0, abt_b200.OUTBEAM_DTYPE)], [pverts], geo_p, th, ph,
+                             LAM, pin, precision="fp32")
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    h2d = beam.nbytes + geo["verts"].nbytes + geo["face_off"].nbytes + geo["face_vi"].nbytes + pin.nbytes
+    d2h = 16 * nb * 8 + 16 * len(th) * 8 + 2 * pin.nbytes
+    e2e = {"value": world * work / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3,
+           "api": "pbt_diff_batch_c (host pointers, pinned)"}
+
+    # reference-exact FP64 drop-in rate on a facet sample
+    if args.fp64_facets > 0:
+        sub = beam[:args.fp64_facets]
+        ctx.diff_main(sub[:64], None, geo, th, ph, LAM, precision="fp64")
+        ctx.set_kernel_timing(True)
+        ctx.kernel_time_ms()
+        t0 = time.perf_counter()
+        ctx.diff_main(sub, None, geo, th, ph, LAM, precision="fp64")
+        wall = time.perf_counter() - t0
+        k64_ms, _ = ctx.kernel_time_ms()
+        ctx.set_kernel_timing(False)
+        r64 = len(sub) * nb / (k64_ms / 1e3)
+        extra["fp64_dropin"] = {"value": r64, "unit": UNIT, "facets": int(len(sub)),
+                                "kernel_ms": k64_ms, "call_ms": wall * 1e3,
+                                "e2e_value": len(sub) * nb / wall}
+        extra["fp32_vs_fp64_kernel_speedup"] = (work / (kern_ms / max(kern_n, 1) / 1e3)) / r64
+
+    # FP32 error against the FP64 drop-in on the full workload
+    if not args.no_error_check:
+        from tests.helpers import mueller_rel_err
+        f64 = ctx.diff_batch([beam], [np.zeros(0, abt_b200.OUTBEAM_DTYPE)], [geo["verts"]], geo,
+                             th, ph, LAM, pin, precision="fp64")
+        mu32 = d_mu.cpu().numpy().reshape(16, len(th), len(ph)).transpose(2, 1, 0)
+        extra["max_rel_mueller_err_vs_fp64"] = mueller_rel_err(mu32, f64[0], 1e-6)
+        extra["max_rel_param_err_vs_fp64"] = max(
+            abs(float(out[2][n]) - float(f64[2][n])) / abs(float(f64[2][n]))
+            for n in ("scatt", "asymmetry", "ext"))
+
+    # roofline of the dominant kernel (k2_main_kernel)
+    kms = kern_ms / max(kern_n, 1)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = clk.get("sm_mhz") or 1965.0
+    peak_fp32 = sms * FP32_PER_SM_CLK * mhz * 1e6
+    ach = W_FP32 * work / (kms / 1e3)
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "k2_main_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch_full")
+        except Exception:
+            traffic = None
+    roof = {"bound": "fp32", "achieved": ach / 1e12, "peak": peak_fp32 / 1e12, "unit": "TFLOP/s",
+            "frac": ach / peak_fp32, "traffic": traffic,
+            "kernel": "k2_main_kernel", "kernel_ms": kms,
+            "peak_basis": "%d SMs x 128 FP32 lanes x 2 flop x %.0f MHz (median sampled SM clock); "
+                          "MEASURED_PEAKS.json has no FP32/SFU figure" % (sms, mhz),
+            "sfu_frac": (W_SFU * work / (kms / 1e3)) / (sms * SFU_PER_SM_CLK * mhz * 1e6),
+            "work_per_facet_bin": {"fp32_flops": W_FP32, "sfu_ops": W_SFU}}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(geo, beam, th, ph, args.cpu_seconds, os.cpu_count() or 1)
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "precision-study beam list: 200000 facets (2000 beams), "
+                                   "721 theta x 360 phi, lambda 0.532 um, FP32 with FP64 phase",
+                       "facets": nf, "bins": nb, "orientations_per_step": 1,
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "256 MB buffer written before every step, inside the timed region"},
+            "orientations_per_s": world * 1e3 / ms_step,
+            "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof,
+            "cpu_baseline": cpu}
+    line.update(extra)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,190 @@
+/*
+ * pbt_diff.h -- C ABI of the B200 far-field diffraction library (libpbt_b200.so).
+ *
+ * Drop-in replacement for PBT's far-field stage: diff_mod (diffraction,
+ * diff_main) and the outputs_mod epilogue (finalise, summation,
+ * divide_by_num_orientations).  Every entry point is extern "C", takes plain
+ * pointers and sizes, and returns an int status (PBT_OK = 0).  A non-zero
+ * status leaves a message for pbt_last_error_string() in the calling thread.
+ *
+ * Array layouts are the reference's Fortran layouts, so a Fortran caller can
+ * pass its arrays unchanged through iso_c_binding:
+ *   amplitude grid  complex(8) ampl(nphi, ntheta, 2, 2), column-major,
+ *                   element (i,j,a,b) at 2*((i-1)+nphi*((j-1)+ntheta*((a-1)+2*(b-1)))) doubles
+ *   Mueller grid    real(8) mueller(nphi, ntheta, 16), column-major
+ *   1-D Mueller     real(8) mueller_1d(ntheta, 16), column-major
+ *   vertices        real(8) v(nverts, 3), column-major (geometry%v)
+ *   faces           CSR: face_off(nfaces+1) 0-based offsets into face_vi,
+ *                   face_vi 1-based vertex indices (geometry%f(:)%vi)
+ *   angles          theta_vals / phi_vals in radians (job_params%theta_vals, %phi_vals)
+ *
+ * Citations are path:line inside the reference project (hballington12/abt).
+ */
+#ifndef PBT_DIFF_H
+#define PBT_DIFF_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define PBT_OK 0
+#define PBT_EINVAL 1   /* bad argument: sizes, indices, null pointers, non-finite input */
+#define PBT_ENOMEM 2   /* device or pinned-host allocation failed */
+#define PBT_ECUDA 3    /* a CUDA call failed */
+#define PBT_ETIMEOUT 4 /* a bounded device-side wait ran out; results not written */
+#define PBT_ENODEV 5   /* no usable sm_100 device */
+#define PBT_ESTATE 6   /* call out of order (e.g. totals of an empty accumulation) */
+
+/* arithmetic of the far-field sum */
+#define PBT_PREC_FP64 0 /* reference-exact FP64 (the plain drop-in) */
+#define PBT_PREC_FP32 1 /* FP32 with the far-field phase formed and range-reduced in FP64 */
+
+/* One outgoing facet: the fields of outbeamtype (src/types_mod.f90:8-17) that
+ * diffraction reads (src/diff_mod.f90:515-531).  128 bytes. */
+typedef struct pbt_outbeam {
+    double ampl[8];     /* ampl(1:2,1:2) complex(8) column-major: (1,1),(2,1),(1,2),(2,2), re/im */
+    double vk7[3];      /* perpendicular e-field direction */
+    double prop_out[3]; /* outgoing propagation direction */
+    double fov;         /* field of view (rad), used when is_fast_diff */
+    int64_t fi;         /* 1-based face index into the face CSR */
+} pbt_outbeam;
+
+/* output_parameters_type (src/types_mod.f90:32-53), same component order.
+ * Inputs to finalise: abs, geo_cross_sec, beam_energy_out, ext_energy_out. */
+typedef struct pbt_output_params {
+    double abs, scatt, ext, albedo, asymmetry, abs_eff, scatt_eff, ext_eff, geo_cross_sec,
+        back_scatt, beam_energy_out, ext_energy_out, scatt_beam, scatt_ext_diff, asymmetry_beam,
+        asymmetry_ext_diff, scatt_eff_beam, scatt_eff_ext_diff;
+} pbt_output_params;
+
+typedef struct pbt_ctx pbt_ctx;
+
+/* ---------------------------------------------------------------- lifecycle */
+
+/* Create a context bound to CUDA device `device`.  The context owns device
+ * buffers reused across calls; it is safe to share between host threads
+ * (calls are serialised on an internal mutex). */
+int pbt_ctx_create(int device, pbt_ctx **out);
+int pbt_ctx_destroy(pbt_ctx *ctx);
+/* Message of the last failed call made by this thread ("" if none). */
+const char *pbt_last_error_string(void);
+/* ABI version: major*10000 + minor*100 + patch. */
+int pbt_version(void);
+
+/* --------------------------------------------------------------- diff_mod */
+
+/* diff_main replacement, src/diff_mod.f90:674-825.
+ * Sums every beam outbeam into ampl_far_beam and every external-diffraction
+ * outbeam (with fov forced to pi/2, src/diff_mod.f90:797) into
+ * ampl_far_ext_diff.  precision = PBT_PREC_FP64 reproduces the reference's
+ * arithmetic (facet order 1..n, no FMA); PBT_PREC_FP32 is the fast form.
+ * Both output grids are overwritten. */
+int pbt_diff_main_c(pbt_ctx *ctx, const pbt_outbeam *beam, int64_t nbeam,
+                    const pbt_outbeam *ext, int64_t next, const double *verts, int64_t nverts,
+                    const int64_t *face_off, const int64_t *face_vi, int64_t nfaces,
+                    const double *theta, int64_t ntheta, const double *phi, int64_t nphi,
+                    double lambda, int32_t is_fast_diff, int32_t precision,
+                    double *ampl_far_beam, double *ampl_far_ext_diff);
+
+/* diffraction replacement, src/diff_mod.f90:446-672: the far-field amplitude
+ * of one outbeam, as used by the -memory path (src/beam_loop_mod.f90:44,71).
+ * amplC is overwritten (zero outside the field of view when is_fast_diff).
+ * FP64, reference-exact. */
+int pbt_diffraction_c(pbt_ctx *ctx, const pbt_outbeam *outbeam, const double *verts,
+                      int64_t nverts, const int64_t *face_off, const int64_t *face_vi,
+                      int64_t nfaces, const double *theta, int64_t ntheta, const double *phi,
+                      int64_t nphi, double lambda, int32_t is_fast_diff, double *amplC);
+
+/* ------------------------------------------------------------ outputs_mod */
+
+/* finalise replacement, src/outputs_mod.f90:63-278 (FP64, reference order).
+ * params: in abs, geo_cross_sec, beam_energy_out, ext_energy_out; out all.
+ * The amplitude grids are read only (the reference scales its copies in
+ * place; the library does not).  When accumulate != 0 the orientation's
+ * mueller, mueller_1d and params are also added to the context's device
+ * totals (summation, src/outputs_mod.f90:407-471).  mueller / mueller_1d
+ * may be NULL when only the totals are wanted. */
+int pbt_finalise_c(pbt_ctx *ctx, const double *ampl_far_beam, const double *ampl_far_ext_diff,
+                   const double *theta, int64_t ntheta, const double *phi, int64_t nphi,
+                   double lambda, int32_t scaling, pbt_output_params *params, double *mueller,
+                   double *mueller_1d, int32_t accumulate);
+
+/* summation replacement, src/outputs_mod.f90:407-471: adds one orientation's
+ * results (host arrays) to the context's device totals. */
+int pbt_summation_c(pbt_ctx *ctx, const double *mueller, const double *mueller_1d,
+                    const pbt_output_params *params, int64_t ntheta, int64_t nphi);
+
+/* divide_by_num_orientations, src/outputs_mod.f90:13-43, applied to copies of
+ * the device totals (the totals are left unchanged). */
+int pbt_divide_by_num_orientations_c(pbt_ctx *ctx, int64_t num_orients, double *mueller_total,
+                                     double *mueller_1d_total, pbt_output_params *params_total);
+
+/* Zero the device totals (start of a new orientation average). */
+int pbt_totals_reset_c(pbt_ctx *ctx);
+
+/* -------------------------------------------------------- batched averaging */
+
+/* Orientation averaging in one call: the per-orientation loop of
+ * src/pbt_seq_mod.f90:146-269 from diff_main through summation, then
+ * divide_by_num_orientations (src/pbt_seq_mod.f90:274).
+ *   beam / ext        outbeams of all orientations, orientation-major; the
+ *                     outbeams of orientation o are beam[beam_off[o] .. beam_off[o+1])
+ *   verts             norient consecutive v(nverts,3) blocks (each orientation's
+ *                     rotated geometry; topology shared)
+ *   params_in         norient records (abs, geo_cross_sec, beam/ext energy)
+ *   mueller_avg       (nphi,ntheta,16) orientation average
+ *   mueller_1d_avg    (ntheta,16) orientation average
+ *   params_avg        averaged parameters
+ *   params_per_orient optional (NULL), norient records
+ * PBT_PREC_FP32 runs the batched FP32 kernel over all orientations with an
+ * FP64 epilogue; PBT_PREC_FP64 runs the reference-exact path per orientation. */
+int pbt_diff_batch_c(pbt_ctx *ctx, int64_t norient, const pbt_outbeam *beam,
+                     const int64_t *beam_off, const pbt_outbeam *ext, const int64_t *ext_off,
+                     const double *verts, int64_t nverts, const int64_t *face_off,
+                     const int64_t *face_vi, int64_t nfaces, const double *theta, int64_t ntheta,
+                     const double *phi, int64_t nphi, double lambda, int32_t is_fast_diff,
+                     int32_t scaling, int32_t precision, const pbt_output_params *params_in,
+                     double *mueller_avg, double *mueller_1d_avg, pbt_output_params *params_avg,
+                     pbt_output_params *params_per_orient);
+
+/* Same as pbt_diff_batch_c with the bulk arrays already in device memory of
+ * the context's device: beam, ext, verts, face_vi, params_in and all outputs
+ * are device pointers; beam_off, ext_off, face_off, theta and phi are host
+ * arrays (the sizes and offsets that plan the launch).  Work is ordered on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream) and the call
+ * returns without synchronising once the grid tables are cached.  FP32 only;
+ * device-side input errors (a face index out of range) are not reported by
+ * this entry point. */
+int pbt_diff_batch_dev_c(pbt_ctx *ctx, void *stream, int64_t norient, const pbt_outbeam *beam,
+                         const int64_t *beam_off, const pbt_outbeam *ext, const int64_t *ext_off,
+                         const double *verts, int64_t nverts, const int64_t *face_off,
+                         const int64_t *face_vi, int64_t nfaces, const double *theta,
+                         int64_t ntheta, const double *phi, int64_t nphi, double lambda,
+                         int32_t is_fast_diff, int32_t scaling, int32_t precision,
+                         const pbt_output_params *params_in, double *mueller_avg,
+                         double *mueller_1d_avg, pbt_output_params *params_avg,
+                         pbt_output_params *params_per_orient);
+
+/* ---------------------------------------------------------- introspection */
+
+/* Number of kernel launches made by the last completed compute call on this
+ * context (for launch accounting in benchmarks). */
+int64_t pbt_last_launch_count(pbt_ctx *ctx);
+
+/* Enable (1) or disable (0) CUDA-event timing of the far-field kernels (the
+ * FP64 and FP32 facet x bin sums).  While enabled, every such launch is
+ * bracketed by events on its stream. */
+int pbt_set_kernel_timing(pbt_ctx *ctx, int32_t enable);
+
+/* Sum of the device durations (ms) of the far-field kernel launches timed
+ * since the previous call, and their number; waits for the last of them.
+ * Resets the record. */
+int pbt_kernel_time_ms(pbt_ctx *ctx, double *total_ms, int64_t *nlaunch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PBT_DIFF_H */

@@ -1,0 +1,88 @@
+"""FP32 form (FP64 phase) against the FP64 references.
+
+Bar (north-star precision target): <= 1e-4 relative on every Mueller element
+at bins whose M11 exceeds 1e-6 of the peak (normalised by the bin's M11, see
+helpers.mueller_rel_err); cross sections and asymmetry parameters within
+1e-5 relative.
+"""
+import numpy as np
+import pytest
+
+import abt_b200
+from abt_b200 import workloads as W
+from oracle import oracle as O
+from tests.helpers import mixed_polygon_geometry, mueller_rel_err, one_triangle, outbeams, rel_err
+
+pytestmark = pytest.mark.gpu
+
+LAM = 0.532
+TOL_MU = 1e-4
+TOL_PARAM = 1e-5
+
+
+def _mueller(afb, afe):
+    k = 2 * abt_b200.PI_REF / LAM
+    return O.ampl_to_mueller((afb + afe) * k)
+
+
+def test_fp32_single_facet_vs_oracle(ctx):
+    rng = np.random.default_rng(1)
+    th, ph = abt_b200.make_angles([0, 180], [1]), abt_b200.make_angles([0, 358], [2])
+    geo = one_triangle(scale=2.0)
+    beam = outbeams(1, rng, 1)
+    ext = outbeams(1, rng, 1, prop=(0, 0, -1))
+    afb, afe = ctx.diff_main(beam, ext, geo, th, ph, LAM, precision="fp32")
+    rfb, rfe = O.diff_main(th, ph, LAM, geo, beam, ext)
+    assert rel_err(afb, rfb) <= 2e-5
+    assert rel_err(afe, rfe) <= 2e-5
+    assert mueller_rel_err(_mueller(afb, afe), _mueller(rfb, rfe)) <= TOL_MU
+
+
+def test_fp32_large_particle_phase_vs_oracle(ctx):
+    """Facets spread over a 100 um cube: far-field phases ~1e3 rad (size parameter ~590)."""
+    th, ph = abt_b200.make_angles([0, 180], [2]), abt_b200.make_angles([0, 356], [4])
+    geo, beam, ext = W.synthetic_beam_list(n_beams=8, facets_per_beam=8, seed=3)
+    afb, afe = ctx.diff_main(beam, ext, geo, th, ph, LAM, precision="fp32")
+    rfb, rfe = O.diff_main(th, ph, LAM, geo, beam, ext)
+    assert rel_err(afb, rfb) <= 1e-4
+    assert mueller_rel_err(_mueller(afb, afe), _mueller(rfb, rfe)) <= TOL_MU
+
+
+def test_fp32_polygons_and_fast_diff(ctx):
+    rng = np.random.default_rng(4)
+    th, ph = abt_b200.make_angles([0, 180], [2]), abt_b200.make_angles([0, 356], [4])
+    geo = mixed_polygon_geometry(rng)
+    nf = len(geo["face_off"]) - 1
+    beam = outbeams(10, rng, nf)
+    ext = outbeams(nf, rng, nf, prop=(0, 0, -1))
+    ext["fi"] = np.arange(1, nf + 1)
+    for fast in (False, True):
+        afb, afe = ctx.diff_main(beam, ext, geo, th, ph, LAM, is_fast_diff=fast, precision="fp32")
+        rfb, rfe = O.diff_main(th, ph, LAM, geo, beam, ext, is_fast_diff=fast)
+        assert mueller_rel_err(_mueller(afb, afe), _mueller(rfb, rfe)) <= TOL_MU
+
+
+@pytest.mark.parametrize("scaling", [False, True])
+def test_batch_fp32_vs_fp64(ctx, scaling):
+    rng = np.random.default_rng(8)
+    th, ph = abt_b200.make_angles([0, 180], [2]), abt_b200.make_angles([0, 356], [4])
+    geo = W.hex_prism(3.0, 6.0, n_side=2, n_len=3, roughness=0.05, seed=2)
+    beams, exts, Vs, pins = [], [], [], []
+    for k in range(5):
+        R = W.euler_rotation(*rng.uniform(0, 2 * np.pi, size=3))
+        V, beam, ext, gcs = W.standin_orientation(geo, R, rng, n_internal=(0, 2))
+        beams.append(beam)
+        exts.append(ext)
+        Vs.append(V)
+        pins.append(abt_b200.params(abs=0.02, geo_cross_sec=gcs, beam_energy_out=0.8 * gcs,
+                                    ext_energy_out=gcs))
+    pins = np.array(pins)
+    r = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pins, scaling=scaling, precision="fp64")
+    f = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pins, scaling=scaling, precision="fp32")
+    assert mueller_rel_err(f[0], r[0]) <= TOL_MU
+    assert rel_err(f[1], r[1]) <= TOL_MU
+    for n in ("scatt", "ext", "asymmetry", "scatt_beam", "scatt_ext_diff", "asymmetry_beam",
+              "asymmetry_ext_diff", "albedo"):
+        assert abs(f[2][n] - r[2][n]) <= TOL_PARAM * abs(r[2][n]), n
+        np.testing.assert_allclose(f[3][n], r[3][n], rtol=TOL_PARAM, err_msg=n)
+    np.testing.assert_allclose(f[3]["back_scatt"], r[3]["back_scatt"], rtol=1e-4)
