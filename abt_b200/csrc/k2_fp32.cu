@@ -47,6 +47,8 @@ constexpr int K2_NST = 3;   // stages
 constexpr double kTwoPi = 6.283185307179586;
 constexpr double kInv2Pi = 0.15915494309189535;
 constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52, round-to-integer constant
+// 1 - c^2 for the reference's clamp c = 0.999999 (a float literal)
+constexpr float kOneMinusClampSq = (float)(1.0 - (double)0.999999f * (double)0.999999f);
 
 struct BinDev {
     double ux, uy, uz;  // unit bin direction, FP64
@@ -342,14 +344,18 @@ __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const
         const float rf = (float)fma(-nq, kTwoPi, ka);
         const float a = fmaf(B.fz, r.eps[2], fmaf(B.fy, r.eps[1], B.fx * r.eps[0]));
         const float ph = fmaf(hkR * fmaf(-a, a, r.b), 1.0f + a, -rf);
-        // bin direction from the facet centre, in the aperture frame
+        // bin direction from the facet centre, in the aperture frame:
+        // (u - e)/|u - e| = u (1 + a + 3a^2/2 - b/2) - e (1 + a) + O(|e|^3), e = c/R.
+        // The second-order terms matter: near k ~ +-y the polarisation matrix
+        // depends on 1 - ky^2 and amplifies direction errors by 1/(1 - ky^2).
         const float opa = 1.0f + a;
+        const float opa2 = fmaf(a, fmaf(1.5f, a, 1.0f), fmaf(-0.5f, r.b, 1.0f));
         const float w0 = fmaf(r.R[2], B.fz, fmaf(r.R[1], B.fy, r.R[0] * B.fx));
         const float w1 = fmaf(r.R[5], B.fz, fmaf(r.R[4], B.fy, r.R[3] * B.fx));
         const float w2 = fmaf(r.R[8], B.fz, fmaf(r.R[7], B.fy, r.R[6] * B.fx));
-        const float kx = fmaf(w0, opa, -r.ea[0]);
-        const float ky = fmaf(w1, opa, -r.ea[1]);
-        const float kz = fmaf(w2, opa, -r.ea[2]);
+        const float kx = fmaf(w0, opa2, -r.ea[0] * opa);
+        const float ky = fmaf(w1, opa2, -r.ea[1] * opa);
+        const float kz = fmaf(w2, opa2, -r.ea[2] * opa);
         bool use = valid[q];
         if (FAST) {
             // lab-frame direction from the centre: u - eps + u a
@@ -366,9 +372,12 @@ __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const
         const float t2 = fmaf(kyy, r.vy[1], fmaf(kxx, r.vx[1], ph));
         const float t3 = fmaf(kyy, r.vy[2], fmaf(kxx, r.vx[2], ph));
         const float2 g = tri_dd(t1, t2, t3);
-        // Karczewski-Wolf polarisation matrix [[d, e], [-e, d]]
+        // Karczewski-Wolf polarisation matrix [[d, e], [-e, d]].  1 - ky^2 is
+        // formed as kx^2 + kz^2 (equal for a unit vector, without the
+        // cancellation near |ky| = 1); the floor is the reference's clamp
+        // |ky| <= 0.999999 (src/diff_mod.f90:151).
         const float kyc = fminf(fmaxf(ky, -0.999999f), 0.999999f);
-        const float tt = fmaf(-kyc, kyc, 1.0f);
+        const float tt = fmaxf(fmaf(kx, kx, kz * kz), kOneMinusClampSq);
         const float rs = rsqrtf(tt);
         const float s = tt * rs;
         const float kyrs = kyc * rs;
@@ -381,9 +390,10 @@ __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const
         if (!(fabsf(dinc) < 0.999f)) {
             const float ah = fmaf(B.hz, r.eps[2], fmaf(B.hy, r.eps[1], B.hx * r.eps[0]));
             const float oh = 1.0f + ah;
-            qx = fmaf(fmaf(r.R[2], B.hz, fmaf(r.R[1], B.hy, r.R[0] * B.hx)), oh, -r.ea[0]);
-            qy = fmaf(fmaf(r.R[5], B.hz, fmaf(r.R[4], B.hy, r.R[3] * B.hx)), oh, -r.ea[1]);
-            qz = fmaf(fmaf(r.R[8], B.hz, fmaf(r.R[7], B.hy, r.R[6] * B.hx)), oh, -r.ea[2]);
+            const float oh2 = fmaf(ah, fmaf(1.5f, ah, 1.0f), fmaf(-0.5f, r.b, 1.0f));
+            qx = fmaf(fmaf(r.R[2], B.hz, fmaf(r.R[1], B.hy, r.R[0] * B.hx)), oh2, -r.ea[0] * oh);
+            qy = fmaf(fmaf(r.R[5], B.hz, fmaf(r.R[4], B.hy, r.R[3] * B.hx)), oh2, -r.ea[1] * oh);
+            qz = fmaf(fmaf(r.R[8], B.hz, fmaf(r.R[7], B.hy, r.R[6] * B.hx)), oh2, -r.ea[2] * oh);
         }
         float hx = fmaf(r.inc[1], qz, -r.inc[2] * qy);
         float hy = fmaf(r.inc[2], qx, -r.inc[0] * qz);

@@ -33,8 +33,8 @@ def test_fp32_single_facet_vs_oracle(ctx):
     ext = outbeams(1, rng, 1, prop=(0, 0, -1))
     afb, afe = ctx.diff_main(beam, ext, geo, th, ph, LAM, precision="fp32")
     rfb, rfe = O.diff_main(th, ph, LAM, geo, beam, ext)
-    assert rel_err(afb, rfb) <= 2e-5
-    assert rel_err(afe, rfe) <= 2e-5
+    assert rel_err(afb, rfb) <= 1e-5
+    assert rel_err(afe, rfe) <= 1e-5
     assert mueller_rel_err(_mueller(afb, afe), _mueller(rfb, rfe)) <= TOL_MU
 
 
