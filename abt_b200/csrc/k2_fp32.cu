@@ -402,9 +402,17 @@ __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const
         hx *= hn;
         hy *= hn;
         hz *= hn;
-        const float ex = fmaf(kyc, m2, -kz * m1);
-        const float ey = fmaf(kz, m0, -kx * m2);
-        const float ez = fmaf(kx, m1, -kyc * m0);
+        float ex = fmaf(kyc, m2, -kz * m1);
+        float ey = fmaf(kz, m0, -kx * m2);
+        float ez = fmaf(kx, m1, -kyc * m0);
+        if (tt <= kOneMinusClampSq) {
+            // inside the clamp cone k and m are not unit vectors and the
+            // reference's normalisation of k x m (src/diff_mod.f90:637) matters
+            const float ne = rsqrtf(fmaf(ez, ez, fmaf(ey, ey, ex * ex)));
+            ex *= ne;
+            ey *= ne;
+            ez *= ne;
+        }
         const float p = fmaf(hz, m2, fmaf(hy, m1, hx * m0));
         const float rr = fmaf(hz, ez, fmaf(hy, ey, hx * ex));
         const float A = fmaf(p, d, rr * e);

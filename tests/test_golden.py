@@ -41,8 +41,8 @@ def test_gpu_fp64_matches_fixture(ctx, name):
     afb, afe = ctx.diff_main(z["beam"], z["ext"], z["geo"], z["theta"], z["phi"], lam)
     assert rel_err(afb, z["ampl_far_beam"]) <= 1e-10
     assert rel_err(afe, z["ampl_far_ext_diff"]) <= 1e-10
-    pin = np.zeros((), dtype=abt_b200.PARAMS_DTYPE)
-    pin.view(np.float64)[:] = z["params_in"]
+    pin = np.frombuffer(np.ascontiguousarray(z["params_in"], dtype=np.float64).tobytes(),
+                        dtype=abt_b200.PARAMS_DTYPE)[0]
     mu, mu1, p = ctx.finalise(afb, afe, z["theta"], z["phi"], lam, pin)
     assert rel_err(mu, z["mueller"]) <= 1e-10
     assert rel_err(mu1, z["mueller_1d"]) <= 1e-10

@@ -1,0 +1,28 @@
+"""The C ABI from compiled C: abt_b200/examples/c_drop_in.c built with gcc."""
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def build_c_caller(tmp_path):
+    exe = str(tmp_path / "c_drop_in")
+    libdir = os.path.join(ROOT, "abt_b200")
+    subprocess.check_call(["gcc", "-O2", "-std=c99", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(libdir, "examples", "c_drop_in.c"), "-o", exe,
+                           "-L", libdir, "-lpbt_b200", "-Wl,-rpath," + libdir, "-lm"])
+    return exe
+
+
+def test_c_caller_builds(tmp_path):
+    assert os.path.exists(build_c_caller(tmp_path))
+
+
+@pytest.mark.gpu
+def test_c_caller_runs(tmp_path):
+    exe = build_c_caller(tmp_path)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("ok ")
