@@ -35,7 +35,7 @@ EXPORTS = ("pbt_ctx_create", "pbt_ctx_destroy", "pbt_last_error_string", "pbt_ve
            "pbt_diff_main_c", "pbt_diffraction_c", "pbt_finalise_c", "pbt_summation_c",
            "pbt_divide_by_num_orientations_c", "pbt_totals_reset_c", "pbt_diff_batch_c",
            "pbt_diff_batch_dev_c", "pbt_last_launch_count", "pbt_set_kernel_timing",
-           "pbt_kernel_time_ms")
+           "pbt_kernel_time_ms", "pbt_diffraction_noalloc_c")
 
 
 class PbtError(RuntimeError):
@@ -76,6 +76,7 @@ def lib():
         "pbt_last_launch_count": (I64, [P]),
         "pbt_set_kernel_timing": (C, [P, I32]),
         "pbt_kernel_time_ms": (C, [P, ctypes.POINTER(D), ctypes.POINTER(I64)]),
+        "pbt_diffraction_noalloc_c": (C, [P, P, I64, P, P, I64, P, I64, P, I64, D, I32, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

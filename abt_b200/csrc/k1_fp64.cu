@@ -9,6 +9,11 @@
 // contour integral (:357-428), then multiplies (:665-670).  The file is built
 // with -fmad=false so no multiply-add is fused.  Facet frames come from the
 // host (host_setup.cpp); the bin grid and cos/sin(phi) are libm values.
+#include <float.h>
+#include <math.h>
+
+#include <mutex>
+
 #include "frame.h"
 #include "pbt_internal.h"
 
@@ -244,3 +249,192 @@ int k1_launch(pbt_ctx *ctx, cudaStream_t st, const K1Facet *d_fac, int64_t nf,
 }
 
 }  // namespace pbt
+
+// ---------------------------------------------------------------------------
+// pbt_diffraction_noalloc_c: pbt_diffraction_c without any allocation.
+//
+// Some host programs cannot let a library allocate device memory: programs
+// whose device memory is reserved up front by their own pool allocator (a
+// cudaMalloc from inside the library would fail, or fragment that pool), and
+// programs run under a rule that nothing is allocated after start-up.  This
+// variant computes the same FP64 far-field amplitude of one outbeam as
+// pbt_diffraction_c, but keeps its device scratch (bin grid, facet record,
+// edges, result grid) in one fixed array compiled into the library and its
+// host staging in static storage, so it calls no cudaMalloc, cudaFree,
+// cudaMallocHost or other allocating routine, and needs no context.
+//
+// Limits: ntheta * nphi <= PBT_NOALLOC_MAX_BINS (65,536 bins), nphi <=
+// PBT_NOALLOC_MAX_PHI (4,096), faces of at most PBT_NOALLOC_MAX_VERTS (64)
+// vertices; larger inputs are rejected with PBT_EINVAL.  The array takes
+// about 5.6 MB on every GPU that loads the library, until the process exits.
+//
+// Set-up: the first call on a device (with that device current) looks up the
+// array's device address with cudaGetSymbolAddress; make that first call
+// before any stream capture.  Every call on a device shares the one array and
+// overwrites what the previous call left there; the result grid is written in
+// full, so nothing has to start at zero.  Calls in one process are serialised
+// by a host lock and finish before they return; calls that overlapped on the
+// GPU would race on the shared array.
+namespace pbt {
+namespace {
+
+constexpr int64_t kNaMaxBins = 65536;
+constexpr int64_t kNaMaxPhi = 4096;
+constexpr int kNaMaxVerts = 64;
+constexpr size_t kNaOffXyz = 0;
+constexpr size_t kNaOffPhi = kNaOffXyz + (size_t)3 * kNaMaxBins * sizeof(double);
+constexpr size_t kNaOffFacet = kNaOffPhi + (size_t)2 * kNaMaxPhi * sizeof(double);
+constexpr size_t kNaOffEdges = kNaOffFacet + 512;
+constexpr size_t kNaOffOut = kNaOffEdges + (((size_t)kNaMaxVerts * sizeof(K1Edge) + 255) & ~(size_t)255);
+constexpr size_t kNaBytes = kNaOffOut + (size_t)8 * kNaMaxBins * sizeof(double);
+static_assert(sizeof(K1Facet) <= 512, "facet slot");
+
+// the device scratch of pbt_diffraction_noalloc_c
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+constexpr int kNaMaxDevices = 64;
+static std::mutex g_na_mu;
+static void *g_na_dev[kNaMaxDevices];  // device address of g_noalloc_scratch, per device
+static double g_na_host[3 * kNaMaxBins + 2 * kNaMaxPhi];  // host staging of the bin grid
+
+int na_fail(int status, const char *msg) {
+    set_error("%s", msg);
+    return status;
+}
+
+}  // namespace
+}  // namespace pbt
+
+extern "C" int pbt_diffraction_noalloc_c(const pbt_outbeam *outbeam, const double *verts,
+                                         int64_t nverts, const int64_t *face_off,
+                                         const int64_t *face_vi, int64_t nfaces,
+                                         const double *theta, int64_t ntheta, const double *phi,
+                                         int64_t nphi, double lambda, int32_t is_fast_diff,
+                                         double *amplC) {
+    using namespace pbt;
+    clear_error();
+    if (!outbeam || !amplC) return na_fail(PBT_EINVAL, "outbeam and amplC must not be NULL");
+    if (!(lambda > 0) || !isfinite(lambda)) return na_fail(PBT_EINVAL, "lambda must be positive and finite");
+    PBT_TRY(validate_angles(theta, ntheta, phi, nphi));
+    if (ntheta * nphi > kNaMaxBins || nphi > kNaMaxPhi) {
+        set_error("pbt_diffraction_noalloc_c: grid %lld x %lld exceeds its fixed scratch "
+                  "(at most %lld bins and %lld phi values); use pbt_diffraction_c",
+                  (long long)ntheta, (long long)nphi, (long long)kNaMaxBins, (long long)kNaMaxPhi);
+        return PBT_EINVAL;
+    }
+    PBT_TRY(validate_geometry(verts, nverts, face_off, face_vi, nfaces));
+    PBT_TRY(validate_outbeams(outbeam, 1, nfaces, "outbeam"));
+    const int64_t fb = face_off[outbeam->fi - 1];
+    const int nv = (int)(face_off[outbeam->fi] - fb);
+    if (nv > kNaMaxVerts) {
+        set_error("pbt_diffraction_noalloc_c: face of %d vertices exceeds its limit of %d", nv,
+                  kNaMaxVerts);
+        return PBT_EINVAL;
+    }
+    int64_t theta_i = -1;
+    for (int64_t i = 0; i < ntheta; i++)
+        if (theta[i] > 1 * kPiRef / 180) {
+            theta_i = i;
+            break;
+        }
+    if (theta_i < 0) return na_fail(PBT_EINVAL, "no theta value above 1 degree");
+
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    int dev = 0;
+    PBT_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNaMaxDevices) return na_fail(PBT_ENODEV, "device index out of range");
+    if (!g_na_dev[dev]) {
+        // once per device, with that device current
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error("cudaGetSymbolAddress(g_noalloc_scratch) failed: %s", cudaGetErrorString(e));
+            return PBT_ECUDA;
+        }
+        g_na_dev[dev] = p;
+    }
+    unsigned char *base = static_cast<unsigned char *>(g_na_dev[dev]);
+
+    // bin grid (make_far_field_bins, phi fastest) and cos/sin(phi), libm values
+    const int64_t nb = ntheta * nphi;
+    double *hx = g_na_host, *hp = g_na_host + 3 * nb;
+    for (int64_t j = 0; j < ntheta; j++)
+        for (int64_t i = 0; i < nphi; i++) {
+            const int64_t o = i + nphi * j;
+            hx[o] = kFarR * sin(theta[j]) * cos(phi[i]);
+            hx[nb + o] = kFarR * sin(theta[j]) * sin(phi[i]);
+            hx[2 * nb + o] = -(kFarR * cos(theta[j]));
+        }
+    for (int64_t i = 0; i < nphi; i++) {
+        hp[i] = cos(phi[i]);
+        hp[nphi + i] = sin(phi[i]);
+    }
+
+    // the facet record and its edges (src/diff_mod.f90:515-574, :334-393), on the stack
+    const double waveno = 2.0 * kPiRef / lambda;
+    double vx[kNaMaxVerts], vy[kNaMaxVerts], vz[kNaMaxVerts];
+    double rx[kNaMaxVerts], ry[kNaMaxVerts], rz[kNaMaxVerts];
+    double xs[kNaMaxVerts], ys[kNaMaxVerts], ms[kNaMaxVerts];
+    for (int i = 0; i < nv; i++) {
+        const int64_t vi = face_vi[fb + i] - 1;
+        vx[i] = verts[vi];
+        vy[i] = verts[vi + nverts];
+        vz[i] = verts[vi + 2 * nverts];
+    }
+    FacetFrame fr;
+    fr.sign = 1.0;
+    facet_frame(vx, vy, vz, nv, outbeam->prop_out, outbeam->vk7, fr, rx, ry, rz);
+    K1Facet F;
+    K1Edge E[kNaMaxVerts];
+    for (int c = 0; c < 3; c++) {
+        F.com[c] = fr.com[c];
+        F.prop2[c] = fr.prop2[c];
+        F.inc2[c] = fr.inc2[c];
+        F.prop0[c] = outbeam->prop_out[c];
+    }
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) F.R[3 * a + b] = fr.R.m[a][b];
+    for (int q = 0; q < 8; q++) F.ampl[q] = fr.sign < 0 ? -outbeam->ampl[q] : outbeam->ampl[q];
+    F.cos_fov = cos(outbeam->fov);
+    F.kinc[0] = fr.prop2[0] * waveno;
+    F.kinc[1] = fr.prop2[1] * waveno;
+    F.edge_off = 0;
+    F.nv = nv;
+    for (int i = 0; i < nv; i++) {
+        double c[3] = {rx[i], ry[i], rz[i]}, r[3];
+        mv33(fr.R, c, r);
+        xs[i] = r[0];
+        ys[i] = r[1];
+    }
+    for (int i = 0; i < nv; i++) {
+        const int in = (i == nv - 1) ? 0 : i + 1;
+        ms[i] = (ys[in] - ys[i]) / (xs[in] - xs[i]);
+    }
+    for (int i = 0; i < nv; i++) {
+        double mj = ms[i], nj = 1 / ms[i];
+        if (fabs(mj) > DBL_MAX) mj = 1e6;
+        if (fabs(nj) > DBL_MAX) nj = 1e6;
+        if (fabs(mj) < 1e-9) nj = 1e6;
+        if (fabs(nj) < 1e-9) mj = 1e6;
+        const int in = (i == nv - 1) ? 0 : i + 1;
+        E[i] = K1Edge{xs[i], ys[i], mj, nj, xs[in] - xs[i], ys[in] - ys[i]};
+    }
+
+    // stage into the fixed array, run, copy the grid out (legacy default stream)
+    double *d_xyz = reinterpret_cast<double *>(base + kNaOffXyz);
+    double *d_phi = reinterpret_cast<double *>(base + kNaOffPhi);
+    K1Facet *d_fac = reinterpret_cast<K1Facet *>(base + kNaOffFacet);
+    K1Edge *d_edges = reinterpret_cast<K1Edge *>(base + kNaOffEdges);
+    double *d_out = reinterpret_cast<double *>(base + kNaOffOut);
+    PBT_CUDA_TRY(cudaMemcpy(d_xyz, hx, 3 * nb * sizeof(double), cudaMemcpyHostToDevice));
+    PBT_CUDA_TRY(cudaMemcpy(d_phi, hp, 2 * nphi * sizeof(double), cudaMemcpyHostToDevice));
+    PBT_CUDA_TRY(cudaMemcpy(d_fac, &F, sizeof(K1Facet), cudaMemcpyHostToDevice));
+    PBT_CUDA_TRY(cudaMemcpy(d_edges, E, nv * sizeof(K1Edge), cudaMemcpyHostToDevice));
+    const int threads = 128;
+    k1_kernel<<<(unsigned)((nb + threads - 1) / threads), threads>>>(
+        d_fac, 1, d_edges, d_xyz, d_phi, nphi, nb, theta_i, waveno, lambda, is_fast_diff ? 1 : 0,
+        d_out);
+    PBT_CUDA_TRY(cudaGetLastError());
+    PBT_CUDA_TRY(cudaMemcpy(amplC, d_out, 8 * nb * sizeof(double), cudaMemcpyDeviceToHost));
+    return PBT_OK;
+}

@@ -98,6 +98,27 @@ int pbt_diffraction_c(pbt_ctx *ctx, const pbt_outbeam *outbeam, const double *ve
                       int64_t nfaces, const double *theta, int64_t ntheta, const double *phi,
                       int64_t nphi, double lambda, int32_t is_fast_diff, double *amplC);
 
+/* pbt_diffraction_c for callers that cannot let a library allocate memory.
+ * No counterpart in the reference.  Programs whose device memory is reserved
+ * up front by their own pool allocator, or that may allocate nothing after
+ * start-up, can call this instead: it computes the same FP64 amplitude of one
+ * outbeam but keeps its device scratch in one fixed array built into the
+ * library (about 5.6 MB on every GPU that loads it, held until exit) and
+ * calls no allocation routine; it needs no context.  Limits: at most
+ * PBT_NOALLOC_MAX_BINS bins (ntheta * nphi), PBT_NOALLOC_MAX_PHI phi values
+ * and PBT_NOALLOC_MAX_VERTS vertices per face; larger inputs return
+ * PBT_EINVAL.  The first call on a device (made with that device current)
+ * looks up the array's address; make it before any stream capture.  All
+ * calls on a device share the array; calls in one process are serialised and
+ * complete before returning, and calls that overlapped on the GPU would race. */
+#define PBT_NOALLOC_MAX_BINS 65536
+#define PBT_NOALLOC_MAX_PHI 4096
+#define PBT_NOALLOC_MAX_VERTS 64
+int pbt_diffraction_noalloc_c(const pbt_outbeam *outbeam, const double *verts, int64_t nverts,
+                              const int64_t *face_off, const int64_t *face_vi, int64_t nfaces,
+                              const double *theta, int64_t ntheta, const double *phi,
+                              int64_t nphi, double lambda, int32_t is_fast_diff, double *amplC);
+
 /* ------------------------------------------------------------ outputs_mod */
 
 /* finalise replacement, src/outputs_mod.f90:63-278 (FP64, reference order).
