@@ -98,6 +98,30 @@ extern "C" int pbt_set_kernel_timing(pbt_ctx *ctx, int32_t enable) {
     return PBT_OK;
 }
 
+extern "C" int pbt_set_plan(pbt_ctx *ctx, int32_t variant, int32_t bins_per_thread,
+                            int64_t records_per_item) {
+    clear_error();
+    if (!ctx) {
+        set_error("context is NULL");
+        return PBT_EINVAL;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (variant < 0) {
+        ctx->plan_variant = -1;
+        return PBT_OK;
+    }
+    if (variant > 1 || (bins_per_thread != 1 && bins_per_thread != 2) || records_per_item < 32 ||
+        records_per_item > (1 << 22)) {
+        set_error("bad plan (variant %d, bins_per_thread %d, records_per_item %lld)", variant,
+                  bins_per_thread, (long long)records_per_item);
+        return PBT_EINVAL;
+    }
+    ctx->plan_variant = variant;
+    ctx->plan_bpt = bins_per_thread;
+    ctx->plan_rpi = records_per_item;
+    return PBT_OK;
+}
+
 extern "C" int pbt_kernel_time_ms(pbt_ctx *ctx, double *total_ms, int64_t *nlaunch) {
     clear_error();
     if (!ctx || !total_ms || !nlaunch) {

@@ -33,3 +33,24 @@ struct __align__(16) K2Fov {
 };
 
 }  // namespace pbt
+
+namespace pbt {
+
+// Two K2Rec records interleaved field by field (x = even record, y = odd
+// record), so that a shared-memory load of a float2 yields the operand pair of
+// a packed FP32x2 instruction evaluating two facets at once.  352 bytes.
+struct __align__(16) K2Pair {
+    double kc[3][2];  // k * com, [component][half]
+    float2 eps[3];
+    float2 b;
+    float2 R[9];
+    float2 nea[3];    // -R * com / R
+    float2 kp[2];
+    float2 hkz_cf, hicf, hkxky_cf;
+    float2 inc[3];
+    float2 vx[3], vy[3];
+    float2 amp[8];
+};
+static_assert(sizeof(K2Pair) == 352, "K2Pair must be 352 bytes");
+
+}  // namespace pbt

@@ -31,6 +31,9 @@
 // k(|X - c| - |X|) = -k u.c + k(|c|^2 - (u.c)^2)(1 + u.c/R)/(2R) is formed
 // with k u.c in FP64 and reduced mod 2 pi before the FP32 work; the common
 // e^{ik|X|} is applied per bin only when amplitudes are returned.
+#include <stdio.h>
+#include <stdlib.h>
+
 #include <cub/device/device_scan.cuh>
 
 #include "frame.h"
@@ -112,12 +115,40 @@ __global__ void k2_count_kernel(RefSrc S, int64_t nrefs, const int64_t *__restri
     cnt[g] = face_off[fi] - face_off[fi - 1] - 2;
 }
 
+// Write record r into half r % 2 of pair r / 2.
+__device__ __forceinline__ void store_pair_half(K2Pair *pairs, int64_t r, const K2Rec &rec) {
+    K2Pair &P = pairs[r >> 1];
+    const int h = (int)(r & 1);
+    auto put = [h](float2 &dst, float v) {
+        if (h)
+            dst.y = v;
+        else
+            dst.x = v;
+    };
+    for (int c = 0; c < 3; c++) {
+        P.kc[c][h] = rec.kc[c];
+        put(P.eps[c], rec.eps[c]);
+        put(P.nea[c], -rec.ea[c]);
+        put(P.inc[c], rec.inc[c]);
+        put(P.vx[c], rec.vx[c]);
+        put(P.vy[c], rec.vy[c]);
+    }
+    put(P.b, rec.b);
+    for (int q = 0; q < 9; q++) put(P.R[q], rec.R[q]);
+    put(P.kp[0], rec.kp[0]);
+    put(P.kp[1], rec.kp[1]);
+    put(P.hkz_cf, rec.hkz_cf);
+    put(P.hicf, rec.hicf);
+    put(P.hkxky_cf, rec.hkxky_cf);
+    for (int q = 0; q < 8; q++) put(P.amp[q], rec.amp[q]);
+}
+
 __global__ void k2_setup_kernel(RefSrc S, int64_t nrefs, const double *__restrict__ verts,
                                 int64_t nverts, const int64_t *__restrict__ face_off,
                                 const int64_t *__restrict__ face_vi, const int64_t *__restrict__ start,
                                 double waveno, double lambda, int fast_diff,
-                                K2Rec *__restrict__ recs, K2Fov *__restrict__ fovs,
-                                int *__restrict__ err) {
+                                K2Rec *__restrict__ recs, K2Pair *__restrict__ pairs,
+                                K2Fov *__restrict__ fovs, int *__restrict__ err) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= nrefs) return;
     int64_t o;
@@ -184,7 +215,10 @@ __global__ void k2_setup_kernel(RefSrc S, int64_t nrefs, const double *__restric
             rec.amp[2 * q] = (float)(-cpre * ob->ampl[2 * q + 1]);
             rec.amp[2 * q + 1] = (float)(cpre * ob->ampl[2 * q]);
         }
-        recs[r0 + t] = rec;
+        if (pairs)
+            store_pair_half(pairs, r0 + t, rec);
+        else
+            recs[r0 + t] = rec;
         if (fast_diff) {
             K2Fov fv;
             const double fov = kind ? kPiRef / 2.0 : ob->fov;
@@ -553,6 +587,365 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
     }
 }
 
+// ---------------------------------------------- packed two-facet main kernel
+//
+// Same arithmetic as k2_record, evaluated for two facets at once with packed
+// FP32x2 instructions (FFMA2/FMUL2/FADD2 of sm_100): the x lane carries the
+// even record of a K2Pair, the y lane the odd one.  The bin's data are
+// loop-invariant broadcast pairs.  Special-function calls, the sort of the
+// three phases and the FP64 phase stay per facet.
+
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 sel2(bool px, bool py, float2 a, float2 b) {
+    return make_float2(px ? a.x : b.x, py ? a.y : b.y);
+}
+
+struct BinPk {
+    double ux, uy, uz;     // unit bin direction, FP64
+    float2 fx, fy, fz;     // same, broadcast FP32 pairs
+    float2 hx, hy, hz;     // forward-bodge bin direction, broadcast pairs
+};
+
+// sin(h)/h (h >= 0) with one shared reciprocal: rh = 1/max(h, 0.5)
+__device__ __forceinline__ float2 sinc_pk(float2 h, float2 rh) {
+    const float2 h2 = mul2(h, h);
+    const float2 p = fma2(h2, fma2(h2, fma2(h2, fma2(h2, bc2(2.7557319e-6f), bc2(-1.9841270e-4f)),
+                                            bc2(8.3333333e-3f)),
+                                   bc2(-1.6666667e-1f)),
+                          bc2(1.0f));
+    const float2 q = mul2(make_float2(__sinf(h.x), __sinf(h.y)), rh);
+    return sel2(h.x < 0.5f, h.y < 0.5f, p, q);
+}
+
+// Second divided difference of e^{ix} at the three phases of each lane.
+__device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float2 &gx, float2 &gy) {
+    float2 lo, hi, mid;
+    lo.x = fminf(t1.x, t2.x);
+    hi.x = fmaxf(t1.x, t2.x);
+    mid.x = fmaxf(lo.x, fminf(hi.x, t3.x));
+    lo.x = fminf(lo.x, t3.x);
+    hi.x = fmaxf(hi.x, t3.x);
+    lo.y = fminf(t1.y, t2.y);
+    hi.y = fmaxf(t1.y, t2.y);
+    mid.y = fmaxf(lo.y, fminf(hi.y, t3.y));
+    lo.y = fminf(lo.y, t3.y);
+    hi.y = fmaxf(hi.y, t3.y);
+    const float2 D = add2(hi, neg2(lo));
+    const float2 h1 = mul2(bc2(0.5f), add2(mid, neg2(lo)));
+    const float2 h2 = mul2(bc2(0.5f), add2(hi, neg2(mid)));
+    const float2 c1 = add2(lo, h1), c2 = add2(mid, h2);
+    float2 s1, k1, s2, k2;
+    __sincosf(c1.x, &s1.x, &k1.x);
+    __sincosf(c1.y, &s1.y, &k1.y);
+    __sincosf(c2.x, &s2.x, &k2.x);
+    __sincosf(c2.y, &s2.y, &k2.y);
+    // 1/max(h1,.5), 1/max(h2,.5) and 1/D from one reciprocal of their product
+    const float2 a1 = make_float2(fmaxf(h1.x, 0.5f), fmaxf(h1.y, 0.5f));
+    const float2 a2 = make_float2(fmaxf(h2.x, 0.5f), fmaxf(h2.y, 0.5f));
+    const float2 Dg = make_float2(fmaxf(D.x, 0.25f), fmaxf(D.y, 0.25f));
+    const float2 p12 = mul2(a1, a2);
+    const float2 pr = mul2(p12, Dg);
+    const float2 r = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
+    const float2 rD = mul2(Dg, r);
+    const float2 sc1 = sinc_pk(h1, mul2(a2, rD));
+    const float2 sc2 = sinc_pk(h2, mul2(a1, rD));
+    const float2 iD = mul2(p12, r);
+    gx = mul2(fma2(sc1, s1, neg2(mul2(sc2, s2))), iD);
+    gy = mul2(fma2(sc2, k2, neg2(mul2(sc1, k1))), iD);
+    if (D.x < 0.25f || D.y < 0.25f) {
+        // all three phases within 0.25 rad: Taylor series about the middle phase
+        const float2 ya = add2(lo, neg2(mid)), yc = add2(hi, neg2(mid));
+        const float2 q1 = add2(ya, yc);
+        const float2 ya2 = mul2(ya, ya);
+        const float2 q2 = fma2(yc, q1, ya2);
+        const float2 ya3 = mul2(ya2, ya);
+        const float2 q3 = fma2(yc, q2, ya3);
+        const float2 ya4 = mul2(ya3, ya);
+        const float2 q4 = fma2(yc, q3, ya4);
+        const float2 q5 = fma2(yc, q4, mul2(ya4, ya));
+        const float2 q6 = fma2(yc, q5, mul2(ya4, ya2));
+        const float2 re = fma2(q6, bc2(1.0f / 40320.0f),
+                               fma2(q4, bc2(-1.0f / 720.0f), fma2(q2, bc2(1.0f / 24.0f), bc2(-0.5f))));
+        const float2 im = fma2(q5, bc2(-1.0f / 5040.0f),
+                               fma2(q3, bc2(1.0f / 120.0f), mul2(q1, bc2(-1.0f / 6.0f))));
+        float2 sm, cm;
+        __sincosf(mid.x, &sm.x, &cm.x);
+        __sincosf(mid.y, &sm.y, &cm.y);
+        const float2 sx = fma2(cm, re, neg2(mul2(sm, im)));
+        const float2 sy = fma2(cm, im, mul2(sm, re));
+        gx = sel2(D.x < 0.25f, D.y < 0.25f, sx, gx);
+        gy = sel2(D.x < 0.25f, D.y < 0.25f, sy, gy);
+    }
+}
+
+template <bool FAST>
+__device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const BinPk &B,
+                                        float2 (&acc)[8], float2 nk, float2 hkR, bool lo_ok,
+                                        bool hi_ok) {
+    // far-field phase per facet: FP64 k u.c, reduced mod 2 pi
+    float2 rf;
+    {
+        const double ka = fma(B.uz, P.kc[2][0], fma(B.uy, P.kc[1][0], B.ux * P.kc[0][0]));
+        const double nq = fma(ka, kInv2Pi, kMagic) - kMagic;
+        rf.x = (float)fma(-nq, kTwoPi, ka);
+        const double kb = fma(B.uz, P.kc[2][1], fma(B.uy, P.kc[1][1], B.ux * P.kc[0][1]));
+        const double nb = fma(kb, kInv2Pi, kMagic) - kMagic;
+        rf.y = (float)fma(-nb, kTwoPi, kb);
+    }
+    const float2 one = bc2(1.0f);
+    const float2 a = fma2(B.fz, P.eps[2], fma2(B.fy, P.eps[1], mul2(B.fx, P.eps[0])));
+    const float2 opa = add2(one, a);
+    const float2 ph = fma2(mul2(hkR, fma2(neg2(a), a, P.b)), opa, neg2(rf));
+    const float2 opa2 = fma2(a, fma2(bc2(1.5f), a, one), fma2(bc2(-0.5f), P.b, one));
+    const float2 w0 = fma2(P.R[2], B.fz, fma2(P.R[1], B.fy, mul2(P.R[0], B.fx)));
+    const float2 w1 = fma2(P.R[5], B.fz, fma2(P.R[4], B.fy, mul2(P.R[3], B.fx)));
+    const float2 w2 = fma2(P.R[8], B.fz, fma2(P.R[7], B.fy, mul2(P.R[6], B.fx)));
+    const float2 kx = fma2(w0, opa2, mul2(P.nea[0], opa));
+    const float2 ky = fma2(w1, opa2, mul2(P.nea[1], opa));
+    const float2 kz = fma2(w2, opa2, mul2(P.nea[2], opa));
+    bool ok_x = lo_ok, ok_y = hi_ok;
+    if (FAST) {
+        const float2 dx = fma2(B.fx, opa, neg2(P.eps[0]));
+        const float2 dy = fma2(B.fy, opa, neg2(P.eps[1]));
+        const float2 dz = fma2(B.fz, opa, neg2(P.eps[2]));
+        const K2Fov &fa = fv[0], &fb = fv[1];
+        const float dpx = fmaf(dz.x, fa.p0[2], fmaf(dy.x, fa.p0[1], dx.x * fa.p0[0]));
+        const float dpy = fmaf(dz.y, fb.p0[2], fmaf(dy.y, fb.p0[1], dx.y * fb.p0[0]));
+        ok_x = ok_x && !(dpx < fa.cos_fov);
+        ok_y = ok_y && !(dpy < fb.cos_fov);
+    }
+    // aperture integral
+    const float2 kxx = fma2(nk, kx, P.kp[0]);
+    const float2 kyy = fma2(nk, ky, P.kp[1]);
+    const float2 t1 = fma2(kyy, P.vy[0], fma2(kxx, P.vx[0], ph));
+    const float2 t2 = fma2(kyy, P.vy[1], fma2(kxx, P.vx[1], ph));
+    const float2 t3 = fma2(kyy, P.vy[2], fma2(kxx, P.vx[2], ph));
+    float2 gx, gy;
+    tri_dd_pk(t1, t2, t3, gx, gy);
+    // polarisation matrix [[d, e], [-e, d]] (see k2_record for the forms)
+    const float2 kyc = make_float2(fminf(fmaxf(ky.x, -0.999999f), 0.999999f),
+                                   fminf(fmaxf(ky.y, -0.999999f), 0.999999f));
+    const float2 tr = fma2(kx, kx, mul2(kz, kz));
+    const float2 tt = make_float2(fmaxf(tr.x, kOneMinusClampSq), fmaxf(tr.y, kOneMinusClampSq));
+    const float2 rs = make_float2(rsqrtf(tt.x), rsqrtf(tt.y));
+    const float2 s = mul2(tt, rs);
+    const float2 kyrs = mul2(kyc, rs);
+    const float2 m0 = neg2(mul2(kx, kyrs)), m1 = s, m2 = neg2(mul2(kz, kyrs));
+    const float2 d = fma2(P.hkz_cf, s, neg2(mul2(mul2(kz, rs), P.hicf)));
+    const float2 e = fma2(P.hkxky_cf, s, neg2(mul2(mul2(kx, kyrs), P.hicf)));
+    float2 qx = kx, qy = kyc, qz = kz;
+    const float2 dinc = fma2(P.inc[2], kz, fma2(P.inc[1], kyc, mul2(P.inc[0], kx)));
+    const bool bx = !(fabsf(dinc.x) < 0.999f), by = !(fabsf(dinc.y) < 0.999f);
+    if (bx || by) {
+        const float2 ah = fma2(B.hz, P.eps[2], fma2(B.hy, P.eps[1], mul2(B.hx, P.eps[0])));
+        const float2 oh = add2(one, ah);
+        const float2 oh2 = fma2(ah, fma2(bc2(1.5f), ah, one), fma2(bc2(-0.5f), P.b, one));
+        const float2 vx = fma2(fma2(P.R[2], B.hz, fma2(P.R[1], B.hy, mul2(P.R[0], B.hx))), oh2,
+                               mul2(P.nea[0], oh));
+        const float2 vy = fma2(fma2(P.R[5], B.hz, fma2(P.R[4], B.hy, mul2(P.R[3], B.hx))), oh2,
+                               mul2(P.nea[1], oh));
+        const float2 vz = fma2(fma2(P.R[8], B.hz, fma2(P.R[7], B.hy, mul2(P.R[6], B.hx))), oh2,
+                               mul2(P.nea[2], oh));
+        qx = sel2(bx, by, vx, qx);
+        qy = sel2(bx, by, vy, qy);
+        qz = sel2(bx, by, vz, qz);
+    }
+    float2 hx = fma2(P.inc[1], qz, neg2(mul2(P.inc[2], qy)));
+    float2 hy = fma2(P.inc[2], qx, neg2(mul2(P.inc[0], qz)));
+    float2 hz = fma2(P.inc[0], qy, neg2(mul2(P.inc[1], qx)));
+    const float2 hn2 = fma2(hz, hz, fma2(hy, hy, mul2(hx, hx)));
+    const float2 hn = make_float2(rsqrtf(hn2.x), rsqrtf(hn2.y));
+    hx = mul2(hx, hn);
+    hy = mul2(hy, hn);
+    hz = mul2(hz, hn);
+    float2 ex = fma2(kyc, m2, neg2(mul2(kz, m1)));
+    float2 ey = fma2(kz, m0, neg2(mul2(kx, m2)));
+    float2 ez = fma2(kx, m1, neg2(mul2(kyc, m0)));
+    const bool cx = tt.x <= kOneMinusClampSq, cy = tt.y <= kOneMinusClampSq;
+    if (cx || cy) {
+        const float2 en2 = fma2(ez, ez, fma2(ey, ey, mul2(ex, ex)));
+        const float2 ne = make_float2(cx ? rsqrtf(en2.x) : 1.0f, cy ? rsqrtf(en2.y) : 1.0f);
+        ex = mul2(ex, ne);
+        ey = mul2(ey, ne);
+        ez = mul2(ez, ne);
+    }
+    const float2 p = fma2(hz, m2, fma2(hy, m1, mul2(hx, m0)));
+    const float2 rr = fma2(hz, ez, fma2(hy, ey, mul2(hx, ex)));
+    const float2 A = fma2(p, d, mul2(rr, e));
+    const float2 Bc = fma2(p, e, neg2(mul2(rr, d)));
+    const float2 nB = neg2(Bc);
+    float2 G[8];
+    G[0] = fma2(A, P.amp[0], mul2(Bc, P.amp[2]));
+    G[1] = fma2(A, P.amp[1], mul2(Bc, P.amp[3]));
+    G[2] = fma2(A, P.amp[2], mul2(nB, P.amp[0]));
+    G[3] = fma2(A, P.amp[3], mul2(nB, P.amp[1]));
+    G[4] = fma2(A, P.amp[4], mul2(Bc, P.amp[6]));
+    G[5] = fma2(A, P.amp[5], mul2(Bc, P.amp[7]));
+    G[6] = fma2(A, P.amp[6], mul2(nB, P.amp[4]));
+    G[7] = fma2(A, P.amp[7], mul2(nB, P.amp[5]));
+    if (FAST || !lo_ok || !hi_ok) {
+        // a lane outside the item or outside the field of view adds nothing
+        gx = sel2(ok_x, ok_y, gx, bc2(0.0f));
+        gy = sel2(ok_x, ok_y, gy, bc2(0.0f));
+#pragma unroll
+        for (int c = 0; c < 8; c++) G[c] = sel2(ok_x, ok_y, G[c], bc2(0.0f));
+    }
+    const float2 ngy = neg2(gy);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        acc[2 * c] = fma2(gx, G[2 * c], fma2(ngy, G[2 * c + 1], acc[2 * c]));
+        acc[2 * c + 1] = fma2(gx, G[2 * c + 1], fma2(gy, G[2 * c], acc[2 * c + 1]));
+    }
+}
+
+constexpr int K2P_CH = 16;  // record pairs per shared-memory stage (32 records)
+
+struct K2PkArgs {
+    const K2Pair *pairs;
+    const K2Fov *fovs;
+    const int64_t *seg_rec;
+    const int64_t *item_pre;
+    int64_t nseg;
+    int64_t rpi;
+    int64_t ntiles;
+    const double *xyz;
+    int64_t nb, nphi;
+    int64_t theta_i;
+    float k;
+    float hkR;
+    float *ws;
+    unsigned long long *counter;
+    int *err;
+};
+
+template <int BPT, bool FAST>
+__global__ void __launch_bounds__(K2_THREADS) k2_main_pk_kernel(K2PkArgs P) {
+    __shared__ __align__(128) K2Pair sbuf[K2_NST][K2P_CH];
+    __shared__ __align__(8) uint64_t bars[K2_NST];
+    __shared__ long long s_item;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < K2_NST; s++) mbar_init(smem_u32(&bars[s]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t parity = 0;  // bit s: phase of stage s
+    const int64_t total = P.item_pre[P.nseg];
+    constexpr int64_t TILE = (int64_t)K2_THREADS * BPT;
+    const float2 nk = bc2(-P.k), hkR = bc2(P.hkR);
+    for (;;) {
+        if (tid == 0) s_item = (long long)atomicAdd(P.counter, 1ull);
+        __syncthreads();
+        const int64_t item = s_item;
+        if (item >= total) break;
+        int64_t lo = 0, hi = P.nseg;
+        while (hi - lo > 1) {
+            const int64_t m = (lo + hi) >> 1;
+            if (P.item_pre[m] <= item)
+                lo = m;
+            else
+                hi = m;
+        }
+        const int64_t seg = lo;
+        const int64_t local = item - P.item_pre[seg];
+        const int64_t split = local / P.ntiles, tile = local % P.ntiles;
+        const int64_t rbeg = P.seg_rec[seg] + split * P.rpi;
+        const int64_t rend = min(rbeg + P.rpi, P.seg_rec[seg + 1]);
+        BinPk bd[BPT];
+        bool valid[BPT];
+        int64_t bin[BPT];
+#pragma unroll
+        for (int q = 0; q < BPT; q++) {
+            bin[q] = tile * TILE + q * K2_THREADS + tid;
+            valid[q] = bin[q] < P.nb;
+            const int64_t o = valid[q] ? bin[q] : 0;
+            const double X = P.xyz[o], Y = P.xyz[P.nb + o], Zc = P.xyz[2 * P.nb + o];
+            const double ir = 1.0 / sqrt(X * X + Y * Y + Zc * Zc);
+            bd[q].ux = X * ir;
+            bd[q].uy = Y * ir;
+            bd[q].uz = Zc * ir;
+            bd[q].fx = bc2((float)bd[q].ux);
+            bd[q].fy = bc2((float)bd[q].uy);
+            bd[q].fz = bc2((float)bd[q].uz);
+            const int64_t oh = (o % P.nphi) + P.nphi * P.theta_i;
+            const double Xh = P.xyz[oh], Yh = P.xyz[P.nb + oh], Zh = P.xyz[2 * P.nb + oh];
+            const double irh = 1.0 / sqrt(Xh * Xh + Yh * Yh + Zh * Zh);
+            bd[q].hx = bc2((float)(Xh * irh));
+            bd[q].hy = bc2((float)(Yh * irh));
+            bd[q].hz = bc2((float)(Zh * irh));
+        }
+        double acc64[BPT][8];
+#pragma unroll
+        for (int q = 0; q < BPT; q++)
+#pragma unroll
+            for (int c = 0; c < 8; c++) acc64[q][c] = 0.0;
+        // record pairs [p0, p1) cover records [rbeg, rend)
+        const int64_t p0 = rbeg >> 1, p1 = (rend + 1) >> 1;
+        const int64_t npair = p1 - p0;
+        const int64_t nchunk = (npair + K2P_CH - 1) / K2P_CH;
+        if (tid == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            for (int64_t c = 0; c < nchunk && c < K2_NST; c++) {
+                const int64_t n = min((int64_t)K2P_CH, npair - c * K2P_CH);
+                bulk_load(smem_u32(&sbuf[c][0]), P.pairs + p0 + c * K2P_CH,
+                          (uint32_t)(n * sizeof(K2Pair)), smem_u32(&bars[c]));
+            }
+        }
+        bool timed_out = false;
+        for (int64_t c = 0; c < nchunk; c++) {
+            const int st = (int)(c % K2_NST);
+            const bool ok = mbar_wait(smem_u32(&bars[st]), (parity >> st) & 1u);
+            parity ^= 1u << st;
+            if (__syncthreads_or(!ok)) {
+                timed_out = true;
+                break;
+            }
+            const int n = (int)min((int64_t)K2P_CH, npair - c * K2P_CH);
+            float2 acc[BPT][8];
+#pragma unroll
+            for (int q = 0; q < BPT; q++)
+#pragma unroll
+                for (int cc = 0; cc < 8; cc++) acc[q][cc] = bc2(0.0f);
+            for (int j = 0; j < n; j++) {
+                const int64_t pi = p0 + c * K2P_CH + j;
+                const bool lo_ok = 2 * pi >= rbeg, hi_ok = 2 * pi + 1 < rend;
+                const K2Fov *fv = FAST ? P.fovs + 2 * pi : nullptr;
+#pragma unroll
+                for (int q = 0; q < BPT; q++)
+                    k2_pair<FAST>(sbuf[st][j], fv, bd[q], acc[q], nk, hkR, lo_ok && valid[q],
+                                  hi_ok && valid[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < BPT; q++)
+#pragma unroll
+                for (int cc = 0; cc < 8; cc++)
+                    acc64[q][cc] += (double)acc[q][cc].x + (double)acc[q][cc].y;
+            __syncthreads();
+            if (tid == 0 && c + K2_NST < nchunk) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                const int64_t c2 = c + K2_NST;
+                const int64_t n2 = min((int64_t)K2P_CH, npair - c2 * K2P_CH);
+                bulk_load(smem_u32(&sbuf[st][0]), P.pairs + p0 + c2 * K2P_CH,
+                          (uint32_t)(n2 * sizeof(K2Pair)), smem_u32(&bars[st]));
+            }
+        }
+        if (timed_out) {
+            if (tid == 0) atomicOr(P.err, 4);
+            return;
+        }
+        float *out = P.ws + seg * 8 * P.nb;
+#pragma unroll
+        for (int q = 0; q < BPT; q++)
+            if (valid[q])
+#pragma unroll
+                for (int cc = 0; cc < 8; cc++) atomicAdd(out + cc * P.nb + bin[q], (float)acc64[q][cc]);
+    }
+}
+
 // --------------------------------------------------------------- epilogue
 
 struct Zd {
@@ -784,14 +1177,41 @@ __global__ void k2_ampl_out_kernel(const float *__restrict__ ws, int64_t nb, int
 
 namespace {
 
+// Launch shape of the main kernel.  variant 1 = packed two-facet kernel over
+// K2Pair records, 0 = one facet per step over K2Rec records.  bpt = bins per
+// thread, rpi = facet records per work item.  PBT_K2_PLAN="variant,bpt,rpi"
+// overrides the default (used by the tuner).
 struct K2Plan {
-    int bpt = 2;
-    int64_t rpi = 2048;  // facet records per work item
+    int variant = 1;
+    int bpt = 1;
+    int64_t rpi = 2048;
 };
+
+K2Plan k2_plan_for(const pbt_ctx *ctx) {
+    K2Plan p;
+    if (ctx->plan_variant >= 0) {
+        p.variant = ctx->plan_variant;
+        p.bpt = ctx->plan_bpt;
+        p.rpi = ctx->plan_rpi;
+        return p;
+    }
+    if (const char *e = getenv("PBT_K2_PLAN")) {
+        int v = 0, b = 0;
+        long long r = 0;
+        if (sscanf(e, "%d,%d,%lld", &v, &b, &r) == 3 && (v == 0 || v == 1) && (b == 1 || b == 2) &&
+            r >= 32 && r <= (1 << 22)) {
+            p.variant = v;
+            p.bpt = b;
+            p.rpi = r;
+        }
+    }
+    return p;
+}
 
 // Device-side set-up shared by the batched and single-orientation entry points.
 struct K2Setup {
     K2Rec *recs = nullptr;
+    K2Pair *pairs = nullptr;
     K2Fov *fovs = nullptr;
     int64_t *start = nullptr;
     int64_t *refbase = nullptr;
@@ -806,7 +1226,7 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
                const int64_t *h_beam_off, const pbt_outbeam *d_ext, const int64_t *h_ext_off,
                const double *d_verts, int64_t nverts, const int64_t *d_face_off,
                const int64_t *d_face_vi, int64_t nfaces, int64_t max_nv, double lambda,
-               int fast_diff, K2Setup &S) {
+               int fast_diff, int variant, K2Setup &S) {
     const int64_t nrefs = h_beam_off[norient] + h_ext_off[norient];
     const int64_t max_recs = std::max<int64_t>(1, nrefs * std::max<int64_t>(1, max_nv - 2));
     // scan temp size
@@ -828,10 +1248,13 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
     S.ext_off = (int64_t *)(base + o_eo);
     S.err = (int *)(base + o_err);
     void *tmp = base + o_tmp;
-    PBT_TRY(ctx->d_rec.ensure(align_up(max_recs * sizeof(K2Rec)) +
-                              (fast_diff ? max_recs * sizeof(K2Fov) : 0)));
-    S.recs = ctx->d_rec.as<K2Rec>();
-    S.fovs = fast_diff ? (K2Fov *)(ctx->d_rec.as<char>() + align_up(max_recs * sizeof(K2Rec))) : nullptr;
+    // records (or record pairs; an even count so the last pair is whole)
+    const int64_t nrec2 = (max_recs + 1) & ~(int64_t)1;
+    const size_t rec_bytes = variant ? (size_t)(nrec2 / 2) * sizeof(K2Pair) : (size_t)max_recs * sizeof(K2Rec);
+    PBT_TRY(ctx->d_rec.ensure(align_up(rec_bytes) + (fast_diff ? nrec2 * sizeof(K2Fov) : 0)));
+    S.recs = variant ? nullptr : ctx->d_rec.as<K2Rec>();
+    S.pairs = variant ? ctx->d_rec.as<K2Pair>() : nullptr;
+    S.fovs = fast_diff ? (K2Fov *)(ctx->d_rec.as<char>() + align_up(rec_bytes)) : nullptr;
     // host-side offsets -> device (pinned staging; the previous call's copy
     // out of the staging buffer must have run before it is overwritten)
     if (ctx->stage_pending) {
@@ -863,7 +1286,7 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
     if (nrefs > 0)
         k2_setup_kernel<<<(unsigned)((nrefs + th - 1) / th), th, 0, st>>>(
             src, nrefs, d_verts, nverts, d_face_off, d_face_vi, S.start, waveno, lambda, fast_diff,
-            S.recs, S.fovs, S.err);
+            S.recs, S.pairs, S.fovs, S.err);
     ctx->launches += 3;
     PBT_CUDA_TRY(cudaGetLastError());
     return PBT_OK;
@@ -880,6 +1303,23 @@ int k2_launch_main(pbt_ctx *ctx, cudaStream_t st, const K2MainArgs &A) {
     const int grid = ctx->sm_count * occ;
     timing_begin(ctx, st);
     k2_main_kernel<BPT, FAST><<<grid, K2_THREADS, 0, st>>>(A);
+    timing_end(ctx, st);
+    ctx->launches++;
+    PBT_CUDA_TRY(cudaGetLastError());
+    return PBT_OK;
+}
+
+template <int BPT, bool FAST>
+int k2_launch_pk(pbt_ctx *ctx, cudaStream_t st, const K2PkArgs &A) {
+    static int occ = -1;
+    if (occ < 0) {
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k2_main_pk_kernel<BPT, FAST>, K2_THREADS, 0);
+        occ = n > 0 ? n : 1;
+    }
+    const int grid = ctx->sm_count * occ;
+    timing_begin(ctx, st);
+    k2_main_pk_kernel<BPT, FAST><<<grid, K2_THREADS, 0, st>>>(A);
     timing_end(ctx, st);
     ctx->launches++;
     PBT_CUDA_TRY(cudaGetLastError());
@@ -914,6 +1354,28 @@ int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, in
     A.ws = ws;
     A.counter = counter;
     A.err = S.err;
+    if (plan.variant == 1) {
+        K2PkArgs B;
+        B.pairs = S.pairs;
+        B.fovs = S.fovs;
+        B.seg_rec = seg_rec;
+        B.item_pre = item_pre;
+        B.nseg = A.nseg;
+        B.rpi = plan.rpi;
+        B.ntiles = ntiles;
+        B.xyz = A.xyz;
+        B.nb = A.nb;
+        B.nphi = A.nphi;
+        B.theta_i = A.theta_i;
+        B.k = A.k;
+        B.hkR = A.hkR;
+        B.ws = ws;
+        B.counter = counter;
+        B.err = S.err;
+        if (plan.bpt == 1)
+            return fast_diff ? k2_launch_pk<1, true>(ctx, st, B) : k2_launch_pk<1, false>(ctx, st, B);
+        return fast_diff ? k2_launch_pk<2, true>(ctx, st, B) : k2_launch_pk<2, false>(ctx, st, B);
+    }
     if (plan.bpt == 1)
         return fast_diff ? k2_launch_main<1, true>(ctx, st, A) : k2_launch_main<1, false>(ctx, st, A);
     return fast_diff ? k2_launch_main<2, true>(ctx, st, A) : k2_launch_main<2, false>(ctx, st, A);
@@ -957,11 +1419,11 @@ int k2_batch_impl(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outb
                   pbt_output_params *d_params_per, int check_errors) {
     const GridCache &g = ctx->grid;
     const int64_t nb = g.nb, nphi = (int64_t)g.phi.size(), ntheta = (int64_t)g.theta.size();
-    K2Plan plan;
+    const K2Plan plan = k2_plan_for(ctx);
     K2Setup S;
     PBT_TRY(k2_prepare(ctx, st, norient, d_beam, h_beam_off, d_ext, h_ext_off, d_verts, nverts,
                        d_face_off, d_face_vi, nfaces, max_face_nv(h_face_off, nfaces), lambda,
-                       fast_diff, S));
+                       fast_diff, plan.variant, S));
     // orientation chunks sized to a workspace cap
     const size_t per_orient = (size_t)2 * 8 * nb * sizeof(float);
     const size_t cap = (size_t)8 << 30;
@@ -1027,11 +1489,11 @@ int k2_diff_main_impl(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *d_beam, 
                       double *d_afb, double *d_afe) {
     const GridCache &g = ctx->grid;
     const int64_t nb = g.nb;
-    K2Plan plan;
+    const K2Plan plan = k2_plan_for(ctx);
     K2Setup S;
     const int64_t hbo[2] = {0, nbeam}, heo[2] = {0, next};
     PBT_TRY(k2_prepare(ctx, st, 1, d_beam, hbo, d_ext, heo, d_verts, nverts, d_face_off, d_face_vi,
-                       nfaces, max_face_nv(h_face_off, nfaces), lambda, fast_diff, S));
+                       nfaces, max_face_nv(h_face_off, nfaces), lambda, fast_diff, plan.variant, S));
     const size_t o_ws = 0, o_seg = align_up(o_ws + (size_t)2 * 8 * nb * sizeof(float)),
                  o_it = align_up(o_seg + 3 * 8), o_cnt = align_up(o_it + 3 * 8), o_end = align_up(o_cnt + 64);
     PBT_TRY(ctx->d_ws.ensure(o_end));

@@ -116,6 +116,9 @@ struct pbt_ctx {
     pbt::DevTotals btot;   // totals of the FP64 batch path
     int64_t launches = 0;            // kernel launches of the last compute call
     int sm_count = 0;
+    // launch plan of the FP32 main kernel (-1: default / PBT_K2_PLAN)
+    int plan_variant = -1, plan_bpt = 1;
+    int64_t plan_rpi = 2048;
     // CUDA-event timing of the far-field kernels
     bool timing = false;
     std::vector<cudaEvent_t> ev;  // start/stop pairs

@@ -119,6 +119,11 @@ class Context:
     def set_kernel_timing(self, enable=True):
         check(_lib.lib().pbt_set_kernel_timing(self._h, int(bool(enable))))
 
+    def set_plan(self, variant=-1, bins_per_thread=1, records_per_item=2048):
+        """Launch plan of the FP32 kernel (variant < 0: default)."""
+        check(_lib.lib().pbt_set_plan(self._h, int(variant), int(bins_per_thread),
+                                      int(records_per_item)))
+
     def kernel_time_ms(self):
         """(total ms, launches) of the far-field kernels timed since the last call."""
         t = ctypes.c_double()
