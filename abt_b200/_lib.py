@@ -35,7 +35,8 @@ EXPORTS = ("pbt_ctx_create", "pbt_ctx_destroy", "pbt_last_error_string", "pbt_ve
            "pbt_diff_main_c", "pbt_diffraction_c", "pbt_finalise_c", "pbt_summation_c",
            "pbt_divide_by_num_orientations_c", "pbt_totals_reset_c", "pbt_diff_batch_c",
            "pbt_diff_batch_dev_c", "pbt_last_launch_count", "pbt_set_kernel_timing",
-           "pbt_kernel_time_ms", "pbt_diffraction_noalloc_c", "pbt_set_plan")
+           "pbt_kernel_time_ms", "pbt_diffraction_noalloc_c", "pbt_set_plan",
+           "pbt_diff_adjoint_c")
 
 
 class PbtError(RuntimeError):
@@ -78,6 +79,8 @@ def lib():
         "pbt_kernel_time_ms": (C, [P, ctypes.POINTER(D), ctypes.POINTER(I64)]),
         "pbt_diffraction_noalloc_c": (C, [P, P, I64, P, P, I64, P, I64, P, I64, D, I32, P]),
         "pbt_set_plan": (C, [P, I32, I32, I64]),
+        "pbt_diff_adjoint_c": (C, [P, P, I64, P, I64, P, I64, P, P, I64, P, I64, P, I64, D, I32,
+                                   P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -27,6 +27,7 @@ UNITS = {
     "k1_fp64.cu": ["-fmad=false"],
     "k3_finalise.cu": ["-fmad=false"],
     "k2_fp32.cu": [],
+    "k4_adjoint.cu": [],
 }
 HOST_UNITS = {"host_setup.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
                                  "-fPIC", "-std=c++17", "-I" + CSRC, "-I" + INCLUDE,

@@ -493,3 +493,37 @@ extern "C" int pbt_diff_batch_dev_c(pbt_ctx *ctx, void *stream, int64_t norient,
                          scaling ? 1 : 0, params_in, mueller_avg, mueller_1d_avg, params_avg,
                          params_per_orient, 0);
 }
+
+namespace pbt {
+int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t nbeam,
+               const pbt_outbeam *ext, int64_t next, const double *verts, int64_t nverts,
+               const int64_t *face_off, const int64_t *face_vi, int64_t nfaces, double lambda,
+               int fast_diff, const double *gafb, const double *gafe, double *gverts,
+               double *gbeam, double *gext);
+}
+
+extern "C" int pbt_diff_adjoint_c(pbt_ctx *ctx, const pbt_outbeam *beam, int64_t nbeam,
+                                  const pbt_outbeam *ext, int64_t next, const double *verts,
+                                  int64_t nverts, const int64_t *face_off, const int64_t *face_vi,
+                                  int64_t nfaces, const double *theta, int64_t ntheta,
+                                  const double *phi, int64_t nphi, double lambda,
+                                  int32_t is_fast_diff, const double *grad_ampl_far_beam,
+                                  const double *grad_ampl_far_ext_diff, double *grad_verts,
+                                  double *grad_beam_ampl, double *grad_ext_ampl) {
+    API_ENTER(ctx);
+    PBT_TRY(check_lambda(lambda));
+    if (!grad_ampl_far_beam || !grad_ampl_far_ext_diff || !grad_verts ||
+        (nbeam > 0 && !grad_beam_ampl) || (next > 0 && !grad_ext_ampl)) {
+        set_error("adjoint: gradient arrays must not be NULL");
+        return PBT_EINVAL;
+    }
+    PBT_TRY(validate_angles(theta, ntheta, phi, nphi));
+    PBT_TRY(validate_geometry(verts, nverts, face_off, face_vi, nfaces));
+    PBT_TRY(validate_outbeams(beam, nbeam, nfaces, "beam"));
+    PBT_TRY(validate_outbeams(ext, next, nfaces, "external diffraction"));
+    PBT_TRY(grid_prepare(ctx, theta, ntheta, phi, nphi, st));
+    PBT_TRY(check_grid_ready(ctx));
+    return k4_adjoint(ctx, st, beam, nbeam, ext, next, verts, nverts, face_off, face_vi, nfaces,
+                      lambda, is_fast_diff ? 1 : 0, grad_ampl_far_beam, grad_ampl_far_ext_diff,
+                      grad_verts, grad_beam_ampl, grad_ext_ampl);
+}

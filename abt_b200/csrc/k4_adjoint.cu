@@ -1,0 +1,720 @@
+// k4_adjoint.cu -- gradients of the FP32 far-field amplitudes (the adjoint).
+//
+// For one orientation the FP32 far-field sum (k2_fp32.cu) maps the facet
+// vertices and the beam amplitude matrices to the amplitude grids
+// ampl_far_beam / ampl_far_ext_diff.  Given the cotangents of those grids
+// (dL/dRe + i dL/dIm, e.g. from a Mueller-matrix loss), this file computes
+// dL/d(vertex coordinates) and dL/d(amplitude matrices): the vector-Jacobian
+// product of the forward, with the beam topology (which facets emit, their
+// propagation and e-perp directions, the anti-parallel sign and the
+// field-of-view masks) held fixed.
+//
+// The forward is restated in terms of the facet centre c, the vertices in the
+// aperture frame (xa_j, ya_j) and the frame R = [x; y; z] itself, where z = -n
+// with n = unit((v1-c) x (v2-c)), x = unit(p - (p.n) n) and y = z x x: that is
+// the frame the reference builds from angles (src/diff_mod.f90:200-289,
+// 540-559).  Per facet x bin the kernel recomputes the forward quantities and
+// back-propagates; everything that depends on the bin only through a linear
+// map of per-facet data is accumulated as a per-facet sum over bins (35
+// floats), so no facet x bin intermediate is stored.  A host pass in FP64 then
+// maps those sums through the frame construction to the vertex gradients.
+//
+// Layout: one warp per record (4 per CTA), lanes striding over a range of
+// bins with the 35 sums in registers; one warp reduction and one FP64 atomic
+// per (record, bin range) at the end.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "frame.h"
+#include "pbt_internal.h"
+
+namespace pbt {
+
+namespace {
+
+constexpr int K4_WARPS = 4;     // records per CTA, one per warp
+constexpr int64_t K4_MAX_LANE_BINS = 1024;  // FP32 terms per lane and accumulator
+constexpr int K4_NACC = 35;     // per-record accumulators
+constexpr double kTwoPi4 = 6.283185307179586;
+constexpr double kInv2Pi4 = 0.15915494309189535;
+constexpr double kMagic4 = 6755399441055744.0;
+constexpr float kClampSq4 = (float)(1.0 - (double)0.999999f * (double)0.999999f);
+
+// accumulator layout
+enum {
+    A_AMP = 0,     // 8: cotangent of amp' (re, im) x 4
+    A_TKX = 8,     // 3: sum theta_bar_j * kxx
+    A_TKY = 11,    // 3: sum theta_bar_j * kyy
+    A_WU = 14,     // 9: sum w_bar (x) u   (row-major, R_bar contribution)
+    A_EA = 23,     // 3: sum ea_bar
+    A_P2 = 26,     // 3: prop2 cotangent
+    A_INC = 29,    // 3: incidence-in-frame cotangent
+    A_C = 32,      // 3: c cotangent (lab)
+};
+
+struct K4Rec {
+    double kc[3];
+    float eps[3], b, R[9], ea[3], kp[2], p2[3], cf, inc[3], xa[3], ya[3], amp[8];
+};
+
+struct Bin4 {
+    double ux, uy, uz;
+    float fx, fy, fz, hx, hy, hz;
+    float G[8];  // cotangent of S' (pre-T, common phase removed) for the record's kind
+};
+
+__device__ __forceinline__ float rcp4(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// sinc(h) and sinc'(h) for h >= 0
+__device__ __forceinline__ void sinc_d(float h, float &sc, float &dsc) {
+    if (h < 0.5f) {
+        const float h2 = h * h;
+        sc = fmaf(h2, fmaf(h2, fmaf(h2, fmaf(h2, 2.7557319e-6f, -1.9841270e-4f), 8.3333333e-3f),
+                           -1.6666667e-1f),
+                  1.0f);
+        // d/dh (sin h / h) = -h/3 + h^3/30 - h^5/840 + h^7/45360
+        dsc = h * fmaf(h2, fmaf(h2, fmaf(h2, 2.2045855e-5f, -1.1904762e-3f), 3.3333333e-2f),
+                       -0.33333333f);
+    } else {
+        float s, c;
+        __sincosf(h, &s, &c);
+        const float r = rcp4(h);
+        sc = s * r;
+        dsc = (c - sc) * r;
+    }
+}
+
+// g = second divided difference of e^{ix} at t[0..2] and dg/dt_j.
+__device__ __forceinline__ void dd_grad(const float t[3], float2 &g, float2 dg[3]) {
+    // sort with indices
+    int i0 = 0, i1 = 1, i2 = 2;
+    if (t[i1] < t[i0]) { int q = i0; i0 = i1; i1 = q; }
+    if (t[i2] < t[i1]) { int q = i1; i1 = i2; i2 = q; }
+    if (t[i1] < t[i0]) { int q = i0; i0 = i1; i1 = q; }
+    const float lo = t[i0], mid = t[i1], hi = t[i2];
+    const float D = hi - lo;
+    float2 dlo, dmid, dhi;
+    if (D >= 0.25f) {
+        const float h1 = 0.5f * (mid - lo), h2 = 0.5f * (hi - mid);
+        float s1, c1, s2, c2;
+        __sincosf(lo + h1, &s1, &c1);
+        __sincosf(mid + h2, &s2, &c2);
+        float sc1, dsc1, sc2, dsc2;
+        sinc_d(h1, sc1, dsc1);
+        sinc_d(h2, sc2, dsc2);
+        const float iD = rcp4(D);
+        // E = i e^{ic} sinc(h): (-s sc, c sc); dE/dc = i E; dE/dh = i e^{ic} sinc'(h)
+        const float2 E1 = make_float2(-s1 * sc1, c1 * sc1), E2 = make_float2(-s2 * sc2, c2 * sc2);
+        const float2 iE1 = make_float2(-E1.y, E1.x), iE2 = make_float2(-E2.y, E2.x);
+        const float2 H1 = make_float2(-s1 * dsc1, c1 * dsc1), H2 = make_float2(-s2 * dsc2, c2 * dsc2);
+        g = make_float2((E2.x - E1.x) * iD, (E2.y - E1.y) * iD);
+        // d g1/d lo = (iE1 - H1)/2, d g1/d mid = (iE1 + H1)/2, d g2/d mid = (iE2 - H2)/2, d g2/d hi = (iE2 + H2)/2
+        dlo = make_float2((-(0.5f * (iE1.x - H1.x)) + g.x) * iD, (-(0.5f * (iE1.y - H1.y)) + g.y) * iD);
+        dmid = make_float2((0.5f * (iE2.x - H2.x) - 0.5f * (iE1.x + H1.x)) * iD,
+                           (0.5f * (iE2.y - H2.y) - 0.5f * (iE1.y + H1.y)) * iD);
+        dhi = make_float2((0.5f * (iE2.x + H2.x) - g.x) * iD, (0.5f * (iE2.y + H2.y) - g.y) * iD);
+    } else {
+        // series about mid: g = e^{i mid} sum_n c_n h_n(ya, yc)
+        const float ya = lo - mid, yc = hi - mid;
+        float hq[8], da[8], dc[8], yap[8];
+        yap[0] = 1.0f;
+        for (int n = 1; n < 8; n++) yap[n] = yap[n - 1] * ya;
+        hq[0] = 1.0f;
+        da[0] = 0.0f;
+        dc[0] = 0.0f;
+        for (int n = 1; n < 8; n++) {
+            hq[n] = fmaf(yc, hq[n - 1], yap[n]);
+            da[n] = fmaf(yc, da[n - 1], (float)n * yap[n - 1]);
+            dc[n] = fmaf(yc, dc[n - 1], hq[n - 1]);
+        }
+        // c_n = i^(n+2)/(n+2)!
+        const float cr[8] = {-0.5f, 0.0f, 1.0f / 24.0f, 0.0f, -1.0f / 720.0f, 0.0f, 1.0f / 40320.0f, 0.0f};
+        const float ci[8] = {0.0f, -1.0f / 6.0f, 0.0f, 1.0f / 120.0f, 0.0f, -1.0f / 5040.0f, 0.0f,
+                             1.0f / 362880.0f};
+        float2 sg = make_float2(0, 0), sa = make_float2(0, 0), sc = make_float2(0, 0);
+        for (int n = 0; n < 8; n++) {
+            sg.x = fmaf(cr[n], hq[n], sg.x);
+            sg.y = fmaf(ci[n], hq[n], sg.y);
+            sa.x = fmaf(cr[n], da[n], sa.x);
+            sa.y = fmaf(ci[n], da[n], sa.y);
+            sc.x = fmaf(cr[n], dc[n], sc.x);
+            sc.y = fmaf(ci[n], dc[n], sc.y);
+        }
+        float sm, cm;
+        __sincosf(mid, &sm, &cm);
+        auto rot = [&](float2 z) { return make_float2(cm * z.x - sm * z.y, cm * z.y + sm * z.x); };
+        g = rot(sg);
+        dlo = rot(sa);
+        dhi = rot(sc);
+        // shift identity: sum_j dg/dt_j = i g
+        dmid = make_float2(-g.y - dlo.x - dhi.x, g.x - dlo.y - dhi.y);
+    }
+    dg[i0] = dlo;
+    dg[i1] = dmid;
+    dg[i2] = dhi;
+}
+
+// Bin direction from the facet centre in the aperture frame (second order in c/R)
+struct Dir4 {
+    float a, b, opa, opa2, w[3], k[3];
+};
+__device__ __forceinline__ Dir4 dir4(const K4Rec &r, float fx, float fy, float fz) {
+    Dir4 d;
+    d.a = fmaf(fz, r.eps[2], fmaf(fy, r.eps[1], fx * r.eps[0]));
+    d.b = r.b;
+    d.opa = 1.0f + d.a;
+    d.opa2 = fmaf(d.a, fmaf(1.5f, d.a, 1.0f), fmaf(-0.5f, r.b, 1.0f));
+    for (int i = 0; i < 3; i++) {
+        d.w[i] = fmaf(r.R[3 * i + 2], fz, fmaf(r.R[3 * i + 1], fy, r.R[3 * i] * fx));
+        d.k[i] = fmaf(d.w[i], d.opa2, -r.ea[i] * d.opa);
+    }
+    return d;
+}
+
+// Back-propagate a cotangent kb of the aperture-frame direction into the
+// accumulators (frame outer product, ea, c).
+__device__ __forceinline__ void dir4_back(const K4Rec &r, const Dir4 &d, const float kb[3], float fx,
+                                          float fy, float fz, float *acc, float Rf) {
+    const float u[3] = {fx, fy, fz};
+    float opa2b = 0.0f, opab = 0.0f;
+    for (int i = 0; i < 3; i++) {
+        const float wb = kb[i] * d.opa2;
+        opa2b = fmaf(kb[i], d.w[i], opa2b);
+        opab = fmaf(-kb[i], r.ea[i], opab);
+        for (int j = 0; j < 3; j++) acc[A_WU + 3 * i + j] = fmaf(wb, u[j], acc[A_WU + 3 * i + j]);
+        acc[A_EA + i] = fmaf(-kb[i], d.opa, acc[A_EA + i]);
+    }
+    const float ab = opab + opa2b * fmaf(3.0f, d.a, 1.0f);
+    const float bb = -0.5f * opa2b;
+    // a = u.c / R ; b = |c|^2 / R^2, with c = eps * R
+    for (int j = 0; j < 3; j++)
+        acc[A_C + j] = fmaf(ab, u[j] / Rf, fmaf(bb, 2.0f * r.eps[j] / Rf, acc[A_C + j]));
+}
+
+// Cotangent contributions of one (record, bin).
+template <bool FAST>
+__device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, float hkR, float Rf,
+                                        float cosfov, const float *p0, float *acc) {
+    // forward
+    const double ka = fma(B.uz, r.kc[2], fma(B.uy, r.kc[1], B.ux * r.kc[0]));
+    const double nq = fma(ka, kInv2Pi4, kMagic4) - kMagic4;
+    const float rf = (float)fma(-nq, kTwoPi4, ka);
+    const Dir4 d = dir4(r, B.fx, B.fy, B.fz);
+    if (FAST) {
+        const float dx = fmaf(B.fx, d.opa, -r.eps[0]), dy = fmaf(B.fy, d.opa, -r.eps[1]),
+                    dz = fmaf(B.fz, d.opa, -r.eps[2]);
+        if (fmaf(dz, p0[2], fmaf(dy, p0[1], dx * p0[0])) < cosfov) return;
+    }
+    const float ph = fmaf(hkR * fmaf(-d.a, d.a, r.b), d.opa, -rf);
+    const float kx = d.k[0], ky = d.k[1], kz = d.k[2];
+    const float kxx = fmaf(-k, kx, r.kp[0]), kyy = fmaf(-k, ky, r.kp[1]);
+    float t[3];
+    for (int j = 0; j < 3; j++) t[j] = fmaf(kyy, r.ya[j], fmaf(kxx, r.xa[j], ph));
+    float2 g, dg[3];
+    dd_grad(t, g, dg);
+    const float Kx = r.p2[0], Ky = r.p2[1], Kz = r.p2[2], cf = r.cf;
+    const bool yclamp = !(fabsf(ky) <= 0.999999f);
+    const float kyc = fminf(fmaxf(ky, -0.999999f), 0.999999f);
+    const float traw = fmaf(kx, kx, kz * kz);
+    const bool floored = !(traw > kClampSq4);
+    const float tt = floored ? kClampSq4 : traw;
+    const float rs = rsqrtf(tt), s = tt * rs;
+    const float m[3] = {-kx * kyc * rs, s, -kz * kyc * rs};
+    const float dd = fmaf(-0.5f * Kz * cf, s, -0.5f * kz * rs / cf);
+    const float ee = fmaf(0.5f * Kx * Ky * cf, s, -0.5f * kx * kyc * rs / cf);
+    const float kc3[3] = {kx, kyc, kz};
+    const float dinc = fmaf(r.inc[2], kz, fmaf(r.inc[1], kyc, r.inc[0] * kx));
+    const bool bodge = !(fabsf(dinc) < 0.999f);
+    Dir4 dh;
+    float q[3] = {kx, kyc, kz};
+    if (bodge) {
+        dh = dir4(r, B.hx, B.hy, B.hz);
+        q[0] = dh.k[0];
+        q[1] = dh.k[1];
+        q[2] = dh.k[2];
+    }
+    const float hr[3] = {fmaf(r.inc[1], q[2], -r.inc[2] * q[1]), fmaf(r.inc[2], q[0], -r.inc[0] * q[2]),
+                         fmaf(r.inc[0], q[1], -r.inc[1] * q[0])};
+    const float hn = rsqrtf(fmaf(hr[2], hr[2], fmaf(hr[1], hr[1], hr[0] * hr[0])));
+    const float hc[3] = {hr[0] * hn, hr[1] * hn, hr[2] * hn};
+    const float vr[3] = {fmaf(kyc, m[2], -kz * m[1]), fmaf(kz, m[0], -kx * m[2]), fmaf(kx, m[1], -kyc * m[0])};
+    float vn = 1.0f;
+    if (floored) vn = rsqrtf(fmaf(vr[2], vr[2], fmaf(vr[1], vr[1], vr[0] * vr[0])));
+    const float ev[3] = {vr[0] * vn, vr[1] * vn, vr[2] * vn};
+    const float pp = fmaf(hc[2], m[2], fmaf(hc[1], m[1], hc[0] * m[0]));
+    const float rr = fmaf(hc[2], ev[2], fmaf(hc[1], ev[1], hc[0] * ev[0]));
+    const float A = fmaf(pp, dd, rr * ee), Bm = fmaf(pp, ee, -rr * dd);
+    // W = [[A, B], [-B, A]] amp' ; order (1,1),(2,1),(1,2),(2,2)
+    const float *a = r.amp;
+    float W[8];
+    W[0] = fmaf(A, a[0], Bm * a[2]);
+    W[1] = fmaf(A, a[1], Bm * a[3]);
+    W[2] = fmaf(A, a[2], -Bm * a[0]);
+    W[3] = fmaf(A, a[3], -Bm * a[1]);
+    W[4] = fmaf(A, a[4], Bm * a[6]);
+    W[5] = fmaf(A, a[5], Bm * a[7]);
+    W[6] = fmaf(A, a[6], -Bm * a[4]);
+    W[7] = fmaf(A, a[7], -Bm * a[5]);
+    // backward.  C = g W:  g_bar = sum G conj(W), W_bar = G conj(g)
+    float2 gb = make_float2(0, 0);
+    float Wb[8];
+    for (int c = 0; c < 4; c++) {
+        const float Gr = B.G[2 * c], Gi = B.G[2 * c + 1], wr = W[2 * c], wi = W[2 * c + 1];
+        gb.x = fmaf(Gr, wr, fmaf(Gi, wi, gb.x));
+        gb.y = fmaf(Gi, wr, fmaf(-Gr, wi, gb.y));
+        Wb[2 * c] = fmaf(Gr, g.x, Gi * g.y);
+        Wb[2 * c + 1] = fmaf(Gi, g.x, -Gr * g.y);
+    }
+    // A_bar, B_bar = Re sum conj(W_bar) dW/dA|B ; amp'_bar = M^T W_bar
+    auto rdot = [&](int wi, int ai) { return fmaf(Wb[2 * wi], a[2 * ai], Wb[2 * wi + 1] * a[2 * ai + 1]); };
+    const float Ab = rdot(0, 0) + rdot(1, 1) + rdot(2, 2) + rdot(3, 3);
+    const float Bb = rdot(0, 1) - rdot(1, 0) + rdot(2, 3) - rdot(3, 2);
+    for (int z = 0; z < 2; z++) {
+        acc[A_AMP + 0 + z] += fmaf(A, Wb[0 + z], -Bm * Wb[2 + z]);
+        acc[A_AMP + 2 + z] += fmaf(Bm, Wb[0 + z], A * Wb[2 + z]);
+        acc[A_AMP + 4 + z] += fmaf(A, Wb[4 + z], -Bm * Wb[6 + z]);
+        acc[A_AMP + 6 + z] += fmaf(Bm, Wb[4 + z], A * Wb[6 + z]);
+    }
+    // A = pp dd + rr ee, B = pp ee - rr dd
+    const float ppb = fmaf(Ab, dd, Bb * ee), rrb = fmaf(Ab, ee, -Bb * dd);
+    const float ddb = fmaf(Ab, pp, -Bb * rr), eeb = fmaf(Ab, rr, Bb * pp);
+    float hcb[3], mb[3], evb[3];
+    for (int i = 0; i < 3; i++) {
+        hcb[i] = fmaf(ppb, m[i], rrb * ev[i]);
+        mb[i] = ppb * hc[i];
+        evb[i] = rrb * hc[i];
+    }
+    // ev = vr * vn (normalised only when floored)
+    float vrb[3];
+    if (floored) {
+        const float dp = evb[0] * ev[0] + evb[1] * ev[1] + evb[2] * ev[2];
+        for (int i = 0; i < 3; i++) vrb[i] = (evb[i] - dp * ev[i]) * vn;
+    } else {
+        for (int i = 0; i < 3; i++) vrb[i] = evb[i];
+    }
+    // vr = kc3 x m
+    float kcb[3];
+    kcb[0] = m[1] * vrb[2] - m[2] * vrb[1];
+    kcb[1] = m[2] * vrb[0] - m[0] * vrb[2];
+    kcb[2] = m[0] * vrb[1] - m[1] * vrb[0];
+    mb[0] += vrb[1] * kc3[2] - vrb[2] * kc3[1];
+    mb[1] += vrb[2] * kc3[0] - vrb[0] * kc3[2];
+    mb[2] += vrb[0] * kc3[1] - vrb[1] * kc3[0];
+    // hc = hr * hn ; hr = inc x q
+    float hrb[3];
+    {
+        const float dp = hcb[0] * hc[0] + hcb[1] * hc[1] + hcb[2] * hc[2];
+        for (int i = 0; i < 3; i++) hrb[i] = (hcb[i] - dp * hc[i]) * hn;
+    }
+    float qb[3];
+    qb[0] = hrb[1] * r.inc[2] - hrb[2] * r.inc[1];
+    qb[1] = hrb[2] * r.inc[0] - hrb[0] * r.inc[2];
+    qb[2] = hrb[0] * r.inc[1] - hrb[1] * r.inc[0];
+    acc[A_INC + 0] += q[1] * hrb[2] - q[2] * hrb[1];
+    acc[A_INC + 1] += q[2] * hrb[0] - q[0] * hrb[2];
+    acc[A_INC + 2] += q[0] * hrb[1] - q[1] * hrb[0];
+    if (bodge) {
+        dir4_back(r, dh, qb, B.hx, B.hy, B.hz, acc, Rf);
+    } else {
+        kcb[0] += qb[0];
+        kcb[1] += qb[1];
+        kcb[2] += qb[2];
+    }
+    // Karczewski-Wolf: m = (-kx kyc rs, s, -kz kyc rs), dd, ee as above
+    float kxb = kcb[0], kycb = kcb[1], kzb = kcb[2];
+    const float rcf = 1.0f / cf;
+    kxb += mb[0] * (-kyc * rs) + eeb * (-0.5f * kyc * rs * rcf);
+    kycb += mb[0] * (-kx * rs) + mb[2] * (-kz * rs) + eeb * (-0.5f * kx * rs * rcf);
+    kzb += mb[2] * (-kyc * rs) + ddb * (-0.5f * rs * rcf);
+    const float rs2 = rs * rs;
+    const float sb = mb[0] * (kx * kyc * rs2) + mb[2] * (kz * kyc * rs2) + mb[1] +
+                     ddb * fmaf(-0.5f * Kz, cf, 0.5f * kz * rs2 * rcf) +
+                     eeb * fmaf(0.5f * Kx * Ky, cf, 0.5f * kx * kyc * rs2 * rcf);
+    const float cfb = ddb * fmaf(-0.5f * Kz, s, 0.5f * kz * rs * rcf * rcf) +
+                      eeb * fmaf(0.5f * Kx * Ky, s, 0.5f * kx * kyc * rs * rcf * rcf);
+    acc[A_P2 + 2] += ddb * (-0.5f * cf * s);
+    acc[A_P2 + 0] += eeb * (0.5f * Ky * cf * s);
+    acc[A_P2 + 1] += eeb * (0.5f * Kx * cf * s) + cfb * Ky * cf * cf * cf;
+    if (!floored) {
+        const float ttb = 0.5f * sb * rs;  // s = sqrt(tt)
+        kxb = fmaf(2.0f * kx, ttb, kxb);
+        kzb = fmaf(2.0f * kz, ttb, kzb);
+    }
+    float kyb = yclamp ? 0.0f : kycb;
+    // phases: t_j = ph + kxx xa_j + kyy ya_j
+    float phb = 0.0f, kxxb = 0.0f, kyyb = 0.0f;
+    for (int j = 0; j < 3; j++) {
+        const float tb = fmaf(gb.x, dg[j].x, gb.y * dg[j].y);  // Re(conj(g_bar) dg/dt_j)
+        phb += tb;
+        kxxb = fmaf(tb, r.xa[j], kxxb);
+        kyyb = fmaf(tb, r.ya[j], kyyb);
+        acc[A_TKX + j] = fmaf(tb, kxx, acc[A_TKX + j]);
+        acc[A_TKY + j] = fmaf(tb, kyy, acc[A_TKY + j]);
+    }
+    // kxx = k p2x - k kx ; kyy = k p2y - k ky
+    kxb = fmaf(-k, kxxb, kxb);
+    kyb = fmaf(-k, kyyb, kyb);
+    acc[A_P2 + 0] = fmaf(k, kxxb, acc[A_P2 + 0]);
+    acc[A_P2 + 1] = fmaf(k, kyyb, acc[A_P2 + 1]);
+    // ph = hkR (b - a^2)(1 + a) - rf ; rf = k u.c (mod 2 pi)
+    {
+        const float dpa = hkR * fmaf(-2.0f * d.a, d.opa, fmaf(-d.a, d.a, r.b));
+        const float dpb = hkR * d.opa;
+        const float u[3] = {B.fx, B.fy, B.fz};
+        for (int j = 0; j < 3; j++)
+            acc[A_C + j] += phb * (fmaf(-k, u[j], dpa * u[j] / Rf) + dpb * 2.0f * r.eps[j] / Rf);
+    }
+    const float kb3[3] = {kxb, kyb, kzb};
+    dir4_back(r, d, kb3, B.fx, B.fy, B.fz, acc, Rf);
+}
+
+// One warp per record, K4_WARPS records per CTA; blockIdx.y selects a range
+// of bins.  Each lane walks the range with stride 32 and keeps the 35 sums of
+// its record in registers (FP32, at most K4_MAX_LANE_BINS terms), so the warp
+// reduction and the FP64 atomic into out[record][35] happen once per
+// (record, range).  The warps of a CTA walk the same bins, which the L1 serves.
+template <bool FAST>
+__global__ void __launch_bounds__(K4_WARPS * 32) k4_adjoint_kernel(
+    const K4Rec *__restrict__ recs, const int *__restrict__ kinds, const float *__restrict__ fovdat,
+    int64_t nrec, const double *__restrict__ ud, const float *__restrict__ uh,
+    const float *__restrict__ gbin, int64_t nb, int64_t chunk, float k, float hkR, float Rf,
+    double *__restrict__ out) {
+    __shared__ K4Rec s_rec[K4_WARPS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t rec = (int64_t)blockIdx.x * K4_WARPS + warp;
+    if (rec >= nrec) return;  // whole warp; no block-wide barrier follows
+    {
+        const float *src = reinterpret_cast<const float *>(recs + rec);
+        float *dst = reinterpret_cast<float *>(&s_rec[warp]);
+        for (int i = lane; i < (int)(sizeof(K4Rec) / 4); i += 32) dst[i] = src[i];
+        __syncwarp();
+    }
+    const K4Rec &r = s_rec[warp];
+    const int kd = kinds[rec];
+    const float *G = gbin + (int64_t)kd * 8 * nb;
+    float cosfov = 0.0f, p0[3] = {0.0f, 0.0f, 0.0f};
+    if (FAST) {
+        p0[0] = fovdat[4 * rec];
+        p0[1] = fovdat[4 * rec + 1];
+        p0[2] = fovdat[4 * rec + 2];
+        cosfov = fovdat[4 * rec + 3];
+    }
+    float acc[K4_NACC];
+#pragma unroll
+    for (int q = 0; q < K4_NACC; q++) acc[q] = 0.0f;
+    const int64_t o0 = (int64_t)blockIdx.y * chunk, o1 = min(nb, o0 + chunk);
+    for (int64_t o = o0 + lane; o < o1; o += 32) {
+        Bin4 B;
+        B.ux = ud[o];
+        B.uy = ud[nb + o];
+        B.uz = ud[2 * nb + o];
+        B.fx = (float)B.ux;
+        B.fy = (float)B.uy;
+        B.fz = (float)B.uz;
+        B.hx = uh[o];
+        B.hy = uh[nb + o];
+        B.hz = uh[2 * nb + o];
+#pragma unroll
+        for (int c = 0; c < 8; c++) B.G[c] = G[c * nb + o];
+        k4_eval<FAST>(r, B, k, hkR, Rf, cosfov, p0, acc);
+    }
+#pragma unroll
+    for (int q = 0; q < K4_NACC; q++) {
+        float v = acc[q];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == (q & 31)) atomicAdd(&out[rec * K4_NACC + q], (double)v);
+    }
+}
+
+// Per-bin inputs of the adjoint: the unit bin direction (FP64), the unit
+// direction of the same-phi bin on the first row above 1 degree (used by the
+// forward-scattering rotation), and the cotangent of S' (pre-T, common phase
+// removed): G' = conj(e^{ik|X|}) G T^T, per kind.
+__global__ void k4_prep_kernel(const double *__restrict__ gafb, const double *__restrict__ gafe,
+                               const double *__restrict__ xyz, const double *__restrict__ phitab,
+                               int64_t nb, int64_t nphi, int64_t theta_i, double k,
+                               double *__restrict__ ud, float *__restrict__ uh,
+                               float *__restrict__ gbin) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nb) return;
+    const double cp = phitab[o % nphi], sp = phitab[nphi + o % nphi];
+    const double X = xyz[o], Y = xyz[nb + o], Zc = xyz[2 * nb + o];
+    const double rho = sqrt(X * X + Y * Y + Zc * Zc), ir = 1.0 / rho;
+    ud[o] = X * ir;
+    ud[nb + o] = Y * ir;
+    ud[2 * nb + o] = Zc * ir;
+    const int64_t oh = (o % nphi) + nphi * theta_i;
+    const double Xh = xyz[oh], Yh = xyz[nb + oh], Zh = xyz[2 * nb + oh];
+    const double irh = 1.0 / sqrt(Xh * Xh + Yh * Yh + Zh * Zh);
+    uh[o] = (float)(Xh * irh);
+    uh[nb + o] = (float)(Yh * irh);
+    uh[2 * nb + o] = (float)(Zh * irh);
+    double sK, cK;
+    sincos(k * rho, &sK, &cK);
+    const double T11 = -sp, T12 = -cp, T21 = cp, T22 = -sp;
+    for (int kd = 0; kd < 2; kd++) {
+        const double *Gc = kd ? gafe : gafb;
+        double gr[4], gi[4];  // (1,1),(2,1),(1,2),(2,2), times conj(e^{iK})
+        for (int c = 0; c < 4; c++) {
+            const double re = Gc[2 * (o + nb * c)], im = Gc[2 * (o + nb * c) + 1];
+            gr[c] = re * cK + im * sK;
+            gi[c] = im * cK - re * sK;
+        }
+        // S = S' T  ->  S'_bar = S_bar T^T : S'(a,1) <- S(a,1) T11 + S(a,2) T12, S'(a,2) <- S(a,1) T21 + S(a,2) T22
+        const double o11r = gr[0] * T11 + gr[2] * T12, o11i = gi[0] * T11 + gi[2] * T12;
+        const double o21r = gr[1] * T11 + gr[3] * T12, o21i = gi[1] * T11 + gi[3] * T12;
+        const double o12r = gr[0] * T21 + gr[2] * T22, o12i = gi[0] * T21 + gi[2] * T22;
+        const double o22r = gr[1] * T21 + gr[3] * T22, o22i = gi[1] * T21 + gi[3] * T22;
+        const double v[8] = {o11r, o11i, o21r, o21i, o12r, o12i, o22r, o22i};
+        for (int c = 0; c < 8; c++) gbin[(kd * 8 + c) * nb + o] = (float)v[c];
+    }
+}
+
+}  // namespace
+
+// Host side: set-up per triangle (FP64, libm), the kernel, and the FP64
+// mapping of the per-record sums to vertex and amplitude gradients.
+int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t nbeam,
+               const pbt_outbeam *ext, int64_t next, const double *verts, int64_t nverts,
+               const int64_t *face_off, const int64_t *face_vi, int64_t nfaces, double lambda,
+               int fast_diff, const double *gafb, const double *gafe, double *gverts,
+               double *gbeam, double *gext) {
+    const GridCache &g = ctx->grid;
+    const int64_t nb = g.nb, nphi = (int64_t)g.phi.size();
+    const double k = 2.0 * kPiRef / lambda, Rf = kFarR;
+    const int64_t nrec = nbeam + next;
+    struct Host4 {
+        double c[3], e[3][3], R[3][3], p[3], As, sign;
+        int64_t vi[3];
+    };
+    std::vector<K4Rec> recs(nrec);
+    std::vector<int> kinds(nrec);
+    std::vector<float> fovd(4 * nrec);
+    std::vector<Host4> H(nrec);
+    for (int64_t q = 0; q < nrec; q++) {
+        const pbt_outbeam &ob = q < nbeam ? beam[q] : ext[q - nbeam];
+        const int64_t fb = face_off[ob.fi - 1];
+        if (face_off[ob.fi] - fb != 3) {
+            set_error("the adjoint supports triangular facets only (outbeam %lld, face %lld)",
+                      (long long)(q + 1), (long long)ob.fi);
+            return PBT_EINVAL;
+        }
+        double vx[3], vy[3], vz[3], rx[3], ry[3], rz[3];
+        for (int i = 0; i < 3; i++) {
+            const int64_t vi = face_vi[fb + i] - 1;
+            H[q].vi[i] = vi;
+            vx[i] = verts[vi];
+            vy[i] = verts[vi + nverts];
+            vz[i] = verts[vi + 2 * nverts];
+        }
+        FacetFrame fr;
+        fr.sign = 1.0;
+        facet_frame(vx, vy, vz, 3, ob.prop_out, ob.vk7, fr, rx, ry, rz);
+        K4Rec &r = recs[q];
+        Host4 &h = H[q];
+        kinds[q] = q < nbeam ? 0 : 1;
+        double ea[3], xa[3], ya[3];
+        mv33(fr.R, fr.com, ea);
+        for (int i = 0; i < 3; i++) {
+            const double d[3] = {rx[i], ry[i], rz[i]};
+            double a3[3];
+            mv33(fr.R, d, a3);
+            xa[i] = a3[0];
+            ya[i] = a3[1];
+            h.e[i][0] = rx[i];
+            h.e[i][1] = ry[i];
+            h.e[i][2] = rz[i];
+        }
+        const double As = 0.5 * ((xa[1] - xa[0]) * (ya[2] - ya[0]) - (xa[2] - xa[0]) * (ya[1] - ya[0]));
+        const double cpre = 2.0 * As / lambda * fr.sign;
+        for (int c = 0; c < 3; c++) {
+            r.kc[c] = k * fr.com[c];
+            r.eps[c] = (float)(fr.com[c] / Rf);
+            r.ea[c] = (float)(ea[c] / Rf);
+            r.p2[c] = (float)fr.prop2[c];
+            r.inc[c] = (float)fr.inc2[c];
+            r.xa[c] = (float)xa[c];
+            r.ya[c] = (float)ya[c];
+            h.c[c] = fr.com[c];
+            h.p[c] = ob.prop_out[c];
+        }
+        r.b = (float)((fr.com[0] * fr.com[0] + fr.com[1] * fr.com[1] + fr.com[2] * fr.com[2]) / (Rf * Rf));
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                r.R[3 * a + b] = (float)fr.R.m[a][b];
+                h.R[a][b] = fr.R.m[a][b];
+            }
+        r.kp[0] = (float)(k * fr.prop2[0]);
+        r.kp[1] = (float)(k * fr.prop2[1]);
+        r.cf = (float)(1.0 / sqrt(1.0 - fr.prop2[1] * fr.prop2[1]));
+        for (int c = 0; c < 4; c++) {
+            r.amp[2 * c] = (float)(-cpre * ob.ampl[2 * c + 1]);
+            r.amp[2 * c + 1] = (float)(cpre * ob.ampl[2 * c]);
+        }
+        h.As = As;
+        h.sign = fr.sign;
+        const double fov = q < nbeam ? ob.fov : kPiRef / 2.0;
+        fovd[4 * q + 0] = (float)ob.prop_out[0];
+        fovd[4 * q + 1] = (float)ob.prop_out[1];
+        fovd[4 * q + 2] = (float)ob.prop_out[2];
+        fovd[4 * q + 3] = (float)cos(fov);
+    }
+    // device buffers: recs | kinds | fov | gafb | gafe | ud | uh | gbin | out
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t o_rec = 0, o_kind = al(nrec * sizeof(K4Rec)), o_fov = al(o_kind + nrec * 4),
+                 o_ga = al(o_fov + 16 * nrec), o_gb = al(o_ga + 8 * nb * 8),
+                 o_ud = al(o_gb + 8 * nb * 8), o_uh = al(o_ud + 3 * nb * 8),
+                 o_gbin = al(o_uh + 3 * nb * 4), o_out = al(o_gbin + 16 * nb * 4),
+                 o_end = al(o_out + nrec * K4_NACC * 8);
+    PBT_TRY(ctx->d_ws.ensure(o_end));
+    char *base = ctx->d_ws.as<char>();
+    if (nrec > 0) {
+        PBT_CUDA_TRY(cudaMemcpyAsync(base + o_rec, recs.data(), nrec * sizeof(K4Rec), cudaMemcpyHostToDevice, st));
+        PBT_CUDA_TRY(cudaMemcpyAsync(base + o_kind, kinds.data(), nrec * 4, cudaMemcpyHostToDevice, st));
+        PBT_CUDA_TRY(cudaMemcpyAsync(base + o_fov, fovd.data(), 16 * nrec, cudaMemcpyHostToDevice, st));
+        PBT_CUDA_TRY(cudaMemsetAsync(base + o_out, 0, nrec * K4_NACC * 8, st));
+    }
+    PBT_CUDA_TRY(cudaMemcpyAsync(base + o_ga, gafb, 8 * nb * 8, cudaMemcpyHostToDevice, st));
+    PBT_CUDA_TRY(cudaMemcpyAsync(base + o_gb, gafe, 8 * nb * 8, cudaMemcpyHostToDevice, st));
+    k4_prep_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, st>>>(
+        (const double *)(base + o_ga), (const double *)(base + o_gb), g.xyz.as<double>(),
+        g.phitab.as<double>(), nb, nphi, g.theta_i, k, (double *)(base + o_ud),
+        (float *)(base + o_uh), (float *)(base + o_gbin));
+    // bin ranges: at most K4_MAX_LANE_BINS terms per lane, and enough CTAs
+    // for a few waves when there are few records
+    const int64_t ncta_rec = (nrec + K4_WARPS - 1) / K4_WARPS;
+    int64_t nsplit = (nb + 32 * K4_MAX_LANE_BINS - 1) / (32 * K4_MAX_LANE_BINS);
+    if (ncta_rec > 0) nsplit = std::max(nsplit, (int64_t)(8 * ctx->sm_count + ncta_rec - 1) / ncta_rec);
+    nsplit = std::min(nsplit, std::max<int64_t>(1, nb / 256));
+    nsplit = std::min<int64_t>(nsplit, 65535);
+    const int64_t chunk = (((nb + nsplit - 1) / nsplit) + 31) / 32 * 32;
+    nsplit = (nb + chunk - 1) / chunk;
+    const dim3 grid((unsigned)ncta_rec, (unsigned)nsplit);
+    timing_begin(ctx, st);
+    if (nrec > 0) {
+        if (fast_diff)
+            k4_adjoint_kernel<true><<<grid, K4_WARPS * 32, 0, st>>>(
+                (const K4Rec *)(base + o_rec), (const int *)(base + o_kind), (const float *)(base + o_fov),
+                nrec, (const double *)(base + o_ud), (const float *)(base + o_uh),
+                (const float *)(base + o_gbin), nb, chunk, (float)k, (float)(0.5 * k * Rf), (float)Rf,
+                (double *)(base + o_out));
+        else
+            k4_adjoint_kernel<false><<<grid, K4_WARPS * 32, 0, st>>>(
+                (const K4Rec *)(base + o_rec), (const int *)(base + o_kind), (const float *)(base + o_fov),
+                nrec, (const double *)(base + o_ud), (const float *)(base + o_uh),
+                (const float *)(base + o_gbin), nb, chunk, (float)k, (float)(0.5 * k * Rf), (float)Rf,
+                (double *)(base + o_out));
+    }
+    timing_end(ctx, st);
+    ctx->launches += nrec > 0 ? 2 : 1;
+    PBT_CUDA_TRY(cudaGetLastError());
+    std::vector<double> acc(nrec * K4_NACC);
+    if (nrec > 0)
+        PBT_CUDA_TRY(cudaMemcpyAsync(acc.data(), base + o_out, acc.size() * 8, cudaMemcpyDeviceToHost, st));
+    PBT_CUDA_TRY(cudaStreamSynchronize(st));
+    // FP64 mapping of the per-record sums to the vertices and amplitudes
+    for (int64_t q = 0; q < 3 * nverts; q++) gverts[q] = 0.0;
+    const double inc[3] = {0, 0, -1};
+    for (int64_t q = 0; q < nrec; q++) {
+        const double *A = &acc[q * K4_NACC];
+        const Host4 &h = H[q];
+        const pbt_outbeam &ob = q < nbeam ? beam[q] : ext[q - nbeam];
+        // amplitude: amp' = i cpre ampl -> ampl_bar = conj(i cpre) amp'_bar = -i cpre amp'_bar
+        const double cpre = 2.0 * h.As / lambda * h.sign;
+        double *ga = q < nbeam ? gbeam + 8 * q : gext + 8 * (q - nbeam);
+        double Asb = 0.0;  // d amp' / d As = i (2 sign / lambda) ampl
+        for (int c = 0; c < 4; c++) {
+            const double br = A[A_AMP + 2 * c], bi = A[A_AMP + 2 * c + 1];
+            ga[2 * c] = cpre * bi;
+            ga[2 * c + 1] = -cpre * br;
+            // Re(conj(amp'_bar) * i (2 sign/lambda) ampl)
+            const double ar = ob.ampl[2 * c], ai = ob.ampl[2 * c + 1];
+            Asb += (2.0 * h.sign / lambda) * (br * (-ai) + bi * ar);
+        }
+        // aperture coordinates xa_j = x.e_j, ya_j = y.e_j
+        double xab[3], yab[3];
+        double xa[3], ya[3];
+        for (int j = 0; j < 3; j++) {
+            xa[j] = h.R[0][0] * h.e[j][0] + h.R[0][1] * h.e[j][1] + h.R[0][2] * h.e[j][2];
+            ya[j] = h.R[1][0] * h.e[j][0] + h.R[1][1] * h.e[j][1] + h.R[1][2] * h.e[j][2];
+        }
+        // As = 0.5 ((x1-x0)(y2-y0) - (x2-x0)(y1-y0))
+        const double dAx[3] = {0.5 * (ya[1] - ya[2]), 0.5 * (ya[2] - ya[0]), 0.5 * (ya[0] - ya[1])};
+        const double dAy[3] = {0.5 * (xa[2] - xa[1]), 0.5 * (xa[0] - xa[2]), 0.5 * (xa[1] - xa[0])};
+        for (int j = 0; j < 3; j++) {
+            xab[j] = A[A_TKX + j] + Asb * dAx[j];
+            yab[j] = A[A_TKY + j] + Asb * dAy[j];
+        }
+        // R_bar
+        double Rb[3][3];
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+                Rb[a][b] = A[A_WU + 3 * a + b] + A[A_EA + a] * h.c[b] / Rf +
+                           A[A_INC + a] * inc[b] + A[A_P2 + a] * h.p[b];
+        double eb[3][3];
+        for (int j = 0; j < 3; j++)
+            for (int b = 0; b < 3; b++) {
+                Rb[0][b] += xab[j] * h.e[j][b];
+                Rb[1][b] += yab[j] * h.e[j][b];
+                eb[j][b] = xab[j] * h.R[0][b] + yab[j] * h.R[1][b];
+            }
+        // c_bar = direct + R^T ea_bar / Rf
+        double cb[3];
+        for (int b = 0; b < 3; b++)
+            cb[b] = A[A_C + b] + (h.R[0][b] * A[A_EA + 0] + h.R[1][b] * A[A_EA + 1] + h.R[2][b] * A[A_EA + 2]) / Rf;
+        // frame: z = -n, x = unit(p - (p.n) n), y = z x x
+        double n[3] = {-h.R[2][0], -h.R[2][1], -h.R[2][2]}, xh[3] = {h.R[0][0], h.R[0][1], h.R[0][2]};
+        double zb[3] = {Rb[2][0], Rb[2][1], Rb[2][2]}, xb[3] = {Rb[0][0], Rb[0][1], Rb[0][2]},
+               yb[3] = {Rb[1][0], Rb[1][1], Rb[1][2]};
+        double z[3] = {-n[0], -n[1], -n[2]};
+        // y = z x x: z_bar += x x y_bar, x_bar += y_bar x z
+        zb[0] += xh[1] * yb[2] - xh[2] * yb[1];
+        zb[1] += xh[2] * yb[0] - xh[0] * yb[2];
+        zb[2] += xh[0] * yb[1] - xh[1] * yb[0];
+        xb[0] += yb[1] * z[2] - yb[2] * z[1];
+        xb[1] += yb[2] * z[0] - yb[0] * z[2];
+        xb[2] += yb[0] * z[1] - yb[1] * z[0];
+        const double pn = h.p[0] * n[0] + h.p[1] * n[1] + h.p[2] * n[2];
+        double w[3] = {h.p[0] - pn * n[0], h.p[1] - pn * n[1], h.p[2] - pn * n[2]};
+        const double wl = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+        const double xdot = xb[0] * xh[0] + xb[1] * xh[1] + xb[2] * xh[2];
+        double wb[3];
+        for (int b = 0; b < 3; b++) wb[b] = (xb[b] - xdot * xh[b]) / wl;
+        const double wbn = wb[0] * n[0] + wb[1] * n[1] + wb[2] * n[2];
+        double nb_[3];
+        for (int b = 0; b < 3; b++) nb_[b] = -zb[b] - wbn * h.p[b] - pn * wb[b];
+        // n = N/|N|, N = e0 x e1
+        const double N[3] = {h.e[0][1] * h.e[1][2] - h.e[0][2] * h.e[1][1],
+                             h.e[0][2] * h.e[1][0] - h.e[0][0] * h.e[1][2],
+                             h.e[0][0] * h.e[1][1] - h.e[0][1] * h.e[1][0]};
+        const double Nl = sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
+        const double ndot = nb_[0] * n[0] + nb_[1] * n[1] + nb_[2] * n[2];
+        double Nb[3];
+        for (int b = 0; b < 3; b++) Nb[b] = (nb_[b] - ndot * n[b]) / Nl;
+        // e0_bar += e1 x N_bar ; e1_bar += N_bar x e0
+        eb[0][0] += h.e[1][1] * Nb[2] - h.e[1][2] * Nb[1];
+        eb[0][1] += h.e[1][2] * Nb[0] - h.e[1][0] * Nb[2];
+        eb[0][2] += h.e[1][0] * Nb[1] - h.e[1][1] * Nb[0];
+        eb[1][0] += Nb[1] * h.e[0][2] - Nb[2] * h.e[0][1];
+        eb[1][1] += Nb[2] * h.e[0][0] - Nb[0] * h.e[0][2];
+        eb[1][2] += Nb[0] * h.e[0][1] - Nb[1] * h.e[0][0];
+        // e_j = v_j - c, c = mean(v)
+        double esum[3] = {0, 0, 0};
+        for (int j = 0; j < 3; j++)
+            for (int b = 0; b < 3; b++) esum[b] += eb[j][b];
+        for (int j = 0; j < 3; j++)
+            for (int b = 0; b < 3; b++)
+                gverts[h.vi[j] + nverts * b] += eb[j][b] + (cb[b] - esum[b]) / 3.0;
+    }
+    return PBT_OK;
+}
+
+}  // namespace pbt

@@ -162,6 +162,34 @@ class Context:
                                            out.ctypes.data))
         return out
 
+    def diff_adjoint(self, beam, ext, geometry, theta, phi, lam, grad_ampl_far_beam,
+                     grad_ampl_far_ext_diff, is_fast_diff=False):
+        """Vector-Jacobian product of the FP32 diff_main (pbt_diff_adjoint_c).
+
+        The cotangents are (nphi,ntheta,2,2) complex arrays dL/dRe + i dL/dIm;
+        returns (grad_verts (nverts,3), grad_beam_ampl (nbeam,8),
+        grad_ext_ampl (next,8)), the amplitude gradients as re/im of
+        ampl(1,1),(2,1),(1,2),(2,2) like the records' ampl field."""
+        beam, ext = _ob(beam), _ob(ext)
+        v, fo, fv = _geo(geometry)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        ga = np.asfortranarray(grad_ampl_far_beam, dtype=np.complex128)
+        ge = np.asfortranarray(grad_ampl_far_ext_diff, dtype=np.complex128)
+        shape = (len(phi), len(theta), 2, 2)
+        if ga.shape != shape or ge.shape != shape:
+            raise ValueError(f"cotangent shape must be {shape}")
+        gv = np.zeros((v.shape[0], 3), order="F")
+        gb = np.zeros((max(len(beam), 1), 8))
+        gx = np.zeros((max(len(ext), 1), 8))
+        check(_lib.lib().pbt_diff_adjoint_c(self._h, ptr(beam), len(beam), ptr(ext), len(ext),
+                                            ptr(v), v.shape[0], ptr(fo), ptr(fv), len(fo) - 1,
+                                            ptr(theta), len(theta), ptr(phi), len(phi), float(lam),
+                                            int(bool(is_fast_diff)), ga.ctypes.data,
+                                            ge.ctypes.data, gv.ctypes.data, gb.ctypes.data,
+                                            gx.ctypes.data))
+        return gv, gb[:len(beam)], gx[:len(ext)]
+
     # --------------------------------------------------------- outputs_mod
     def finalise(self, ampl_far_beam, ampl_far_ext_diff, theta, phi, lam, params_in,
                  scaling=False, accumulate=False):

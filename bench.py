@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--adjoint-facets", type=int, default=20000,
+                    help="facet sample for the adjoint / forward kernel-time ratio (0: skip)")
     return ap.parse_args()
 
 
@@ -292,6 +294,29 @@ def main():
                                 "kernel_ms": k64_ms, "call_ms": wall * 1e3,
                                 "e2e_value": len(sub) * nb / wall}
         extra["fp32_vs_fp64_kernel_speedup"] = (work / (kern_ms / max(kern_n, 1) / 1e3)) / r64
+
+    # adjoint (vector-Jacobian product) against the forward, same facets and grid
+    if args.adjoint_facets > 0:
+        sub = beam[:args.adjoint_facets]
+        rng = np.random.default_rng(1)
+        shape = (len(ph), len(th), 2, 2)
+        gA = rng.normal(size=shape) + 1j * rng.normal(size=shape)
+        gZ = np.zeros(shape, np.complex128)
+        ctx.diff_main(sub, None, geo, th, ph, LAM, precision="fp32")
+        ctx.diff_adjoint(sub[:64], None, geo, th, ph, LAM, gA, gZ)
+        ctx.set_kernel_timing(True)
+        ctx.kernel_time_ms()
+        ctx.diff_main(sub, None, geo, th, ph, LAM, precision="fp32")
+        fwd_ms, _ = ctx.kernel_time_ms()
+        t0 = time.perf_counter()
+        ctx.diff_adjoint(sub, None, geo, th, ph, LAM, gA, gZ)
+        adj_call = time.perf_counter() - t0
+        adj_ms, _ = ctx.kernel_time_ms()
+        ctx.set_kernel_timing(False)
+        extra["adjoint"] = {"facets": int(len(sub)), "bins": nb, "forward_kernel_ms": fwd_ms,
+                            "adjoint_kernel_ms": adj_ms, "adjoint_over_forward": adj_ms / fwd_ms,
+                            "adjoint_call_ms": adj_call * 1e3,
+                            "value": len(sub) * nb / (adj_ms / 1e3), "unit": UNIT}
 
     # FP32 error against the FP64 drop-in on the full workload
     if not args.no_error_check:

@@ -119,6 +119,23 @@ int pbt_diffraction_noalloc_c(const pbt_outbeam *outbeam, const double *verts, i
                               const double *theta, int64_t ntheta, const double *phi,
                               int64_t nphi, double lambda, int32_t is_fast_diff, double *amplC);
 
+/* Gradients of the FP32 far-field sum of one orientation: the vector-Jacobian
+ * product of pbt_diff_main_c with PBT_PREC_FP32.  No counterpart in the
+ * reference (it has no derivatives).  Inputs as pbt_diff_main_c plus the
+ * cotangents of its two output grids (dL/dRe + i dL/dIm, reference layout);
+ * outputs dL/dverts (nverts,3) and dL/dampl per outbeam (8 doubles, re/im of
+ * ampl(1,1),(2,1),(1,2),(2,2)).  The beam topology (which facets emit, their
+ * directions, anti-parallel sign and field-of-view masks) is held fixed.
+ * Triangular facets only.  Phase terms are recomputed per facet x bin; no
+ * facet x bin intermediate is stored. */
+int pbt_diff_adjoint_c(pbt_ctx *ctx, const pbt_outbeam *beam, int64_t nbeam,
+                       const pbt_outbeam *ext, int64_t next, const double *verts, int64_t nverts,
+                       const int64_t *face_off, const int64_t *face_vi, int64_t nfaces,
+                       const double *theta, int64_t ntheta, const double *phi, int64_t nphi,
+                       double lambda, int32_t is_fast_diff, const double *grad_ampl_far_beam,
+                       const double *grad_ampl_far_ext_diff, double *grad_verts,
+                       double *grad_beam_ampl, double *grad_ext_ampl);
+
 /* ------------------------------------------------------------ outputs_mod */
 
 /* finalise replacement, src/outputs_mod.f90:63-278 (FP64, reference order).
