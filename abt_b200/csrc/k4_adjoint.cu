@@ -15,14 +15,15 @@
 // the frame the reference builds from angles (src/diff_mod.f90:200-289,
 // 540-559).  Per facet x bin the kernel recomputes the forward quantities and
 // back-propagates; everything that depends on the bin only through a linear
-// map of per-facet data is accumulated as a per-facet sum over bins (35
+// map of per-facet data is accumulated as a per-facet sum over bins (36
 // floats), so no facet x bin intermediate is stored.  A host pass in FP64 then
 // maps those sums through the frame construction to the vertex gradients.
 //
 // Layout: one warp per record (4 per CTA), lanes striding over a range of
-// bins with the 35 sums in registers; one warp reduction and one FP64 atomic
+// bins with the 36 sums in registers; one warp reduction and one FP64 atomic
 // per (record, bin range) at the end.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -37,7 +38,7 @@ namespace {
 
 constexpr int K4_WARPS = 4;     // records per CTA, one per warp
 constexpr int64_t K4_MAX_LANE_BINS = 1024;  // FP32 terms per lane and accumulator
-constexpr int K4_NACC = 35;     // per-record accumulators
+constexpr int K4_NACC = 36;     // per-record accumulators
 constexpr double kTwoPi4 = 6.283185307179586;
 constexpr double kInv2Pi4 = 0.15915494309189535;
 constexpr double kMagic4 = 6755399441055744.0;
@@ -52,19 +53,35 @@ enum {
     A_EA = 23,     // 3: sum ea_bar
     A_P2 = 26,     // 3: prop2 cotangent
     A_INC = 29,    // 3: incidence-in-frame cotangent
-    A_C = 32,      // 3: c cotangent (lab)
+    A_CU = 32,     // 3: sum of (c-direct coefficient) x u, the u-parallel part of c_bar
+    A_CE = 35,     // 1: sum of the coefficient of 2 c / R^2 in c_bar
 };
 
 struct K4Rec {
     double kc[3];
-    float eps[3], b, R[9], ea[3], kp[2], p2[3], cf, inc[3], xa[3], ya[3], amp[8];
+    float eps[3], b, R[9], ea[3], kp[2], p2[3], cf, icf, inc[3], xa[3], ya[3], amp[8];
+};
+
+// Per-bin inputs in HBM: 48 B, three 16-byte loads.
+struct __align__(16) K4Bin {
+    double ux, uy, uz;  // unit bin direction, FP64
+    float fx, fy;       // the same in FP32
+    float hx, hy, hz;   // forward-bodge direction (same phi, first row above 1 degree)
+    float fz;
 };
 
 struct Bin4 {
     double ux, uy, uz;
     float fx, fy, fz, hx, hy, hz;
-    float G[8];  // cotangent of S' (pre-T, common phase removed) for the record's kind
+    float2 G[4];   // cotangent of S' (pre-T, common phase removed) for the record's kind
+    float2 Gm[4];  // -i G
 };
+
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 
 __device__ __forceinline__ float rcp4(float x) {
     float r;
@@ -72,44 +89,46 @@ __device__ __forceinline__ float rcp4(float x) {
     return r;
 }
 
-// sinc(h) and sinc'(h) for h >= 0
-__device__ __forceinline__ void sinc_d(float h, float &sc, float &dsc) {
-    if (h < 0.5f) {
-        const float h2 = h * h;
-        sc = fmaf(h2, fmaf(h2, fmaf(h2, fmaf(h2, 2.7557319e-6f, -1.9841270e-4f), 8.3333333e-3f),
-                           -1.6666667e-1f),
-                  1.0f);
-        // d/dh (sin h / h) = -h/3 + h^3/30 - h^5/840 + h^7/45360
-        dsc = h * fmaf(h2, fmaf(h2, fmaf(h2, 2.2045855e-5f, -1.1904762e-3f), 3.3333333e-2f),
-                       -0.33333333f);
-    } else {
-        float s, c;
-        __sincosf(h, &s, &c);
-        const float r = rcp4(h);
-        sc = s * r;
-        dsc = (c - sc) * r;
-    }
+// sinc(h) and sinc'(h) for h >= 0, branch-free: series below 0.5, else
+// sin(h)/h and (cos h - sinc h)/h with rh = 1/max(h, 0.5).
+__device__ __forceinline__ void sinc_d(float h, float rh, float &sc, float &dsc) {
+    const float h2 = h * h;
+    const float ps = fmaf(h2, fmaf(h2, fmaf(h2, fmaf(h2, 2.7557319e-6f, -1.9841270e-4f), 8.3333333e-3f),
+                                   -1.6666667e-1f),
+                          1.0f);
+    // d/dh (sin h / h) = -h/3 + h^3/30 - h^5/840 + h^7/45360
+    const float pd = h * fmaf(h2, fmaf(h2, fmaf(h2, 2.2045855e-5f, -1.1904762e-3f), 3.3333333e-2f),
+                              -0.33333333f);
+    float s, c;
+    __sincosf(h, &s, &c);
+    const float qs = s * rh;
+    const float qd = (c - qs) * rh;
+    const bool small = h < 0.5f;
+    sc = small ? ps : qs;
+    dsc = small ? pd : qd;
 }
 
-// g = second divided difference of e^{ix} at t[0..2] and dg/dt_j.
-__device__ __forceinline__ void dd_grad(const float t[3], float2 &g, float2 dg[3]) {
-    // sort with indices
-    int i0 = 0, i1 = 1, i2 = 2;
-    if (t[i1] < t[i0]) { int q = i0; i0 = i1; i1 = q; }
-    if (t[i2] < t[i1]) { int q = i1; i1 = i2; i2 = q; }
-    if (t[i1] < t[i0]) { int q = i0; i0 = i1; i1 = q; }
-    const float lo = t[i0], mid = t[i1], hi = t[i2];
+// g = second divided difference of e^{ix} at t0, t1, t2, and dg/dlo, dg/dhi
+// for the smallest and largest phase (dg/dmid = i g - dg/dlo - dg/dhi, since
+// g(t + s) = e^{is} g(t)).
+__device__ __forceinline__ void dd_grad(float t0, float t1, float t2, float2 &g, float2 &dlo,
+                                        float2 &dhi) {
+    const float lo = fminf(fminf(t0, t1), t2), hi = fmaxf(fmaxf(t0, t1), t2);
+    const float mid = fmaxf(fminf(t0, t1), fminf(fmaxf(t0, t1), t2));
     const float D = hi - lo;
-    float2 dlo, dmid, dhi;
-    if (D >= 0.25f) {
+    {
         const float h1 = 0.5f * (mid - lo), h2 = 0.5f * (hi - mid);
         float s1, c1, s2, c2;
         __sincosf(lo + h1, &s1, &c1);
         __sincosf(mid + h2, &s2, &c2);
+        // 1/max(h1,.5), 1/max(h2,.5), 1/max(D,.25) from one reciprocal
+        const float a1 = fmaxf(h1, 0.5f), a2 = fmaxf(h2, 0.5f), Dg = fmaxf(D, 0.25f);
+        const float p12 = a1 * a2;
+        const float r = rcp4(p12 * Dg);
+        const float rD = Dg * r, iD = p12 * r;
         float sc1, dsc1, sc2, dsc2;
-        sinc_d(h1, sc1, dsc1);
-        sinc_d(h2, sc2, dsc2);
-        const float iD = rcp4(D);
+        sinc_d(h1, a2 * rD, sc1, dsc1);
+        sinc_d(h2, a1 * rD, sc2, dsc2);
         // E = i e^{ic} sinc(h): (-s sc, c sc); dE/dc = i E; dE/dh = i e^{ic} sinc'(h)
         const float2 E1 = make_float2(-s1 * sc1, c1 * sc1), E2 = make_float2(-s2 * sc2, c2 * sc2);
         const float2 iE1 = make_float2(-E1.y, E1.x), iE2 = make_float2(-E2.y, E2.x);
@@ -117,35 +136,28 @@ __device__ __forceinline__ void dd_grad(const float t[3], float2 &g, float2 dg[3
         g = make_float2((E2.x - E1.x) * iD, (E2.y - E1.y) * iD);
         // d g1/d lo = (iE1 - H1)/2, d g1/d mid = (iE1 + H1)/2, d g2/d mid = (iE2 - H2)/2, d g2/d hi = (iE2 + H2)/2
         dlo = make_float2((-(0.5f * (iE1.x - H1.x)) + g.x) * iD, (-(0.5f * (iE1.y - H1.y)) + g.y) * iD);
-        dmid = make_float2((0.5f * (iE2.x - H2.x) - 0.5f * (iE1.x + H1.x)) * iD,
-                           (0.5f * (iE2.y - H2.y) - 0.5f * (iE1.y + H1.y)) * iD);
         dhi = make_float2((0.5f * (iE2.x + H2.x) - g.x) * iD, (0.5f * (iE2.y + H2.y) - g.y) * iD);
-    } else {
-        // series about mid: g = e^{i mid} sum_n c_n h_n(ya, yc)
+    }
+    if (D < 0.25f) {
+        // series about mid: g = e^{i mid} sum_n c_n h_n(ya, yc), c_n = i^(n+2)/(n+2)!
         const float ya = lo - mid, yc = hi - mid;
-        float hq[8], da[8], dc[8], yap[8];
-        yap[0] = 1.0f;
-        for (int n = 1; n < 8; n++) yap[n] = yap[n - 1] * ya;
-        hq[0] = 1.0f;
-        da[0] = 0.0f;
-        dc[0] = 0.0f;
-        for (int n = 1; n < 8; n++) {
-            hq[n] = fmaf(yc, hq[n - 1], yap[n]);
-            da[n] = fmaf(yc, da[n - 1], (float)n * yap[n - 1]);
-            dc[n] = fmaf(yc, dc[n - 1], hq[n - 1]);
-        }
-        // c_n = i^(n+2)/(n+2)!
         const float cr[8] = {-0.5f, 0.0f, 1.0f / 24.0f, 0.0f, -1.0f / 720.0f, 0.0f, 1.0f / 40320.0f, 0.0f};
         const float ci[8] = {0.0f, -1.0f / 6.0f, 0.0f, 1.0f / 120.0f, 0.0f, -1.0f / 5040.0f, 0.0f,
                              1.0f / 362880.0f};
-        float2 sg = make_float2(0, 0), sa = make_float2(0, 0), sc = make_float2(0, 0);
-        for (int n = 0; n < 8; n++) {
-            sg.x = fmaf(cr[n], hq[n], sg.x);
-            sg.y = fmaf(ci[n], hq[n], sg.y);
-            sa.x = fmaf(cr[n], da[n], sa.x);
-            sa.y = fmaf(ci[n], da[n], sa.y);
-            sc.x = fmaf(cr[n], dc[n], sc.x);
-            sc.y = fmaf(ci[n], dc[n], sc.y);
+        float hq = 1.0f, da = 0.0f, dc = 0.0f, yap = 1.0f;
+        float2 sg = make_float2(cr[0], ci[0]), sa = make_float2(0, 0), sc = make_float2(0, 0);
+#pragma unroll
+        for (int n = 1; n < 8; n++) {
+            dc = fmaf(yc, dc, hq);
+            da = fmaf(yc, da, (float)n * yap);
+            yap *= ya;
+            hq = fmaf(yc, hq, yap);
+            sg.x = fmaf(cr[n], hq, sg.x);
+            sg.y = fmaf(ci[n], hq, sg.y);
+            sa.x = fmaf(cr[n], da, sa.x);
+            sa.y = fmaf(ci[n], da, sa.y);
+            sc.x = fmaf(cr[n], dc, sc.x);
+            sc.y = fmaf(ci[n], dc, sc.y);
         }
         float sm, cm;
         __sincosf(mid, &sm, &cm);
@@ -153,12 +165,7 @@ __device__ __forceinline__ void dd_grad(const float t[3], float2 &g, float2 dg[3
         g = rot(sg);
         dlo = rot(sa);
         dhi = rot(sc);
-        // shift identity: sum_j dg/dt_j = i g
-        dmid = make_float2(-g.y - dlo.x - dhi.x, g.x - dlo.y - dhi.y);
     }
-    dg[i0] = dlo;
-    dg[i1] = dmid;
-    dg[i2] = dhi;
 }
 
 // Bin direction from the facet centre in the aperture frame (second order in c/R)
@@ -179,9 +186,10 @@ __device__ __forceinline__ Dir4 dir4(const K4Rec &r, float fx, float fy, float f
 }
 
 // Back-propagate a cotangent kb of the aperture-frame direction into the
-// accumulators (frame outer product, ea, c).
+// frame outer product and ea accumulators; returns the cotangents of
+// a = u.c/R (ab) and b = |c|^2/R^2 (bb) for the caller's c terms.
 __device__ __forceinline__ void dir4_back(const K4Rec &r, const Dir4 &d, const float kb[3], float fx,
-                                          float fy, float fz, float *acc, float Rf) {
+                                          float fy, float fz, float *acc, float &ab, float &bb) {
     const float u[3] = {fx, fy, fz};
     float opa2b = 0.0f, opab = 0.0f;
     for (int i = 0; i < 3; i++) {
@@ -191,17 +199,14 @@ __device__ __forceinline__ void dir4_back(const K4Rec &r, const Dir4 &d, const f
         for (int j = 0; j < 3; j++) acc[A_WU + 3 * i + j] = fmaf(wb, u[j], acc[A_WU + 3 * i + j]);
         acc[A_EA + i] = fmaf(-kb[i], d.opa, acc[A_EA + i]);
     }
-    const float ab = opab + opa2b * fmaf(3.0f, d.a, 1.0f);
-    const float bb = -0.5f * opa2b;
-    // a = u.c / R ; b = |c|^2 / R^2, with c = eps * R
-    for (int j = 0; j < 3; j++)
-        acc[A_C + j] = fmaf(ab, u[j] / Rf, fmaf(bb, 2.0f * r.eps[j] / Rf, acc[A_C + j]));
+    ab = opab + opa2b * fmaf(3.0f, d.a, 1.0f);
+    bb = -0.5f * opa2b;
 }
 
 // Cotangent contributions of one (record, bin).
 template <bool FAST>
-__device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, float hkR, float Rf,
-                                        float cosfov, const float *p0, float *acc) {
+__device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, float hkR, float iRf,
+                                        float cosfov, const float *p0, float *acc, float2 *accA) {
     // forward
     const double ka = fma(B.uz, r.kc[2], fma(B.uy, r.kc[1], B.ux * r.kc[0]));
     const double nq = fma(ka, kInv2Pi4, kMagic4) - kMagic4;
@@ -217,9 +222,9 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const float kxx = fmaf(-k, kx, r.kp[0]), kyy = fmaf(-k, ky, r.kp[1]);
     float t[3];
     for (int j = 0; j < 3; j++) t[j] = fmaf(kyy, r.ya[j], fmaf(kxx, r.xa[j], ph));
-    float2 g, dg[3];
-    dd_grad(t, g, dg);
-    const float Kx = r.p2[0], Ky = r.p2[1], Kz = r.p2[2], cf = r.cf;
+    float2 g, dlo, dhi;
+    dd_grad(t[0], t[1], t[2], g, dlo, dhi);
+    const float Kx = r.p2[0], Ky = r.p2[1], Kz = r.p2[2], cf = r.cf, rcf = r.icf;
     const bool yclamp = !(fabsf(ky) <= 0.999999f);
     const float kyc = fminf(fmaxf(ky, -0.999999f), 0.999999f);
     const float traw = fmaf(kx, kx, kz * kz);
@@ -227,8 +232,8 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const float tt = floored ? kClampSq4 : traw;
     const float rs = rsqrtf(tt), s = tt * rs;
     const float m[3] = {-kx * kyc * rs, s, -kz * kyc * rs};
-    const float dd = fmaf(-0.5f * Kz * cf, s, -0.5f * kz * rs / cf);
-    const float ee = fmaf(0.5f * Kx * Ky * cf, s, -0.5f * kx * kyc * rs / cf);
+    const float dd = fmaf(-0.5f * Kz * cf, s, -0.5f * kz * rs * rcf);
+    const float ee = fmaf(0.5f * Kx * Ky * cf, s, -0.5f * kx * kyc * rs * rcf);
     const float kc3[3] = {kx, kyc, kz};
     const float dinc = fmaf(r.inc[2], kz, fmaf(r.inc[1], kyc, r.inc[0] * kx));
     const bool bodge = !(fabsf(dinc) < 0.999f);
@@ -251,37 +256,33 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const float pp = fmaf(hc[2], m[2], fmaf(hc[1], m[1], hc[0] * m[0]));
     const float rr = fmaf(hc[2], ev[2], fmaf(hc[1], ev[1], hc[0] * ev[0]));
     const float A = fmaf(pp, dd, rr * ee), Bm = fmaf(pp, ee, -rr * dd);
-    // W = [[A, B], [-B, A]] amp' ; order (1,1),(2,1),(1,2),(2,2)
-    const float *a = r.amp;
-    float W[8];
-    W[0] = fmaf(A, a[0], Bm * a[2]);
-    W[1] = fmaf(A, a[1], Bm * a[3]);
-    W[2] = fmaf(A, a[2], -Bm * a[0]);
-    W[3] = fmaf(A, a[3], -Bm * a[1]);
-    W[4] = fmaf(A, a[4], Bm * a[6]);
-    W[5] = fmaf(A, a[5], Bm * a[7]);
-    W[6] = fmaf(A, a[6], -Bm * a[4]);
-    W[7] = fmaf(A, a[7], -Bm * a[5]);
-    // backward.  C = g W:  g_bar = sum G conj(W), W_bar = G conj(g)
+    // W = [[A, B], [-B, A]] amp' ; complex order (1,1),(2,1),(1,2),(2,2)
+    const float2 *a = reinterpret_cast<const float2 *>(r.amp);
+    const float2 A2 = bc2(A), B2 = bc2(Bm), nB2 = bc2(-Bm);
+    float2 W[4];
+    W[0] = fma2(A2, a[0], mul2(B2, a[1]));
+    W[1] = fma2(A2, a[1], mul2(nB2, a[0]));
+    W[2] = fma2(A2, a[2], mul2(B2, a[3]));
+    W[3] = fma2(A2, a[3], mul2(nB2, a[2]));
+    // backward.  C = g W:  g_bar = sum G conj(W) = sum (Re W) G + (Im W)(-i G),
+    // W_bar = G conj(g) = (Re g) G + (Im g)(-i G)
     float2 gb = make_float2(0, 0);
-    float Wb[8];
+    float2 Wb[4];
+    const float2 gx2 = bc2(g.x), gy2 = bc2(g.y);
+#pragma unroll
     for (int c = 0; c < 4; c++) {
-        const float Gr = B.G[2 * c], Gi = B.G[2 * c + 1], wr = W[2 * c], wi = W[2 * c + 1];
-        gb.x = fmaf(Gr, wr, fmaf(Gi, wi, gb.x));
-        gb.y = fmaf(Gi, wr, fmaf(-Gr, wi, gb.y));
-        Wb[2 * c] = fmaf(Gr, g.x, Gi * g.y);
-        Wb[2 * c + 1] = fmaf(Gi, g.x, -Gr * g.y);
+        gb = fma2(bc2(W[c].x), B.G[c], fma2(bc2(W[c].y), B.Gm[c], gb));
+        Wb[c] = fma2(gx2, B.G[c], mul2(gy2, B.Gm[c]));
     }
-    // A_bar, B_bar = Re sum conj(W_bar) dW/dA|B ; amp'_bar = M^T W_bar
-    auto rdot = [&](int wi, int ai) { return fmaf(Wb[2 * wi], a[2 * ai], Wb[2 * wi + 1] * a[2 * ai + 1]); };
-    const float Ab = rdot(0, 0) + rdot(1, 1) + rdot(2, 2) + rdot(3, 3);
-    const float Bb = rdot(0, 1) - rdot(1, 0) + rdot(2, 3) - rdot(3, 2);
-    for (int z = 0; z < 2; z++) {
-        acc[A_AMP + 0 + z] += fmaf(A, Wb[0 + z], -Bm * Wb[2 + z]);
-        acc[A_AMP + 2 + z] += fmaf(Bm, Wb[0 + z], A * Wb[2 + z]);
-        acc[A_AMP + 4 + z] += fmaf(A, Wb[4 + z], -Bm * Wb[6 + z]);
-        acc[A_AMP + 6 + z] += fmaf(Bm, Wb[4 + z], A * Wb[6 + z]);
-    }
+    // A_bar = Re sum conj(W_bar) dW/dA, B_bar likewise ; amp'_bar = M^T W_bar
+    const float2 pa = fma2(Wb[0], a[0], fma2(Wb[1], a[1], fma2(Wb[2], a[2], mul2(Wb[3], a[3]))));
+    const float2 pb = sub2(fma2(Wb[0], a[1], mul2(Wb[2], a[3])), fma2(Wb[1], a[0], mul2(Wb[3], a[2])));
+    const float Ab = pa.x + pa.y;
+    const float Bb = pb.x + pb.y;
+    accA[0] = fma2(A2, Wb[0], fma2(nB2, Wb[1], accA[0]));
+    accA[1] = fma2(B2, Wb[0], fma2(A2, Wb[1], accA[1]));
+    accA[2] = fma2(A2, Wb[2], fma2(nB2, Wb[3], accA[2]));
+    accA[3] = fma2(B2, Wb[2], fma2(A2, Wb[3], accA[3]));
     // A = pp dd + rr ee, B = pp ee - rr dd
     const float ppb = fmaf(Ab, dd, Bb * ee), rrb = fmaf(Ab, ee, -Bb * dd);
     const float ddb = fmaf(Ab, pp, -Bb * rr), eeb = fmaf(Ab, rr, Bb * pp);
@@ -321,7 +322,13 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     acc[A_INC + 1] += q[2] * hrb[0] - q[0] * hrb[2];
     acc[A_INC + 2] += q[0] * hrb[1] - q[1] * hrb[0];
     if (bodge) {
-        dir4_back(r, dh, qb, B.hx, B.hy, B.hz, acc, Rf);
+        float abh, bbh;
+        dir4_back(r, dh, qb, B.hx, B.hy, B.hz, acc, abh, bbh);
+        const float ch = abh * iRf;
+        acc[A_CU + 0] = fmaf(ch, B.hx, acc[A_CU + 0]);
+        acc[A_CU + 1] = fmaf(ch, B.hy, acc[A_CU + 1]);
+        acc[A_CU + 2] = fmaf(ch, B.hz, acc[A_CU + 2]);
+        acc[A_CE] += bbh;
     } else {
         kcb[0] += qb[0];
         kcb[1] += qb[1];
@@ -329,7 +336,6 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     }
     // Karczewski-Wolf: m = (-kx kyc rs, s, -kz kyc rs), dd, ee as above
     float kxb = kcb[0], kycb = kcb[1], kzb = kcb[2];
-    const float rcf = 1.0f / cf;
     kxb += mb[0] * (-kyc * rs) + eeb * (-0.5f * kyc * rs * rcf);
     kycb += mb[0] * (-kx * rs) + mb[2] * (-kz * rs) + eeb * (-0.5f * kx * rs * rcf);
     kzb += mb[2] * (-kyc * rs) + ddb * (-0.5f * rs * rcf);
@@ -348,11 +354,17 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
         kzb = fmaf(2.0f * kz, ttb, kzb);
     }
     float kyb = yclamp ? 0.0f : kycb;
-    // phases: t_j = ph + kxx xa_j + kyy ya_j
-    float phb = 0.0f, kxxb = 0.0f, kyyb = 0.0f;
+    // phases: t_j = ph + kxx xa_j + kyy ya_j.  t_bar = Re(conj(g_bar) dg/dt),
+    // assigned by rank (ties broken by index); phb = sum_j t_bar_j = Re(conj(g_bar) i g).
+    const float tlo = fmaf(gb.x, dlo.x, gb.y * dlo.y), thi = fmaf(gb.x, dhi.x, gb.y * dhi.y);
+    const float phb = fmaf(gb.y, g.x, -gb.x * g.y);
+    const float tmid = phb - tlo - thi;
+    const int rk[3] = {(t[1] < t[0]) + (t[2] < t[0]), (t[0] <= t[1]) + (t[2] < t[1]),
+                       (t[0] <= t[2]) + (t[1] <= t[2])};
+    float kxxb = 0.0f, kyyb = 0.0f;
+#pragma unroll
     for (int j = 0; j < 3; j++) {
-        const float tb = fmaf(gb.x, dg[j].x, gb.y * dg[j].y);  // Re(conj(g_bar) dg/dt_j)
-        phb += tb;
+        const float tb = rk[j] == 0 ? tlo : (rk[j] == 1 ? tmid : thi);
         kxxb = fmaf(tb, r.xa[j], kxxb);
         kyyb = fmaf(tb, r.ya[j], kyyb);
         acc[A_TKX + j] = fmaf(tb, kxx, acc[A_TKX + j]);
@@ -363,28 +375,30 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     kyb = fmaf(-k, kyyb, kyb);
     acc[A_P2 + 0] = fmaf(k, kxxb, acc[A_P2 + 0]);
     acc[A_P2 + 1] = fmaf(k, kyyb, acc[A_P2 + 1]);
-    // ph = hkR (b - a^2)(1 + a) - rf ; rf = k u.c (mod 2 pi)
-    {
-        const float dpa = hkR * fmaf(-2.0f * d.a, d.opa, fmaf(-d.a, d.a, r.b));
-        const float dpb = hkR * d.opa;
-        const float u[3] = {B.fx, B.fy, B.fz};
-        for (int j = 0; j < 3; j++)
-            acc[A_C + j] += phb * (fmaf(-k, u[j], dpa * u[j] / Rf) + dpb * 2.0f * r.eps[j] / Rf);
-    }
     const float kb3[3] = {kxb, kyb, kzb};
-    dir4_back(r, d, kb3, B.fx, B.fy, B.fz, acc, Rf);
+    float ab, bb;
+    dir4_back(r, d, kb3, B.fx, B.fy, B.fz, acc, ab, bb);
+    // ph = hkR (b - a^2)(1 + a) - rf with rf = k u.c (mod 2 pi), a = u.c/R, b = |c|^2/R^2:
+    // c_bar = (ab + phb dph/da) u / R - phb k u + (bb + phb dph/db) 2 c / R^2
+    const float dpa = hkR * fmaf(-2.0f * d.a, d.opa, fmaf(-d.a, d.a, r.b));
+    const float dpb = hkR * d.opa;
+    const float cu = fmaf(fmaf(phb, dpa, ab), iRf, -k * phb);
+    acc[A_CU + 0] = fmaf(cu, B.fx, acc[A_CU + 0]);
+    acc[A_CU + 1] = fmaf(cu, B.fy, acc[A_CU + 1]);
+    acc[A_CU + 2] = fmaf(cu, B.fz, acc[A_CU + 2]);
+    acc[A_CE] += fmaf(phb, dpb, bb);
 }
 
 // One warp per record, K4_WARPS records per CTA; blockIdx.y selects a range
-// of bins.  Each lane walks the range with stride 32 and keeps the 35 sums of
+// of bins.  Each lane walks the range with stride 32 and keeps the 36 sums of
 // its record in registers (FP32, at most K4_MAX_LANE_BINS terms), so the warp
-// reduction and the FP64 atomic into out[record][35] happen once per
+// reduction and the FP64 atomic into out[record][36] happen once per
 // (record, range).  The warps of a CTA walk the same bins, which the L1 serves.
-template <bool FAST>
-__global__ void __launch_bounds__(K4_WARPS * 32) k4_adjoint_kernel(
+template <bool FAST, int MINB>
+__global__ void __launch_bounds__(K4_WARPS * 32, MINB) k4_adjoint_kernel(
     const K4Rec *__restrict__ recs, const int *__restrict__ kinds, const float *__restrict__ fovdat,
-    int64_t nrec, const double *__restrict__ ud, const float *__restrict__ uh,
-    const float *__restrict__ gbin, int64_t nb, int64_t chunk, float k, float hkR, float Rf,
+    int64_t nrec, const K4Bin *__restrict__ bins, const float4 *__restrict__ gbin, int64_t nb,
+    int64_t chunk, float k, float hkR, float iRf,
     double *__restrict__ out) {
     __shared__ K4Rec s_rec[K4_WARPS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -398,7 +412,7 @@ __global__ void __launch_bounds__(K4_WARPS * 32) k4_adjoint_kernel(
     }
     const K4Rec &r = s_rec[warp];
     const int kd = kinds[rec];
-    const float *G = gbin + (int64_t)kd * 8 * nb;
+    const float4 *G = gbin + (int64_t)kd * 4 * nb;
     float cosfov = 0.0f, p0[3] = {0.0f, 0.0f, 0.0f};
     if (FAST) {
         p0[0] = fovdat[4 * rec];
@@ -407,23 +421,41 @@ __global__ void __launch_bounds__(K4_WARPS * 32) k4_adjoint_kernel(
         cosfov = fovdat[4 * rec + 3];
     }
     float acc[K4_NACC];
+    float2 accA[4];
 #pragma unroll
     for (int q = 0; q < K4_NACC; q++) acc[q] = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) accA[q] = make_float2(0.0f, 0.0f);
     const int64_t o0 = (int64_t)blockIdx.y * chunk, o1 = min(nb, o0 + chunk);
     for (int64_t o = o0 + lane; o < o1; o += 32) {
         Bin4 B;
-        B.ux = ud[o];
-        B.uy = ud[nb + o];
-        B.uz = ud[2 * nb + o];
-        B.fx = (float)B.ux;
-        B.fy = (float)B.uy;
-        B.fz = (float)B.uz;
-        B.hx = uh[o];
-        B.hy = uh[nb + o];
-        B.hz = uh[2 * nb + o];
+        const float4 *pb = reinterpret_cast<const float4 *>(bins + o);
+        const float4 q0 = pb[0], q1 = pb[1], q2 = pb[2];
+        B.ux = __hiloint2double(__float_as_int(q0.y), __float_as_int(q0.x));
+        B.uy = __hiloint2double(__float_as_int(q0.w), __float_as_int(q0.z));
+        B.uz = __hiloint2double(__float_as_int(q1.y), __float_as_int(q1.x));
+        B.fx = q1.z;
+        B.fy = q1.w;
+        B.hx = q2.x;
+        B.hy = q2.y;
+        B.hz = q2.z;
+        B.fz = q2.w;
+        const float4 *pg = G + 4 * o;
+        const float4 g0 = pg[0], g1 = pg[1], g2 = pg[2], g3 = pg[3];
+        B.G[0] = make_float2(g0.x, g0.y);
+        B.G[1] = make_float2(g0.z, g0.w);
+        B.G[2] = make_float2(g1.x, g1.y);
+        B.G[3] = make_float2(g1.z, g1.w);
+        B.Gm[0] = make_float2(g2.x, g2.y);
+        B.Gm[1] = make_float2(g2.z, g2.w);
+        B.Gm[2] = make_float2(g3.x, g3.y);
+        B.Gm[3] = make_float2(g3.z, g3.w);
+        k4_eval<FAST>(r, B, k, hkR, iRf, cosfov, p0, acc, accA);
+    }
 #pragma unroll
-        for (int c = 0; c < 8; c++) B.G[c] = G[c * nb + o];
-        k4_eval<FAST>(r, B, k, hkR, Rf, cosfov, p0, acc);
+    for (int q = 0; q < 4; q++) {
+        acc[A_AMP + 2 * q] = accA[q].x;
+        acc[A_AMP + 2 * q + 1] = accA[q].y;
     }
 #pragma unroll
     for (int q = 0; q < K4_NACC; q++) {
@@ -441,22 +473,26 @@ __global__ void __launch_bounds__(K4_WARPS * 32) k4_adjoint_kernel(
 __global__ void k4_prep_kernel(const double *__restrict__ gafb, const double *__restrict__ gafe,
                                const double *__restrict__ xyz, const double *__restrict__ phitab,
                                int64_t nb, int64_t nphi, int64_t theta_i, double k,
-                               double *__restrict__ ud, float *__restrict__ uh,
-                               float *__restrict__ gbin) {
+                               K4Bin *__restrict__ bins, float4 *__restrict__ gbin) {
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= nb) return;
     const double cp = phitab[o % nphi], sp = phitab[nphi + o % nphi];
     const double X = xyz[o], Y = xyz[nb + o], Zc = xyz[2 * nb + o];
     const double rho = sqrt(X * X + Y * Y + Zc * Zc), ir = 1.0 / rho;
-    ud[o] = X * ir;
-    ud[nb + o] = Y * ir;
-    ud[2 * nb + o] = Zc * ir;
+    K4Bin bn;
+    bn.ux = X * ir;
+    bn.uy = Y * ir;
+    bn.uz = Zc * ir;
+    bn.fx = (float)bn.ux;
+    bn.fy = (float)bn.uy;
+    bn.fz = (float)bn.uz;
     const int64_t oh = (o % nphi) + nphi * theta_i;
     const double Xh = xyz[oh], Yh = xyz[nb + oh], Zh = xyz[2 * nb + oh];
     const double irh = 1.0 / sqrt(Xh * Xh + Yh * Yh + Zh * Zh);
-    uh[o] = (float)(Xh * irh);
-    uh[nb + o] = (float)(Yh * irh);
-    uh[2 * nb + o] = (float)(Zh * irh);
+    bn.hx = (float)(Xh * irh);
+    bn.hy = (float)(Yh * irh);
+    bn.hz = (float)(Zh * irh);
+    bins[o] = bn;
     double sK, cK;
     sincos(k * rho, &sK, &cK);
     const double T11 = -sp, T12 = -cp, T21 = cp, T22 = -sp;
@@ -473,8 +509,12 @@ __global__ void k4_prep_kernel(const double *__restrict__ gafb, const double *__
         const double o21r = gr[1] * T11 + gr[3] * T12, o21i = gi[1] * T11 + gi[3] * T12;
         const double o12r = gr[0] * T21 + gr[2] * T22, o12i = gi[0] * T21 + gi[2] * T22;
         const double o22r = gr[1] * T21 + gr[3] * T22, o22i = gi[1] * T21 + gi[3] * T22;
-        const double v[8] = {o11r, o11i, o21r, o21i, o12r, o12i, o22r, o22i};
-        for (int c = 0; c < 8; c++) gbin[(kd * 8 + c) * nb + o] = (float)v[c];
+        // G and -i G = (Im, -Re)
+        float4 *dst = gbin + (kd * nb + o) * 4;
+        dst[0] = make_float4((float)o11r, (float)o11i, (float)o21r, (float)o21i);
+        dst[1] = make_float4((float)o12r, (float)o12i, (float)o22r, (float)o22i);
+        dst[2] = make_float4((float)o11i, -(float)o11r, (float)o21i, -(float)o21r);
+        dst[3] = make_float4((float)o12i, -(float)o12r, (float)o22i, -(float)o22r);
     }
 }
 
@@ -555,6 +595,7 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
         r.kp[0] = (float)(k * fr.prop2[0]);
         r.kp[1] = (float)(k * fr.prop2[1]);
         r.cf = (float)(1.0 / sqrt(1.0 - fr.prop2[1] * fr.prop2[1]));
+        r.icf = (float)sqrt(1.0 - fr.prop2[1] * fr.prop2[1]);
         for (int c = 0; c < 4; c++) {
             r.amp[2 * c] = (float)(-cpre * ob.ampl[2 * c + 1]);
             r.amp[2 * c + 1] = (float)(cpre * ob.ampl[2 * c]);
@@ -571,8 +612,8 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t o_rec = 0, o_kind = al(nrec * sizeof(K4Rec)), o_fov = al(o_kind + nrec * 4),
                  o_ga = al(o_fov + 16 * nrec), o_gb = al(o_ga + 8 * nb * 8),
-                 o_ud = al(o_gb + 8 * nb * 8), o_uh = al(o_ud + 3 * nb * 8),
-                 o_gbin = al(o_uh + 3 * nb * 4), o_out = al(o_gbin + 16 * nb * 4),
+                 o_bin = al(o_gb + 8 * nb * 8), o_gbin = al(o_bin + nb * sizeof(K4Bin)),
+                 o_out = al(o_gbin + 32 * nb * 4),
                  o_end = al(o_out + nrec * K4_NACC * 8);
     PBT_TRY(ctx->d_ws.ensure(o_end));
     char *base = ctx->d_ws.as<char>();
@@ -586,8 +627,8 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
     PBT_CUDA_TRY(cudaMemcpyAsync(base + o_gb, gafe, 8 * nb * 8, cudaMemcpyHostToDevice, st));
     k4_prep_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, st>>>(
         (const double *)(base + o_ga), (const double *)(base + o_gb), g.xyz.as<double>(),
-        g.phitab.as<double>(), nb, nphi, g.theta_i, k, (double *)(base + o_ud),
-        (float *)(base + o_uh), (float *)(base + o_gbin));
+        g.phitab.as<double>(), nb, nphi, g.theta_i, k, (K4Bin *)(base + o_bin),
+        (float4 *)(base + o_gbin));
     // bin ranges: at most K4_MAX_LANE_BINS terms per lane, and enough CTAs
     // for a few waves when there are few records
     const int64_t ncta_rec = (nrec + K4_WARPS - 1) / K4_WARPS;
@@ -599,19 +640,31 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
     nsplit = (nb + chunk - 1) / chunk;
     const dim3 grid((unsigned)ncta_rec, (unsigned)nsplit);
     timing_begin(ctx, st);
+    // Minimum CTAs per SM for the register budget: 3 (168 registers, a few
+    // bytes of spill) by default; PBT_K4_MINB=1|2|4 selects another build.
+    static const int minb = [] {
+        const char *e = getenv("PBT_K4_MINB");
+        const int v = e ? atoi(e) : 3;
+        return (v == 1 || v == 2 || v == 4) ? v : 3;
+    }();
     if (nrec > 0) {
-        if (fast_diff)
-            k4_adjoint_kernel<true><<<grid, K4_WARPS * 32, 0, st>>>(
+        auto launch = [&](auto kern) {
+            kern<<<grid, K4_WARPS * 32, 0, st>>>(
                 (const K4Rec *)(base + o_rec), (const int *)(base + o_kind), (const float *)(base + o_fov),
-                nrec, (const double *)(base + o_ud), (const float *)(base + o_uh),
-                (const float *)(base + o_gbin), nb, chunk, (float)k, (float)(0.5 * k * Rf), (float)Rf,
-                (double *)(base + o_out));
-        else
-            k4_adjoint_kernel<false><<<grid, K4_WARPS * 32, 0, st>>>(
-                (const K4Rec *)(base + o_rec), (const int *)(base + o_kind), (const float *)(base + o_fov),
-                nrec, (const double *)(base + o_ud), (const float *)(base + o_uh),
-                (const float *)(base + o_gbin), nb, chunk, (float)k, (float)(0.5 * k * Rf), (float)Rf,
-                (double *)(base + o_out));
+                nrec, (const K4Bin *)(base + o_bin), (const float4 *)(base + o_gbin), nb, chunk, (float)k,
+                (float)(0.5 * k * Rf), (float)(1.0 / Rf), (double *)(base + o_out));
+        };
+        if (fast_diff) {
+            if (minb == 1) launch(k4_adjoint_kernel<true, 1>);
+            else if (minb == 2) launch(k4_adjoint_kernel<true, 2>);
+            else if (minb == 4) launch(k4_adjoint_kernel<true, 4>);
+            else launch(k4_adjoint_kernel<true, 3>);
+        } else {
+            if (minb == 1) launch(k4_adjoint_kernel<false, 1>);
+            else if (minb == 2) launch(k4_adjoint_kernel<false, 2>);
+            else if (minb == 4) launch(k4_adjoint_kernel<false, 4>);
+            else launch(k4_adjoint_kernel<false, 3>);
+        }
     }
     timing_end(ctx, st);
     ctx->launches += nrec > 0 ? 2 : 1;
@@ -669,7 +722,8 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
         // c_bar = direct + R^T ea_bar / Rf
         double cb[3];
         for (int b = 0; b < 3; b++)
-            cb[b] = A[A_C + b] + (h.R[0][b] * A[A_EA + 0] + h.R[1][b] * A[A_EA + 1] + h.R[2][b] * A[A_EA + 2]) / Rf;
+            cb[b] = A[A_CU + b] + A[A_CE] * 2.0 * h.c[b] / (Rf * Rf) +
+                    (h.R[0][b] * A[A_EA + 0] + h.R[1][b] * A[A_EA + 1] + h.R[2][b] * A[A_EA + 2]) / Rf;
         // frame: z = -n, x = unit(p - (p.n) n), y = z x x
         double n[3] = {-h.R[2][0], -h.R[2][1], -h.R[2][2]}, xh[3] = {h.R[0][0], h.R[0][1], h.R[0][2]};
         double zb[3] = {Rb[2][0], Rb[2][1], Rb[2][2]}, xb[3] = {Rb[0][0], Rb[0][1], Rb[0][2]},
