@@ -244,3 +244,41 @@ def standin_orientation(geometry, R, rng, lam=LAMBDA, n_internal=(0, 6), rbi=1.3
     beam["fov"] = 8 * lam / 10.0
     geo = float((area[lit] * cosi[lit]).sum())
     return V, beam, ext, geo
+
+
+def uniform_euler(rng, n):
+    """n (alpha, beta, gamma) triples uniform on SO(3): alpha = 2 pi u1,
+    beta = acos(1 - 2 u2), gamma = 2 pi u3 (the law of
+    src/input_mod.f90:1848-1855)."""
+    u = rng.uniform(size=(n, 3))
+    return np.stack([2 * np.pi * u[:, 0], np.arccos(1 - 2 * u[:, 1]), 2 * np.pi * u[:, 2]], 1)
+
+
+def grid_orientation_average():
+    """361 theta x 180 phi (-theta 0 0.5 180, -phi 0 2 358)."""
+    return make_angles([0, 180], [0.5]), make_angles([0, 358], [2])
+
+
+def rough_column_orientations(n_orient=1024, seed=3, radius=10.0, length=20.0, roughness=0.1,
+                              n_side=6, n_len=12, m_range=(2, 20), lam=LAMBDA):
+    """Stand-in beam lists of the orientation-averaging workload: a Gaussian-rough
+    hexagonal column (radius 10 um, length 20 um, sigma 0.1 um, 1296 triangles),
+    n_orient orientations uniform on SO(3), and per orientation a maximum number
+    m of outgoing beams per facet drawn from m_range, so the outgoing facet count
+    is uneven across orientations (about 2,000 to 14,000).
+    Returns (geometry, [V], [beam], [ext], params_in)."""
+    from .diff import params as _params
+    rng = np.random.default_rng(seed)
+    geo = hex_prism(radius, length, n_side=n_side, n_len=n_len, roughness=roughness, seed=seed)
+    eul = uniform_euler(rng, n_orient)
+    Vs, beams, exts = [], [], []
+    pin = np.zeros(n_orient, dtype=_params().dtype)
+    for i, (a, b, c) in enumerate(eul):
+        m = int(rng.integers(m_range[0], m_range[1] + 1))
+        V, beam, ext, gcs = standin_orientation(geo, euler_rotation(a, b, c), rng, lam=lam,
+                                                n_internal=(0, m))
+        Vs.append(V)
+        beams.append(beam)
+        exts.append(ext)
+        pin[i] = _params(geo_cross_sec=gcs, beam_energy_out=1.0, ext_energy_out=1.0)
+    return geo, Vs, beams, exts, pin

@@ -57,6 +57,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--orient", type=int, default=1024,
+                    help="orientations of the rough-column orientation average (0: skip)")
+    ap.add_argument("--orient-fp64", type=int, default=16,
+                    help="orientations timed with the FP64 drop-in and used for the error")
     ap.add_argument("--adjoint-facets", type=int, default=20000,
                     help="facet sample for the adjoint / forward kernel-time ratio (0: skip)")
     return ap.parse_args()
@@ -133,6 +137,58 @@ def workload(args):
                                            seed=2024)
     th, ph = W.grid_precision_study()
     return geo, beam, ext, th, ph
+
+
+def orientation_average(ctx, args):
+    """Batched FP32 orientation average of the rough hexagonal column (stand-in
+    beam lists, 361 x 180 bins) against the plain per-orientation FP64 drop-in,
+    timed on the first --orient-fp64 orientations and extrapolated by facet·bin
+    count; the error of the averaged Mueller matrix and cross sections is taken
+    on those orientations."""
+    import abt_b200
+    from abt_b200 import workloads as W
+    from tests.helpers import mueller_rel_err
+    geo, Vs, beams, exts, pin = W.rough_column_orientations(args.orient, seed=3)
+    th, ph = W.grid_orientation_average()
+    nb = len(th) * len(ph)
+    F = np.array([len(b) + len(e) for b, e in zip(beams, exts)])
+    k = max(1, min(args.orient_fp64, args.orient))
+    # FP32 batched, all orientations (host API: H2D, one persistent launch per chunk, D2H)
+    ctx.diff_batch(beams[:2], exts[:2], Vs[:2], geo, th, ph, LAM, pin[:2], precision="fp32")
+    ctx.set_kernel_timing(True)
+    ctx.kernel_time_ms()
+    t0 = time.perf_counter()
+    ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp32")
+    t32 = time.perf_counter() - t0
+    k32_ms, k32_n = ctx.kernel_time_ms()
+    # FP32 and FP64 on the first k orientations
+    f32 = ctx.diff_batch(beams[:k], exts[:k], Vs[:k], geo, th, ph, LAM, pin[:k], precision="fp32")
+    ctx.kernel_time_ms()
+    t0 = time.perf_counter()
+    f64 = ctx.diff_batch(beams[:k], exts[:k], Vs[:k], geo, th, ph, LAM, pin[:k], precision="fp64")
+    t64k = time.perf_counter() - t0
+    k64_ms, _ = ctx.kernel_time_ms()
+    ctx.set_kernel_timing(False)
+    work = float(F.sum()) * nb
+    work_k = float(F[:k].sum()) * nb
+    t64 = t64k * work / work_k
+    perr = max(abs(float(f32[2][n]) - float(f64[2][n])) / abs(float(f64[2][n]))
+               for n in ("scatt", "ext", "asymmetry", "back_scatt"))
+    return {"workload": "rough hexagonal column r 10 um, L 20 um, sigma 0.1 um (1296 triangles), "
+                        "stand-in beam lists, %d orientations uniform on SO(3), 361 theta x 180 phi"
+                        % args.orient,
+            "orientations": int(args.orient), "facets_total": int(F.sum()),
+            "facets_per_orientation": [int(F.min()), int(F.mean()), int(F.max())], "bins": nb,
+            "fp32_batched_s": t32, "fp32_orientations_per_s": args.orient / t32,
+            "fp32_facet_bin_per_s": work / t32, "fp32_kernel_ms": k32_ms,
+            "fp32_main_launches": int(k32_n),
+            "fp64_dropin_sample_orientations": k, "fp64_dropin_sample_s": t64k,
+            "fp64_dropin_kernel_ms": k64_ms,
+            "fp64_dropin_orientations_per_s": args.orient / t64,
+            "speedup_fp32_batched_vs_fp64_dropin": t64 / t32,
+            "max_rel_mueller_err_vs_fp64": mueller_rel_err(f32[0], f64[0], 1e-6),
+            "max_rel_param_err_vs_fp64": perr,
+            "api": "pbt_diff_batch_c (host pointers), wall clock"}
 
 
 def cpu_baseline(geo, beam, th, ph, seconds, nthreads):
@@ -317,6 +373,9 @@ def main():
                             "adjoint_kernel_ms": adj_ms, "adjoint_over_forward": adj_ms / fwd_ms,
                             "adjoint_call_ms": adj_call * 1e3,
                             "value": len(sub) * nb / (adj_ms / 1e3), "unit": UNIT}
+
+    if args.orient > 0 and rank == 0:
+        extra["orientation_average"] = orientation_average(ctx, args)
 
     # FP32 error against the FP64 drop-in on the full workload
     if not args.no_error_check:
