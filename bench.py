@@ -40,6 +40,8 @@ W_FP32 = 170.0   # FP32 flops (FMA = 2)
 W_SFU = 20.0     # special-function ops
 FP32_PER_SM_CLK = 128 * 2   # FP32 lanes x 2 flops
 SFU_PER_SM_CLK = 16
+W_FP64 = 12.0    # FP64 flops (the phase k u.c and its reduction)
+FP64_PER_SM_CLK = 64 * 2    # FP64 lanes x 2 flops
 
 
 def parse():
@@ -388,12 +390,10 @@ def main():
             abs(float(out[2][n]) - float(f64[2][n])) / abs(float(f64[2][n]))
             for n in ("scatt", "asymmetry", "ext"))
 
-    # roofline of the dominant kernel (k2_main_kernel)
+    # roofline of the dominant kernel (k2_main_pk_kernel)
     kms = kern_ms / max(kern_n, 1)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     mhz = clk.get("sm_mhz") or 1965.0
-    peak_fp32 = sms * FP32_PER_SM_CLK * mhz * 1e6
-    ach = W_FP32 * work / (kms / 1e3)
     traffic = None
     prof = os.path.join(ROOT, "profiles", "k2_main_traffic.json")
     if os.path.exists(prof):
@@ -401,13 +401,24 @@ def main():
             traffic = json.load(open(prof)).get("dram_bytes_per_launch_full")
         except Exception:
             traffic = None
-    roof = {"bound": "fp32", "achieved": ach / 1e12, "peak": peak_fp32 / 1e12, "unit": "TFLOP/s",
-            "frac": ach / peak_fp32, "traffic": traffic,
-            "kernel": "k2_main_kernel", "kernel_ms": kms,
-            "peak_basis": "%d SMs x 128 FP32 lanes x 2 flop x %.0f MHz (median sampled SM clock); "
-                          "MEASURED_PEAKS.json has no FP32/SFU figure" % (sms, mhz),
-            "sfu_frac": (W_SFU * work / (kms / 1e3)) / (sms * SFU_PER_SM_CLK * mhz * 1e6),
-            "work_per_facet_bin": {"fp32_flops": W_FP32, "sfu_ops": W_SFU}}
+    # binding term of t_roof = work x max(W_FP32/P_FP32, W_SFU/P_SFU, W_FP64/P_FP64)
+    hz = mhz * 1e6
+    terms = {}
+    for name, w, per_clk, unit in (("fp32", W_FP32, FP32_PER_SM_CLK, "TFLOP/s"),
+                                   ("mufu", W_SFU, SFU_PER_SM_CLK, "Tops/s"),
+                                   ("fp64", W_FP64, FP64_PER_SM_CLK, "TFLOP/s")):
+        a_ = w * work / (kms / 1e3)
+        p_ = sms * per_clk * hz
+        terms[name] = {"achieved": a_ / 1e12, "peak": p_ / 1e12, "unit": unit, "frac": a_ / p_,
+                       "per_facet_bin": w}
+    bound = max(terms, key=lambda n: terms[n]["frac"])
+    roof = {"bound": bound, "achieved": terms[bound]["achieved"], "peak": terms[bound]["peak"],
+            "unit": terms[bound]["unit"], "frac": terms[bound]["frac"], "traffic": traffic,
+            "kernel": "k2_main_pk_kernel", "kernel_ms": kms, "units_per_launch": work,
+            "terms": terms,
+            "peak_basis": "%d SMs x %.0f MHz (median sampled SM clock) x per-clock issue width "
+                          "(FP32 128 lanes, MUFU 16, FP64 64); MEASURED_PEAKS.json has no "
+                          "FP32/MUFU/FP64 figure" % (sms, mhz)}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
