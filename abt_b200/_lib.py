@@ -36,7 +36,8 @@ EXPORTS = ("pbt_ctx_create", "pbt_ctx_destroy", "pbt_last_error_string", "pbt_ve
            "pbt_divide_by_num_orientations_c", "pbt_totals_reset_c", "pbt_diff_batch_c",
            "pbt_diff_batch_dev_c", "pbt_last_launch_count", "pbt_set_kernel_timing",
            "pbt_kernel_time_ms", "pbt_diffraction_noalloc_c", "pbt_set_plan",
-           "pbt_diff_adjoint_c")
+           "pbt_diff_adjoint_c", "pbt_diff_batch_dev_graph_c", "pbt_graph_launch_c",
+           "pbt_graph_kernel_count", "pbt_graph_destroy_c")
 
 
 class PbtError(RuntimeError):
@@ -74,6 +75,11 @@ def lib():
                                  I32, I32, P, P, P, P, P]),
         "pbt_diff_batch_dev_c": (C, [P, P, I64, P, P, P, P, P, I64, P, P, I64, P, I64, P, I64, D,
                                      I32, I32, I32, P, P, P, P, P]),
+        "pbt_diff_batch_dev_graph_c": (C, [P, P, I64, P, P, P, P, P, I64, P, P, I64, P, I64, P,
+                                           I64, D, I32, I32, P, P, P, P, P, P]),
+        "pbt_graph_launch_c": (C, [P, P]),
+        "pbt_graph_kernel_count": (I64, [P]),
+        "pbt_graph_destroy_c": (C, [P]),
         "pbt_last_launch_count": (I64, [P]),
         "pbt_set_kernel_timing": (C, [P, I32]),
         "pbt_kernel_time_ms": (C, [P, ctypes.POINTER(D), ctypes.POINTER(I64)]),

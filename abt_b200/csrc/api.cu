@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <new>
 #include <vector>
 
 #include "frame.h"
@@ -456,21 +457,19 @@ extern "C" int pbt_diff_batch_c(pbt_ctx *ctx, int64_t norient, const pbt_outbeam
     return PBT_OK;
 }
 
-extern "C" int pbt_diff_batch_dev_c(pbt_ctx *ctx, void *stream, int64_t norient,
-                                    const pbt_outbeam *beam, const int64_t *beam_off,
-                                    const pbt_outbeam *ext, const int64_t *ext_off,
-                                    const double *verts, int64_t nverts, const int64_t *face_off,
-                                    const int64_t *face_vi, int64_t nfaces, const double *theta,
-                                    int64_t ntheta, const double *phi, int64_t nphi, double lambda,
-                                    int32_t is_fast_diff, int32_t scaling, int32_t precision,
-                                    const pbt_output_params *params_in, double *mueller_avg,
-                                    double *mueller_1d_avg, pbt_output_params *params_avg,
-                                    pbt_output_params *params_per_orient) {
-    clear_error();
-    PBT_TRY(check_ctx(ctx));
-    std::lock_guard<std::mutex> lock_(ctx->mu);
+namespace {
+
+// Checks and enqueue of the device-pointer batch; copy_face_off = false when
+// the face offsets are already on the device (a graph capture reuses them).
+int dev_batch_enqueue(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam *beam,
+                      const int64_t *beam_off, const pbt_outbeam *ext, const int64_t *ext_off,
+                      const double *verts, int64_t nverts, const int64_t *face_off,
+                      const int64_t *face_vi, int64_t nfaces, const double *theta, int64_t ntheta,
+                      const double *phi, int64_t nphi, double lambda, int32_t is_fast_diff,
+                      int32_t scaling, int32_t precision, const pbt_output_params *params_in,
+                      double *mueller_avg, double *mueller_1d_avg, pbt_output_params *params_avg,
+                      pbt_output_params *params_per_orient, bool copy_face_off) {
     ctx->launches = 0;
-    cudaStream_t st = (cudaStream_t)stream;
     PBT_TRY(batch_common_checks(ctx, norient, beam_off, ext_off, face_off, nfaces, theta, ntheta,
                                 phi, nphi, lambda, precision, mueller_avg, mueller_1d_avg,
                                 params_avg, params_in));
@@ -487,11 +486,159 @@ extern "C" int pbt_diff_batch_dev_c(pbt_ctx *ctx, void *stream, int64_t norient,
     PBT_TRY(check_grid_ready(ctx));
     // the face offsets are needed on the device too
     PBT_TRY(ctx->d_items.ensure((nfaces + 1) * 8));
-    PBT_CUDA_TRY(cudaMemcpyAsync(ctx->d_items.p, face_off, (nfaces + 1) * 8, cudaMemcpyHostToDevice, st));
+    if (copy_face_off)
+        PBT_CUDA_TRY(cudaMemcpyAsync(ctx->d_items.p, face_off, (nfaces + 1) * 8,
+                                     cudaMemcpyHostToDevice, st));
     return k2_batch_impl(ctx, st, norient, beam, beam_off, ext, ext_off, verts, nverts, face_off,
                          ctx->d_items.as<int64_t>(), face_vi, nfaces, lambda, is_fast_diff ? 1 : 0,
                          scaling ? 1 : 0, params_in, mueller_avg, mueller_1d_avg, params_avg,
                          params_per_orient, 0);
+}
+
+}  // namespace
+
+extern "C" int pbt_diff_batch_dev_c(pbt_ctx *ctx, void *stream, int64_t norient,
+                                    const pbt_outbeam *beam, const int64_t *beam_off,
+                                    const pbt_outbeam *ext, const int64_t *ext_off,
+                                    const double *verts, int64_t nverts, const int64_t *face_off,
+                                    const int64_t *face_vi, int64_t nfaces, const double *theta,
+                                    int64_t ntheta, const double *phi, int64_t nphi, double lambda,
+                                    int32_t is_fast_diff, int32_t scaling, int32_t precision,
+                                    const pbt_output_params *params_in, double *mueller_avg,
+                                    double *mueller_1d_avg, pbt_output_params *params_avg,
+                                    pbt_output_params *params_per_orient) {
+    clear_error();
+    PBT_TRY(check_ctx(ctx));
+    std::lock_guard<std::mutex> lock_(ctx->mu);
+    return dev_batch_enqueue(ctx, (cudaStream_t)stream, norient, beam, beam_off, ext, ext_off,
+                             verts, nverts, face_off, face_vi, nfaces, theta, ntheta, phi, nphi,
+                             lambda, is_fast_diff, scaling, precision, params_in, mueller_avg,
+                             mueller_1d_avg, params_avg, params_per_orient, true);
+}
+
+// A CUDA graph of the device-pointer batch.  The graph owns a private context
+// (its scratch buffers, bin tables and staged offsets), so nothing else
+// writes what a replay reads; the caller's device arrays are baked in by
+// address and read at every replay.
+struct pbt_graph {
+    pbt_ctx *gctx = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0;
+    int device = 0;
+};
+
+extern "C" int pbt_diff_batch_dev_graph_c(pbt_ctx *ctx, void *stream, int64_t norient,
+                                          const pbt_outbeam *beam, const int64_t *beam_off,
+                                          const pbt_outbeam *ext, const int64_t *ext_off,
+                                          const double *verts, int64_t nverts,
+                                          const int64_t *face_off, const int64_t *face_vi,
+                                          int64_t nfaces, const double *theta, int64_t ntheta,
+                                          const double *phi, int64_t nphi, double lambda,
+                                          int32_t is_fast_diff, int32_t scaling,
+                                          const pbt_output_params *params_in,
+                                          double *mueller_avg, double *mueller_1d_avg,
+                                          pbt_output_params *params_avg,
+                                          pbt_output_params *params_per_orient, pbt_graph **out) {
+    clear_error();
+    PBT_TRY(check_ctx(ctx));
+    if (!out) {
+        set_error("graph: out must not be NULL");
+        return PBT_EINVAL;
+    }
+    *out = nullptr;
+    PBT_CUDA_TRY(cudaSetDevice(ctx->device));
+    pbt_ctx *g = nullptr;
+    PBT_TRY(pbt_ctx_create(ctx->device, &g));
+    g->plan_variant = ctx->plan_variant;
+    g->plan_bpt = ctx->plan_bpt;
+    g->plan_rpi = ctx->plan_rpi;
+    cudaStream_t st = (cudaStream_t)stream;
+    auto fail = [&](int rc) {
+        pbt_ctx_destroy(g);
+        return rc;
+    };
+    auto cfail = [&](const char *what, cudaError_t e) {
+        set_error("%s failed: %s", what, cudaGetErrorString(e));
+        return fail(e == cudaErrorMemoryAllocation ? PBT_ENOMEM : PBT_ECUDA);
+    };
+    cudaError_t e;
+    // a plain run sizes every buffer, stages the offsets and fills the bin tables
+    int rc = dev_batch_enqueue(g, st, norient, beam, beam_off, ext, ext_off, verts, nverts,
+                               face_off, face_vi, nfaces, theta, ntheta, phi, nphi, lambda,
+                               is_fast_diff, scaling, PBT_PREC_FP32, params_in, mueller_avg,
+                               mueller_1d_avg, params_avg, params_per_orient, true);
+    if (rc != PBT_OK) return fail(rc);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cfail("graph warm-up", e);
+    cudaStream_t cs = nullptr;
+    if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess)
+        return cfail("cudaStreamCreateWithFlags", e);
+    g->capturing = true;
+    cudaGraph_t graph = nullptr;
+    if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed)) != cudaSuccess) {
+        g->capturing = false;
+        cudaStreamDestroy(cs);
+        return cfail("cudaStreamBeginCapture", e);
+    }
+    rc = dev_batch_enqueue(g, cs, norient, beam, beam_off, ext, ext_off, verts, nverts, face_off,
+                           face_vi, nfaces, theta, ntheta, phi, nphi, lambda, is_fast_diff,
+                           scaling, PBT_PREC_FP32, params_in, mueller_avg, mueller_1d_avg,
+                           params_avg, params_per_orient, false);
+    const cudaError_t ce = cudaStreamEndCapture(cs, &graph);
+    g->capturing = false;
+    cudaStreamDestroy(cs);
+    if (rc != PBT_OK || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        (void)cudaGetLastError();
+        if (rc == PBT_OK) {
+            set_error("graph capture failed: %s", cudaGetErrorString(ce));
+            rc = PBT_ECUDA;
+        }
+        return fail(rc);
+    }
+    cudaGraphExec_t exec = nullptr;
+    if ((e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return cfail("cudaGraphInstantiate", e);
+    }
+    pbt_graph *G = new (std::nothrow) pbt_graph;
+    if (!G) {
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        set_error("graph: out of host memory");
+        return fail(PBT_ENOMEM);
+    }
+    G->gctx = g;
+    G->graph = graph;
+    G->exec = exec;
+    G->launches = g->launches;
+    G->device = ctx->device;
+    *out = G;
+    return PBT_OK;
+}
+
+extern "C" int pbt_graph_launch_c(pbt_graph *G, void *stream) {
+    clear_error();
+    if (!G || !G->exec) {
+        set_error("graph: NULL or destroyed graph");
+        return PBT_EINVAL;
+    }
+    PBT_CUDA_TRY(cudaSetDevice(G->device));
+    PBT_CUDA_TRY(cudaGraphLaunch(G->exec, (cudaStream_t)stream));
+    return PBT_OK;
+}
+
+extern "C" int64_t pbt_graph_kernel_count(const pbt_graph *G) { return G ? G->launches : -1; }
+
+extern "C" int pbt_graph_destroy_c(pbt_graph *G) {
+    clear_error();
+    if (!G) return PBT_OK;
+    cudaSetDevice(G->device);
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    if (G->graph) cudaGraphDestroy(G->graph);
+    pbt_ctx_destroy(G->gctx);
+    delete G;
+    return PBT_OK;
 }
 
 namespace pbt {

@@ -62,7 +62,7 @@ void HostBuf::release() {
 }
 
 void timing_begin(pbt_ctx *ctx, cudaStream_t st) {
-    if (!ctx->timing) return;
+    if (!ctx->timing || ctx->capturing) return;
     if (ctx->ev_used + 2 > ctx->ev.size()) {
         for (int i = 0; i < 2; i++) {
             cudaEvent_t e;
@@ -77,7 +77,7 @@ void timing_begin(pbt_ctx *ctx, cudaStream_t st) {
 }
 
 void timing_end(pbt_ctx *ctx, cudaStream_t st) {
-    if (!ctx->timing || ctx->ev_used + 2 > ctx->ev.size()) return;
+    if (!ctx->timing || ctx->capturing || ctx->ev_used + 2 > ctx->ev.size()) return;
     cudaEventRecord(ctx->ev[ctx->ev_used + 1], st);
     ctx->ev_used += 2;
 }

@@ -734,7 +734,6 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     const float2 rs = make_float2(rsqrtf(tt.x), rsqrtf(tt.y));
     const float2 s = mul2(tt, rs);
     const float2 kyrs = mul2(kyc, rs);
-    const float2 m0 = neg2(mul2(kx, kyrs)), m1 = s, m2 = neg2(mul2(kz, kyrs));
     const float2 d = fma2(P.hkz_cf, s, neg2(mul2(mul2(kz, rs), P.hicf)));
     const float2 e = fma2(P.hkxky_cf, s, neg2(mul2(mul2(kx, kyrs), P.hicf)));
     float2 qx = kx, qy = kyc, qz = kz;
@@ -754,27 +753,34 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
         qy = sel2(bx, by, vy, qy);
         qz = sel2(bx, by, vz, qz);
     }
-    float2 hx = fma2(P.inc[1], qz, neg2(mul2(P.inc[2], qy)));
-    float2 hy = fma2(P.inc[2], qx, neg2(mul2(P.inc[0], qz)));
-    float2 hz = fma2(P.inc[0], qy, neg2(mul2(P.inc[1], qx)));
+    // hc = h / |h| with h = inc x q; p = hc.m, rr = hc.evo2
+    const float2 hx = fma2(P.inc[1], qz, neg2(mul2(P.inc[2], qy)));
+    const float2 hy = fma2(P.inc[2], qx, neg2(mul2(P.inc[0], qz)));
+    const float2 hz = fma2(P.inc[0], qy, neg2(mul2(P.inc[1], qx)));
     const float2 hn2 = fma2(hz, hz, fma2(hy, hy, mul2(hx, hx)));
     const float2 hn = make_float2(rsqrtf(hn2.x), rsqrtf(hn2.y));
-    hx = mul2(hx, hn);
-    hy = mul2(hy, hn);
-    hz = mul2(hz, hn);
-    float2 ex = fma2(kyc, m2, neg2(mul2(kz, m1)));
-    float2 ey = fma2(kz, m0, neg2(mul2(kx, m2)));
-    float2 ez = fma2(kx, m1, neg2(mul2(kyc, m0)));
     const bool cx = tt.x <= kOneMinusClampSq, cy = tt.y <= kOneMinusClampSq;
-    if (cx || cy) {
+    float2 p, rr;
+    if (!(cx || cy)) {
+        // unit k, |ky| inside the clamp: evo2 = k x m = (-kz, 0, kx) / s, so
+        // p = hy s - (ky/s)(hx kx + hz kz) and rr = (hz kx - hx kz) / s, over |h|
+        const float2 t = fma2(hx, kx, mul2(hz, kz));
+        p = mul2(hn, fma2(hy, s, neg2(mul2(kyrs, t))));
+        rr = mul2(mul2(hn, rs), fma2(hz, kx, neg2(mul2(hx, kz))));
+    } else {
+        // a lane on the clamp: evo2 = normalise(k x m) with the clamped ky
+        const float2 m0 = neg2(mul2(kx, kyrs)), m1 = s, m2 = neg2(mul2(kz, kyrs));
+        float2 ex = fma2(kyc, m2, neg2(mul2(kz, m1)));
+        float2 ey = fma2(kz, m0, neg2(mul2(kx, m2)));
+        float2 ez = fma2(kx, m1, neg2(mul2(kyc, m0)));
         const float2 en2 = fma2(ez, ez, fma2(ey, ey, mul2(ex, ex)));
         const float2 ne = make_float2(cx ? rsqrtf(en2.x) : 1.0f, cy ? rsqrtf(en2.y) : 1.0f);
         ex = mul2(ex, ne);
         ey = mul2(ey, ne);
         ez = mul2(ez, ne);
+        p = mul2(hn, fma2(hz, m2, fma2(hy, m1, mul2(hx, m0))));
+        rr = mul2(hn, fma2(hz, ez, fma2(hy, ey, mul2(hx, ex))));
     }
-    const float2 p = fma2(hz, m2, fma2(hy, m1, mul2(hx, m0)));
-    const float2 rr = fma2(hz, ez, fma2(hy, ey, mul2(hx, ex)));
     const float2 A = fma2(p, d, mul2(rr, e));
     const float2 Bc = fma2(p, e, neg2(mul2(rr, d)));
     const float2 nB = neg2(Bc);
@@ -802,7 +808,7 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     }
 }
 
-constexpr int K2P_CH = 16;  // record pairs per shared-memory stage (32 records)
+constexpr int K2P_CH = 32;  // record pairs per shared-memory stage (64 records)
 
 struct K2PkArgs {
     const K2Pair *pairs;
@@ -910,10 +916,12 @@ __global__ void __launch_bounds__(K2_THREADS) k2_main_pk_kernel(K2PkArgs P) {
             for (int q = 0; q < BPT; q++)
 #pragma unroll
                 for (int cc = 0; cc < 8; cc++) acc[q][cc] = bc2(0.0f);
+            // only the item's first pair (odd rbeg) and last pair (odd rend) are partial
+            const int j_lo = (c == 0 && (rbeg & 1)) ? 0 : -1;
+            const int j_hi = (c == nchunk - 1 && (rend & 1)) ? n - 1 : -1;
             for (int j = 0; j < n; j++) {
-                const int64_t pi = p0 + c * K2P_CH + j;
-                const bool lo_ok = 2 * pi >= rbeg, hi_ok = 2 * pi + 1 < rend;
-                const K2Fov *fv = FAST ? P.fovs + 2 * pi : nullptr;
+                const bool lo_ok = j != j_lo, hi_ok = j != j_hi;
+                const K2Fov *fv = FAST ? P.fovs + 2 * (p0 + c * K2P_CH + j) : nullptr;
 #pragma unroll
                 for (int q = 0; q < BPT; q++)
                     k2_pair<FAST>(sbuf[st][j], fv, bd[q], acc[q], nk, hkR, lo_ok && valid[q],
@@ -1257,7 +1265,7 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
     S.fovs = fast_diff ? (K2Fov *)(ctx->d_rec.as<char>() + align_up(rec_bytes)) : nullptr;
     // host-side offsets -> device (pinned staging; the previous call's copy
     // out of the staging buffer must have run before it is overwritten)
-    if (ctx->stage_pending) {
+    if (ctx->stage_pending && !ctx->capturing) {
         PBT_CUDA_TRY(cudaEventSynchronize(ctx->stage_ev));
         ctx->stage_pending = false;
     }
@@ -1274,8 +1282,10 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
                                  cudaMemcpyHostToDevice, st));
     PBT_CUDA_TRY(cudaMemcpyAsync(S.ext_off, hs + 2 * (norient + 1), (norient + 1) * 8,
                                  cudaMemcpyHostToDevice, st));
-    PBT_CUDA_TRY(cudaEventRecord(ctx->stage_ev, st));
-    ctx->stage_pending = true;
+    if (!ctx->capturing) {
+        PBT_CUDA_TRY(cudaEventRecord(ctx->stage_ev, st));
+        ctx->stage_pending = true;
+    }
     PBT_CUDA_TRY(cudaMemsetAsync(S.err, 0, sizeof(int), st));
     RefSrc src{d_beam, d_ext, S.beam_off, S.ext_off, S.refbase, norient};
     const int th = 256;

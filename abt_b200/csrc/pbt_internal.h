@@ -122,6 +122,8 @@ struct pbt_ctx {
     // CUDA-event timing of the far-field kernels
     bool timing = false;
     std::vector<cudaEvent_t> ev;  // start/stop pairs
+    // set while a graph captures this context's enqueue: no host waits, no events
+    bool capturing = false;
     size_t ev_used = 0;
 };
 

@@ -287,3 +287,43 @@ def diff_batch_dev(ctx, stream, norient, d_beam, beam_off, d_ext, ext_off, d_ver
         ptr(phi), len(phi), float(lam), int(bool(is_fast_diff)), int(bool(scaling)),
         PBT_PREC_FP32, ptr(d_params_in), ptr(d_mueller_avg), ptr(d_m1d_avg), ptr(d_params_avg),
         ptr(d_params_per)))
+
+
+class BatchGraph:
+    """pbt_diff_batch_dev_graph_c: the device-pointer FP32 batch captured as a
+    CUDA graph.  Construction runs the batch once and captures it; launch()
+    replays it on a stream (the device arrays are re-read at every replay)."""
+
+    def __init__(self, ctx, stream, norient, d_beam, beam_off, d_ext, ext_off, d_verts, nverts,
+                 face_off, d_face_vi, theta, phi, lam, d_params_in, d_mueller_avg, d_m1d_avg,
+                 d_params_avg, d_params_per=None, is_fast_diff=False, scaling=False):
+        boff = np.ascontiguousarray(beam_off, dtype=np.int64)
+        eoff = np.ascontiguousarray(ext_off, dtype=np.int64)
+        fo = np.ascontiguousarray(face_off, dtype=np.int64)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        h = ctypes.c_void_p()
+        check(_lib.lib().pbt_diff_batch_dev_graph_c(
+            ctx.handle, stream, int(norient), ptr(d_beam), ptr(boff), ptr(d_ext), ptr(eoff),
+            ptr(d_verts), int(nverts), ptr(fo), ptr(d_face_vi), len(fo) - 1, ptr(theta),
+            len(theta), ptr(phi), len(phi), float(lam), int(bool(is_fast_diff)),
+            int(bool(scaling)), ptr(d_params_in), ptr(d_mueller_avg), ptr(d_m1d_avg),
+            ptr(d_params_avg), ptr(d_params_per), ctypes.byref(h)))
+        self._h = h
+
+    def launch(self, stream):
+        check(_lib.lib().pbt_graph_launch_c(self._h, stream))
+
+    def kernel_count(self):
+        return int(_lib.lib().pbt_graph_kernel_count(self._h))
+
+    def close(self):
+        if self._h:
+            _lib.lib().pbt_graph_destroy_c(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-graph", action="store_true",
+                    help="enqueue each step through the C ABI instead of replaying a CUDA graph")
     ap.add_argument("--orient", type=int, default=1024,
                     help="orientations of the rough-column orientation average (0: skip)")
     ap.add_argument("--orient-fp64", type=int, default=16,
@@ -281,18 +283,40 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
     stream = torch.cuda.current_stream(dev)
 
-    def step():
+    def direct():
         diff_batch_dev(ctx, stream.cuda_stream, 1, d_beam, boff, d_ext, eoff, d_verts, nverts,
                        geo["face_off"], d_fvi, th, ph, LAM, d_pin, d_mu, d_m1, d_pav, d_pper)
+
+    # the step: one replay of the batch captured as a CUDA graph (the capture
+    # runs the batch once); --no-graph enqueues it through the C ABI instead
+    graph = None
+    if not args.no_graph:
+        from abt_b200.diff import BatchGraph
+        graph = BatchGraph(ctx, stream.cuda_stream, 1, d_beam, boff, d_ext, eoff, d_verts, nverts,
+                           geo["face_off"], d_fvi, th, ph, LAM, d_pin, d_mu, d_m1, d_pav, d_pper)
+        step_kernels = graph.kernel_count()
+
+        def step():
+            graph.launch(stream.cuda_stream)
+    else:
+        step = direct
 
     for _ in range(max(3, args.warmup)):
         flush.zero_()
         step()
     torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
+    # kernel time of the far-field kernel (CUDA events inside the library), same
+    # conditions as a step: L2 flushed before each call
     ctx.set_kernel_timing(True)
     ctx.kernel_time_ms()
+    for _ in range(2):
+        flush.zero_()
+        direct()
+    torch.cuda.synchronize()
+    kern_ms, kern_n = ctx.kernel_time_ms()
+    ctx.set_kernel_timing(False)
+    if dist is not None:
+        dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
     launches = 0
@@ -302,13 +326,13 @@ def main():
     for _ in range(args.steps):
         flush.zero_()
         step()
-        launches += ctx.last_launch_count()
+        launches += step_kernels if graph is not None else ctx.last_launch_count()
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
     ms_total = e0.elapsed_time(e1)
-    kern_ms, kern_n = ctx.kernel_time_ms()
-    ctx.set_kernel_timing(False)
+    if graph is not None:
+        graph.close()
     if dist is not None:
         t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -431,7 +455,9 @@ def main():
                                    "721 theta x 360 phi, lambda 0.532 um, FP32 with FP64 phase",
                        "facets": nf, "bins": nb, "orientations_per_step": 1,
                        "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "256 MB buffer written before every step, inside the timed region"},
+                       "l2": "256 MB buffer written before every step, inside the timed region",
+                       "step": "CUDA graph replay of pbt_diff_batch_dev_c" if not args.no_graph
+                               else "pbt_diff_batch_dev_c"},
             "orientations_per_s": world * 1e3 / ms_step,
             "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof,
             "cpu_baseline": cpu}

@@ -206,6 +206,31 @@ int pbt_diff_batch_dev_c(pbt_ctx *ctx, void *stream, int64_t norient, const pbt_
                          double *mueller_1d_avg, pbt_output_params *params_avg,
                          pbt_output_params *params_per_orient);
 
+/* CUDA graph of pbt_diff_batch_dev_c (no counterpart in the reference: the
+ * orientation loop of src/pbt_seq_mod.f90:146-274 as one replayable graph).
+ * Runs the batch once (the outputs hold its result), then captures the same
+ * enqueue into a graph that owns private scratch, bin tables and staged
+ * offsets.  The device arrays are baked in by address: refill them in place
+ * and call pbt_graph_launch_c to recompute; the host arrays (offsets, face
+ * offsets, theta, phi) are read only here.  One replay at a time per graph
+ * (replays share its scratch); the arrays must outlive the graph. */
+typedef struct pbt_graph pbt_graph;
+int pbt_diff_batch_dev_graph_c(pbt_ctx *ctx, void *stream, int64_t norient,
+                               const pbt_outbeam *beam, const int64_t *beam_off,
+                               const pbt_outbeam *ext, const int64_t *ext_off,
+                               const double *verts, int64_t nverts, const int64_t *face_off,
+                               const int64_t *face_vi, int64_t nfaces, const double *theta,
+                               int64_t ntheta, const double *phi, int64_t nphi, double lambda,
+                               int32_t is_fast_diff, int32_t scaling,
+                               const pbt_output_params *params_in, double *mueller_avg,
+                               double *mueller_1d_avg, pbt_output_params *params_avg,
+                               pbt_output_params *params_per_orient, pbt_graph **out);
+/* Replay on `stream` (a cudaStream_t); returns without synchronising. */
+int pbt_graph_launch_c(pbt_graph *graph, void *stream);
+/* Kernels one replay launches. */
+int64_t pbt_graph_kernel_count(const pbt_graph *graph);
+int pbt_graph_destroy_c(pbt_graph *graph);
+
 /* ---------------------------------------------------------- introspection */
 
 /* Number of kernel launches made by the last completed compute call on this
