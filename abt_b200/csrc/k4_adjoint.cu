@@ -57,22 +57,25 @@ enum {
     A_CE = 35,     // 1: sum of the coefficient of 2 c / R^2 in c_bar
 };
 
+// packed accumulator pairs: (TKX_j, TKY_j) and (WU_i0, WU_i1)
+enum { P_TK = 0, P_WU01 = 3, K4_NPAIR = 6 };
+
 struct K4Rec {
     double kc[3];
     float eps[3], b, R[9], ea[3], kp[2], p2[3], cf, icf, inc[3], xa[3], ya[3], amp[8];
 };
 
-// Per-bin inputs in HBM: 48 B, three 16-byte loads.
+// Per-bin input in HBM: the unit bin direction in FP64, 32 B (two 16-byte
+// loads).  The forward-bodge direction (same phi, first row above 1 degree)
+// is read from the same table inside the (rare) bodge branch.
 struct __align__(16) K4Bin {
-    double ux, uy, uz;  // unit bin direction, FP64
-    float fx, fy;       // the same in FP32
-    float hx, hy, hz;   // forward-bodge direction (same phi, first row above 1 degree)
-    float fz;
+    double ux, uy, uz, pad;
 };
 
 struct Bin4 {
     double ux, uy, uz;
-    float fx, fy, fz, hx, hy, hz;
+    float fx, fy, fz;
+    int64_t o;     // bin index
     float2 G[4];   // cotangent of S' (pre-T, common phase removed) for the record's kind
     float2 Gm[4];  // -i G
 };
@@ -129,14 +132,15 @@ __device__ __forceinline__ void dd_grad(float t0, float t1, float t2, float2 &g,
         float sc1, dsc1, sc2, dsc2;
         sinc_d(h1, a2 * rD, sc1, dsc1);
         sinc_d(h2, a1 * rD, sc2, dsc2);
-        // E = i e^{ic} sinc(h): (-s sc, c sc); dE/dc = i E; dE/dh = i e^{ic} sinc'(h)
-        const float2 E1 = make_float2(-s1 * sc1, c1 * sc1), E2 = make_float2(-s2 * sc2, c2 * sc2);
-        const float2 iE1 = make_float2(-E1.y, E1.x), iE2 = make_float2(-E2.y, E2.x);
-        const float2 H1 = make_float2(-s1 * dsc1, c1 * dsc1), H2 = make_float2(-s2 * dsc2, c2 * dsc2);
-        g = make_float2((E2.x - E1.x) * iD, (E2.y - E1.y) * iD);
-        // d g1/d lo = (iE1 - H1)/2, d g1/d mid = (iE1 + H1)/2, d g2/d mid = (iE2 - H2)/2, d g2/d hi = (iE2 + H2)/2
-        dlo = make_float2((-(0.5f * (iE1.x - H1.x)) + g.x) * iD, (-(0.5f * (iE1.y - H1.y)) + g.y) * iD);
-        dhi = make_float2((0.5f * (iE2.x + H2.x) - g.x) * iD, (0.5f * (iE2.y + H2.y) - g.y) * iD);
+        // E = i e^{ic} sinc(h) = sc n with n = i e^{ic} = (-s, c); dE/dc = i E = sc (i n),
+        // i n = (-c, -s); dE/dh = dsc n.  g = (E2 - E1) / D,
+        // dg/dlo = (g - (iE1 - H1)/2) / D, dg/dhi = ((iE2 + H2)/2 - g) / D
+        const float2 n1 = make_float2(-s1, c1), n2 = make_float2(-s2, c2);
+        const float2 in1 = make_float2(-c1, -s1), in2 = make_float2(-c2, -s2);
+        const float2 iD2 = bc2(iD);
+        g = mul2(fma2(bc2(sc2), n2, mul2(bc2(-sc1), n1)), iD2);
+        dlo = mul2(fma2(bc2(0.5f * dsc1), n1, fma2(bc2(-0.5f * sc1), in1, g)), iD2);
+        dhi = mul2(fma2(bc2(0.5f * dsc2), n2, fma2(bc2(0.5f * sc2), in2, make_float2(-g.x, -g.y))), iD2);
     }
     if (D < 0.25f) {
         // series about mid: g = e^{i mid} sum_n c_n h_n(ya, yc), c_n = i^(n+2)/(n+2)!
@@ -189,14 +193,16 @@ __device__ __forceinline__ Dir4 dir4(const K4Rec &r, float fx, float fy, float f
 // frame outer product and ea accumulators; returns the cotangents of
 // a = u.c/R (ab) and b = |c|^2/R^2 (bb) for the caller's c terms.
 __device__ __forceinline__ void dir4_back(const K4Rec &r, const Dir4 &d, const float kb[3], float fx,
-                                          float fy, float fz, float *acc, float &ab, float &bb) {
-    const float u[3] = {fx, fy, fz};
+                                          float fy, float fz, float *acc, float2 *accP, float &ab,
+                                          float &bb) {
+    const float2 u01 = make_float2(fx, fy);
     float opa2b = 0.0f, opab = 0.0f;
     for (int i = 0; i < 3; i++) {
         const float wb = kb[i] * d.opa2;
         opa2b = fmaf(kb[i], d.w[i], opa2b);
         opab = fmaf(-kb[i], r.ea[i], opab);
-        for (int j = 0; j < 3; j++) acc[A_WU + 3 * i + j] = fmaf(wb, u[j], acc[A_WU + 3 * i + j]);
+        accP[P_WU01 + i] = fma2(bc2(wb), u01, accP[P_WU01 + i]);
+        acc[A_WU + 3 * i + 2] = fmaf(wb, fz, acc[A_WU + 3 * i + 2]);
         acc[A_EA + i] = fmaf(-kb[i], d.opa, acc[A_EA + i]);
     }
     ab = opab + opa2b * fmaf(3.0f, d.a, 1.0f);
@@ -206,7 +212,9 @@ __device__ __forceinline__ void dir4_back(const K4Rec &r, const Dir4 &d, const f
 // Cotangent contributions of one (record, bin).
 template <bool FAST>
 __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, float hkR, float iRf,
-                                        float cosfov, const float *p0, float *acc, float2 *accA) {
+                                        float cosfov, const float *p0, const K4Bin *__restrict__ bins,
+                                        int64_t nphi, int64_t theta_i, float *acc, float2 *accA,
+                                        float2 *accP) {
     // forward
     const double ka = fma(B.uz, r.kc[2], fma(B.uy, r.kc[1], B.ux * r.kc[0]));
     const double nq = fma(ka, kInv2Pi4, kMagic4) - kMagic4;
@@ -231,7 +239,8 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const bool floored = !(traw > kClampSq4);
     const float tt = floored ? kClampSq4 : traw;
     const float rs = rsqrtf(tt), s = tt * rs;
-    const float m[3] = {-kx * kyc * rs, s, -kz * kyc * rs};
+    const float kyrs = kyc * rs;
+    const float m[3] = {-kx * kyrs, s, -kz * kyrs};
     const float dd = fmaf(-0.5f * Kz * cf, s, -0.5f * kz * rs * rcf);
     const float ee = fmaf(0.5f * Kx * Ky * cf, s, -0.5f * kx * kyc * rs * rcf);
     const float kc3[3] = {kx, kyc, kz};
@@ -239,8 +248,13 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const bool bodge = !(fabsf(dinc) < 0.999f);
     Dir4 dh;
     float q[3] = {kx, kyc, kz};
+    float hx = 0.0f, hy = 0.0f, hz = 0.0f;
     if (bodge) {
-        dh = dir4(r, B.hx, B.hy, B.hz);
+        const K4Bin hb = bins[B.o % nphi + nphi * theta_i];
+        hx = (float)hb.ux;
+        hy = (float)hb.uy;
+        hz = (float)hb.uz;
+        dh = dir4(r, hx, hy, hz);
         q[0] = dh.k[0];
         q[1] = dh.k[1];
         q[2] = dh.k[2];
@@ -248,13 +262,26 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const float hr[3] = {fmaf(r.inc[1], q[2], -r.inc[2] * q[1]), fmaf(r.inc[2], q[0], -r.inc[0] * q[2]),
                          fmaf(r.inc[0], q[1], -r.inc[1] * q[0])};
     const float hn = rsqrtf(fmaf(hr[2], hr[2], fmaf(hr[1], hr[1], hr[0] * hr[0])));
-    const float hc[3] = {hr[0] * hn, hr[1] * hn, hr[2] * hn};
-    const float vr[3] = {fmaf(kyc, m[2], -kz * m[1]), fmaf(kz, m[0], -kx * m[2]), fmaf(kx, m[1], -kyc * m[0])};
-    float vn = 1.0f;
-    if (floored) vn = rsqrtf(fmaf(vr[2], vr[2], fmaf(vr[1], vr[1], vr[0] * vr[0])));
-    const float ev[3] = {vr[0] * vn, vr[1] * vn, vr[2] * vn};
-    const float pp = fmaf(hc[2], m[2], fmaf(hc[1], m[1], hc[0] * m[0]));
-    const float rr = fmaf(hc[2], ev[2], fmaf(hc[1], ev[1], hc[0] * ev[0]));
+    // p = hc.m, rr = hc.evo2 with hc = hr hn.  Inside the clamp k is a unit
+    // vector and evo2 = k x m = (-kz, 0, kx) / s, so p = hn (hy s - ky T1 / s),
+    // T1 = hx kx + hz kz, and rr = hn (hz kx - hx kz) / s.
+    float pp, rr, T1 = 0.0f, P0 = 0.0f, R0 = 0.0f;
+    float hc[3], ev[3], vn = 1.0f;
+    if (!floored) {
+        T1 = fmaf(hr[0], kx, hr[2] * kz);
+        P0 = fmaf(hr[1], s, -kyrs * T1);
+        R0 = fmaf(hr[2], kx, -hr[0] * kz);
+        pp = hn * P0;
+        rr = hn * rs * R0;
+    } else {
+        for (int i = 0; i < 3; i++) hc[i] = hr[i] * hn;
+        const float vr[3] = {fmaf(kyc, m[2], -kz * m[1]), fmaf(kz, m[0], -kx * m[2]),
+                             fmaf(kx, m[1], -kyc * m[0])};
+        vn = rsqrtf(fmaf(vr[2], vr[2], fmaf(vr[1], vr[1], vr[0] * vr[0])));
+        for (int i = 0; i < 3; i++) ev[i] = vr[i] * vn;
+        pp = fmaf(hc[2], m[2], fmaf(hc[1], m[1], hc[0] * m[0]));
+        rr = fmaf(hc[2], ev[2], fmaf(hc[1], ev[1], hc[0] * ev[0]));
+    }
     const float A = fmaf(pp, dd, rr * ee), Bm = fmaf(pp, ee, -rr * dd);
     // W = [[A, B], [-B, A]] amp' ; complex order (1,1),(2,1),(1,2),(2,2)
     const float2 *a = reinterpret_cast<const float2 *>(r.amp);
@@ -286,33 +313,45 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     // A = pp dd + rr ee, B = pp ee - rr dd
     const float ppb = fmaf(Ab, dd, Bb * ee), rrb = fmaf(Ab, ee, -Bb * dd);
     const float ddb = fmaf(Ab, pp, -Bb * rr), eeb = fmaf(Ab, rr, Bb * pp);
-    float hcb[3], mb[3], evb[3];
-    for (int i = 0; i < 3; i++) {
-        hcb[i] = fmaf(ppb, m[i], rrb * ev[i]);
-        mb[i] = ppb * hc[i];
-        evb[i] = rrb * hc[i];
-    }
-    // ev = vr * vn (normalised only when floored)
-    float vrb[3];
-    if (floored) {
-        const float dp = evb[0] * ev[0] + evb[1] * ev[1] + evb[2] * ev[2];
-        for (int i = 0; i < 3; i++) vrb[i] = (evb[i] - dp * ev[i]) * vn;
+    float hrb[3], kxb, kycb, kzb, sbm;  // sbm: cotangent of s from p and rr
+    if (!floored) {
+        const float Pb = ppb * hn, Rb = rrb * hn * rs;
+        const float hn3 = -fmaf(ppb, P0, rrb * rs * R0) * hn * hn * hn;
+        const float T1b = -Pb * kyrs;
+        hrb[0] = fmaf(T1b, kx, fmaf(-Rb, kz, hn3 * hr[0]));
+        hrb[1] = fmaf(Pb, s, hn3 * hr[1]);
+        hrb[2] = fmaf(T1b, kz, fmaf(Rb, kx, hn3 * hr[2]));
+        kxb = fmaf(T1b, hr[0], Rb * hr[2]);
+        kzb = fmaf(T1b, hr[2], -Rb * hr[0]);
+        kycb = -Pb * rs * T1;
+        sbm = fmaf(Pb, fmaf(kyc * T1, rs * rs, hr[1]), -Rb * R0 * rs);
     } else {
-        for (int i = 0; i < 3; i++) vrb[i] = evb[i];
-    }
-    // vr = kc3 x m
-    float kcb[3];
-    kcb[0] = m[1] * vrb[2] - m[2] * vrb[1];
-    kcb[1] = m[2] * vrb[0] - m[0] * vrb[2];
-    kcb[2] = m[0] * vrb[1] - m[1] * vrb[0];
-    mb[0] += vrb[1] * kc3[2] - vrb[2] * kc3[1];
-    mb[1] += vrb[2] * kc3[0] - vrb[0] * kc3[2];
-    mb[2] += vrb[0] * kc3[1] - vrb[1] * kc3[0];
-    // hc = hr * hn ; hr = inc x q
-    float hrb[3];
-    {
+        float hcb[3], mb[3], evb[3];
+        for (int i = 0; i < 3; i++) {
+            hcb[i] = fmaf(ppb, m[i], rrb * ev[i]);
+            mb[i] = ppb * hc[i];
+            evb[i] = rrb * hc[i];
+        }
+        // ev = vr * vn ; vr = kc3 x m
+        float vrb[3];
+        {
+            const float dp = evb[0] * ev[0] + evb[1] * ev[1] + evb[2] * ev[2];
+            for (int i = 0; i < 3; i++) vrb[i] = (evb[i] - dp * ev[i]) * vn;
+        }
+        kxb = m[1] * vrb[2] - m[2] * vrb[1];
+        kycb = m[2] * vrb[0] - m[0] * vrb[2];
+        kzb = m[0] * vrb[1] - m[1] * vrb[0];
+        mb[0] += vrb[1] * kc3[2] - vrb[2] * kc3[1];
+        mb[1] += vrb[2] * kc3[0] - vrb[0] * kc3[2];
+        mb[2] += vrb[0] * kc3[1] - vrb[1] * kc3[0];
+        // hc = hr * hn
         const float dp = hcb[0] * hc[0] + hcb[1] * hc[1] + hcb[2] * hc[2];
         for (int i = 0; i < 3; i++) hrb[i] = (hcb[i] - dp * hc[i]) * hn;
+        // m = (-kx kyc rs, s, -kz kyc rs)
+        kxb += mb[0] * (-kyrs);
+        kycb += mb[0] * (-kx * rs) + mb[2] * (-kz * rs);
+        kzb += mb[2] * (-kyrs);
+        sbm = mb[0] * (kx * kyrs * rs) + mb[2] * (kz * kyrs * rs) + mb[1];
     }
     float qb[3];
     qb[0] = hrb[1] * r.inc[2] - hrb[2] * r.inc[1];
@@ -323,25 +362,23 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     acc[A_INC + 2] += q[0] * hrb[1] - q[1] * hrb[0];
     if (bodge) {
         float abh, bbh;
-        dir4_back(r, dh, qb, B.hx, B.hy, B.hz, acc, abh, bbh);
+        dir4_back(r, dh, qb, hx, hy, hz, acc, accP, abh, bbh);
         const float ch = abh * iRf;
-        acc[A_CU + 0] = fmaf(ch, B.hx, acc[A_CU + 0]);
-        acc[A_CU + 1] = fmaf(ch, B.hy, acc[A_CU + 1]);
-        acc[A_CU + 2] = fmaf(ch, B.hz, acc[A_CU + 2]);
+        acc[A_CU + 0] = fmaf(ch, hx, acc[A_CU + 0]);
+        acc[A_CU + 1] = fmaf(ch, hy, acc[A_CU + 1]);
+        acc[A_CU + 2] = fmaf(ch, hz, acc[A_CU + 2]);
         acc[A_CE] += bbh;
     } else {
-        kcb[0] += qb[0];
-        kcb[1] += qb[1];
-        kcb[2] += qb[2];
+        kxb += qb[0];
+        kycb += qb[1];
+        kzb += qb[2];
     }
-    // Karczewski-Wolf: m = (-kx kyc rs, s, -kz kyc rs), dd, ee as above
-    float kxb = kcb[0], kycb = kcb[1], kzb = kcb[2];
-    kxb += mb[0] * (-kyc * rs) + eeb * (-0.5f * kyc * rs * rcf);
-    kycb += mb[0] * (-kx * rs) + mb[2] * (-kz * rs) + eeb * (-0.5f * kx * rs * rcf);
-    kzb += mb[2] * (-kyc * rs) + ddb * (-0.5f * rs * rcf);
+    // Karczewski-Wolf dd, ee as above
+    kxb += eeb * (-0.5f * kyrs * rcf);
+    kycb += eeb * (-0.5f * kx * rs * rcf);
+    kzb += ddb * (-0.5f * rs * rcf);
     const float rs2 = rs * rs;
-    const float sb = mb[0] * (kx * kyc * rs2) + mb[2] * (kz * kyc * rs2) + mb[1] +
-                     ddb * fmaf(-0.5f * Kz, cf, 0.5f * kz * rs2 * rcf) +
+    const float sb = sbm + ddb * fmaf(-0.5f * Kz, cf, 0.5f * kz * rs2 * rcf) +
                      eeb * fmaf(0.5f * Kx * Ky, cf, 0.5f * kx * kyc * rs2 * rcf);
     const float cfb = ddb * fmaf(-0.5f * Kz, s, 0.5f * kz * rs * rcf * rcf) +
                       eeb * fmaf(0.5f * Kx * Ky, s, 0.5f * kx * kyc * rs * rcf * rcf);
@@ -362,13 +399,13 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const int rk[3] = {(t[1] < t[0]) + (t[2] < t[0]), (t[0] <= t[1]) + (t[2] < t[1]),
                        (t[0] <= t[2]) + (t[1] <= t[2])};
     float kxxb = 0.0f, kyyb = 0.0f;
+    const float2 kk2 = make_float2(kxx, kyy);
 #pragma unroll
     for (int j = 0; j < 3; j++) {
         const float tb = rk[j] == 0 ? tlo : (rk[j] == 1 ? tmid : thi);
         kxxb = fmaf(tb, r.xa[j], kxxb);
         kyyb = fmaf(tb, r.ya[j], kyyb);
-        acc[A_TKX + j] = fmaf(tb, kxx, acc[A_TKX + j]);
-        acc[A_TKY + j] = fmaf(tb, kyy, acc[A_TKY + j]);
+        accP[P_TK + j] = fma2(bc2(tb), kk2, accP[P_TK + j]);
     }
     // kxx = k p2x - k kx ; kyy = k p2y - k ky
     kxb = fmaf(-k, kxxb, kxb);
@@ -377,7 +414,7 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     acc[A_P2 + 1] = fmaf(k, kyyb, acc[A_P2 + 1]);
     const float kb3[3] = {kxb, kyb, kzb};
     float ab, bb;
-    dir4_back(r, d, kb3, B.fx, B.fy, B.fz, acc, ab, bb);
+    dir4_back(r, d, kb3, B.fx, B.fy, B.fz, acc, accP, ab, bb);
     // ph = hkR (b - a^2)(1 + a) - rf with rf = k u.c (mod 2 pi), a = u.c/R, b = |c|^2/R^2:
     // c_bar = (ab + phb dph/da) u / R - phb k u + (bb + phb dph/db) 2 c / R^2
     const float dpa = hkR * fmaf(-2.0f * d.a, d.opa, fmaf(-d.a, d.a, r.b));
@@ -398,7 +435,7 @@ template <bool FAST, int MINB>
 __global__ void __launch_bounds__(K4_WARPS * 32, MINB) k4_adjoint_kernel(
     const K4Rec *__restrict__ recs, const int *__restrict__ kinds, const float *__restrict__ fovdat,
     int64_t nrec, const K4Bin *__restrict__ bins, const float4 *__restrict__ gbin, int64_t nb,
-    int64_t chunk, float k, float hkR, float iRf,
+    int64_t nphi, int64_t theta_i, int64_t chunk, float k, float hkR, float iRf,
     double *__restrict__ out) {
     __shared__ K4Rec s_rec[K4_WARPS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -412,7 +449,7 @@ __global__ void __launch_bounds__(K4_WARPS * 32, MINB) k4_adjoint_kernel(
     }
     const K4Rec &r = s_rec[warp];
     const int kd = kinds[rec];
-    const float4 *G = gbin + (int64_t)kd * 4 * nb;
+    const float4 *G = gbin + (int64_t)kd * 2 * nb;
     float cosfov = 0.0f, p0[3] = {0.0f, 0.0f, 0.0f};
     if (FAST) {
         p0[0] = fovdat[4 * rec];
@@ -421,41 +458,46 @@ __global__ void __launch_bounds__(K4_WARPS * 32, MINB) k4_adjoint_kernel(
         cosfov = fovdat[4 * rec + 3];
     }
     float acc[K4_NACC];
-    float2 accA[4];
+    float2 accA[4], accP[K4_NPAIR];
 #pragma unroll
     for (int q = 0; q < K4_NACC; q++) acc[q] = 0.0f;
+#pragma unroll
+    for (int q = 0; q < K4_NPAIR; q++) accP[q] = make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int q = 0; q < 4; q++) accA[q] = make_float2(0.0f, 0.0f);
     const int64_t o0 = (int64_t)blockIdx.y * chunk, o1 = min(nb, o0 + chunk);
     for (int64_t o = o0 + lane; o < o1; o += 32) {
         Bin4 B;
-        const float4 *pb = reinterpret_cast<const float4 *>(bins + o);
-        const float4 q0 = pb[0], q1 = pb[1], q2 = pb[2];
-        B.ux = __hiloint2double(__float_as_int(q0.y), __float_as_int(q0.x));
-        B.uy = __hiloint2double(__float_as_int(q0.w), __float_as_int(q0.z));
-        B.uz = __hiloint2double(__float_as_int(q1.y), __float_as_int(q1.x));
-        B.fx = q1.z;
-        B.fy = q1.w;
-        B.hx = q2.x;
-        B.hy = q2.y;
-        B.hz = q2.z;
-        B.fz = q2.w;
-        const float4 *pg = G + 4 * o;
-        const float4 g0 = pg[0], g1 = pg[1], g2 = pg[2], g3 = pg[3];
+        const double2 *pb = reinterpret_cast<const double2 *>(bins + o);
+        const double2 q0 = pb[0], q1 = pb[1];
+        B.ux = q0.x;
+        B.uy = q0.y;
+        B.uz = q1.x;
+        B.fx = (float)B.ux;
+        B.fy = (float)B.uy;
+        B.fz = (float)B.uz;
+        B.o = o;
+        const float4 *pg = G + 2 * o;
+        const float4 g0 = pg[0], g1 = pg[1];
         B.G[0] = make_float2(g0.x, g0.y);
         B.G[1] = make_float2(g0.z, g0.w);
         B.G[2] = make_float2(g1.x, g1.y);
         B.G[3] = make_float2(g1.z, g1.w);
-        B.Gm[0] = make_float2(g2.x, g2.y);
-        B.Gm[1] = make_float2(g2.z, g2.w);
-        B.Gm[2] = make_float2(g3.x, g3.y);
-        B.Gm[3] = make_float2(g3.z, g3.w);
-        k4_eval<FAST>(r, B, k, hkR, iRf, cosfov, p0, acc, accA);
+#pragma unroll
+        for (int c = 0; c < 4; c++) B.Gm[c] = make_float2(B.G[c].y, -B.G[c].x);
+        k4_eval<FAST>(r, B, k, hkR, iRf, cosfov, p0, bins, nphi, theta_i, acc, accA, accP);
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         acc[A_AMP + 2 * q] = accA[q].x;
         acc[A_AMP + 2 * q + 1] = accA[q].y;
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        acc[A_TKX + j] = accP[P_TK + j].x;
+        acc[A_TKY + j] = accP[P_TK + j].y;
+        acc[A_WU + 3 * j] += accP[P_WU01 + j].x;
+        acc[A_WU + 3 * j + 1] += accP[P_WU01 + j].y;
     }
 #pragma unroll
     for (int q = 0; q < K4_NACC; q++) {
@@ -466,14 +508,13 @@ __global__ void __launch_bounds__(K4_WARPS * 32, MINB) k4_adjoint_kernel(
     }
 }
 
-// Per-bin inputs of the adjoint: the unit bin direction (FP64), the unit
-// direction of the same-phi bin on the first row above 1 degree (used by the
-// forward-scattering rotation), and the cotangent of S' (pre-T, common phase
-// removed): G' = conj(e^{ik|X|}) G T^T, per kind.
+// Per-bin inputs of the adjoint: the unit bin direction (FP64) and the
+// cotangent of S' (pre-T, common phase removed): G' = conj(e^{ik|X|}) G T^T,
+// per kind.
 __global__ void k4_prep_kernel(const double *__restrict__ gafb, const double *__restrict__ gafe,
                                const double *__restrict__ xyz, const double *__restrict__ phitab,
-                               int64_t nb, int64_t nphi, int64_t theta_i, double k,
-                               K4Bin *__restrict__ bins, float4 *__restrict__ gbin) {
+                               int64_t nb, int64_t nphi, double k, K4Bin *__restrict__ bins,
+                               float4 *__restrict__ gbin) {
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= nb) return;
     const double cp = phitab[o % nphi], sp = phitab[nphi + o % nphi];
@@ -483,15 +524,7 @@ __global__ void k4_prep_kernel(const double *__restrict__ gafb, const double *__
     bn.ux = X * ir;
     bn.uy = Y * ir;
     bn.uz = Zc * ir;
-    bn.fx = (float)bn.ux;
-    bn.fy = (float)bn.uy;
-    bn.fz = (float)bn.uz;
-    const int64_t oh = (o % nphi) + nphi * theta_i;
-    const double Xh = xyz[oh], Yh = xyz[nb + oh], Zh = xyz[2 * nb + oh];
-    const double irh = 1.0 / sqrt(Xh * Xh + Yh * Yh + Zh * Zh);
-    bn.hx = (float)(Xh * irh);
-    bn.hy = (float)(Yh * irh);
-    bn.hz = (float)(Zh * irh);
+    bn.pad = 0.0;
     bins[o] = bn;
     double sK, cK;
     sincos(k * rho, &sK, &cK);
@@ -509,12 +542,9 @@ __global__ void k4_prep_kernel(const double *__restrict__ gafb, const double *__
         const double o21r = gr[1] * T11 + gr[3] * T12, o21i = gi[1] * T11 + gi[3] * T12;
         const double o12r = gr[0] * T21 + gr[2] * T22, o12i = gi[0] * T21 + gi[2] * T22;
         const double o22r = gr[1] * T21 + gr[3] * T22, o22i = gi[1] * T21 + gi[3] * T22;
-        // G and -i G = (Im, -Re)
-        float4 *dst = gbin + (kd * nb + o) * 4;
+        float4 *dst = gbin + (kd * nb + o) * 2;
         dst[0] = make_float4((float)o11r, (float)o11i, (float)o21r, (float)o21i);
         dst[1] = make_float4((float)o12r, (float)o12i, (float)o22r, (float)o22i);
-        dst[2] = make_float4((float)o11i, -(float)o11r, (float)o21i, -(float)o21r);
-        dst[3] = make_float4((float)o12i, -(float)o12r, (float)o22i, -(float)o22r);
     }
 }
 
@@ -613,7 +643,7 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
     const size_t o_rec = 0, o_kind = al(nrec * sizeof(K4Rec)), o_fov = al(o_kind + nrec * 4),
                  o_ga = al(o_fov + 16 * nrec), o_gb = al(o_ga + 8 * nb * 8),
                  o_bin = al(o_gb + 8 * nb * 8), o_gbin = al(o_bin + nb * sizeof(K4Bin)),
-                 o_out = al(o_gbin + 32 * nb * 4),
+                 o_out = al(o_gbin + 16 * nb * 4),
                  o_end = al(o_out + nrec * K4_NACC * 8);
     PBT_TRY(ctx->d_ws.ensure(o_end));
     char *base = ctx->d_ws.as<char>();
@@ -627,7 +657,7 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
     PBT_CUDA_TRY(cudaMemcpyAsync(base + o_gb, gafe, 8 * nb * 8, cudaMemcpyHostToDevice, st));
     k4_prep_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, st>>>(
         (const double *)(base + o_ga), (const double *)(base + o_gb), g.xyz.as<double>(),
-        g.phitab.as<double>(), nb, nphi, g.theta_i, k, (K4Bin *)(base + o_bin),
+        g.phitab.as<double>(), nb, nphi, k, (K4Bin *)(base + o_bin),
         (float4 *)(base + o_gbin));
     // bin ranges: at most K4_MAX_LANE_BINS terms per lane, and enough CTAs
     // for a few waves when there are few records
@@ -651,7 +681,8 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
         auto launch = [&](auto kern) {
             kern<<<grid, K4_WARPS * 32, 0, st>>>(
                 (const K4Rec *)(base + o_rec), (const int *)(base + o_kind), (const float *)(base + o_fov),
-                nrec, (const K4Bin *)(base + o_bin), (const float4 *)(base + o_gbin), nb, chunk, (float)k,
+                nrec, (const K4Bin *)(base + o_bin), (const float4 *)(base + o_gbin), nb, nphi,
+                g.theta_i, chunk, (float)k,
                 (float)(0.5 * k * Rf), (float)(1.0 / Rf), (double *)(base + o_out));
         };
         if (fast_diff) {
