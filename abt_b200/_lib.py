@@ -37,7 +37,9 @@ EXPORTS = ("pbt_ctx_create", "pbt_ctx_destroy", "pbt_last_error_string", "pbt_ve
            "pbt_diff_batch_dev_c", "pbt_last_launch_count", "pbt_set_kernel_timing",
            "pbt_kernel_time_ms", "pbt_diffraction_noalloc_c", "pbt_set_plan",
            "pbt_diff_adjoint_c", "pbt_diff_batch_dev_graph_c", "pbt_graph_launch_c",
-           "pbt_graph_kernel_count", "pbt_graph_destroy_c")
+           "pbt_graph_kernel_count", "pbt_graph_destroy_c", "pbt_beamlist_writer_open",
+           "pbt_beamlist_writer_add", "pbt_beamlist_writer_close", "pbt_beamlist_read",
+           "pbt_beamlist_info", "pbt_beamlist_arrays", "pbt_beamlist_free")
 
 
 class PbtError(RuntimeError):
@@ -78,6 +80,13 @@ def lib():
         "pbt_diff_batch_dev_graph_c": (C, [P, P, I64, P, P, P, P, P, I64, P, P, I64, P, I64, P,
                                            I64, D, I32, I32, P, P, P, P, P, P]),
         "pbt_graph_launch_c": (C, [P, P]),
+        "pbt_beamlist_writer_open": (C, [ctypes.c_char_p, P, I64, P, I64, I64, P, P, I64, D, P]),
+        "pbt_beamlist_writer_add": (C, [P, P, I64, P, I64, P, P]),
+        "pbt_beamlist_writer_close": (C, [P]),
+        "pbt_beamlist_read": (C, [ctypes.c_char_p, P]),
+        "pbt_beamlist_info": (C, [P, P, P]),
+        "pbt_beamlist_arrays": (C, [P] + [P] * 10),
+        "pbt_beamlist_free": (C, [P]),
         "pbt_graph_kernel_count": (I64, [P]),
         "pbt_graph_destroy_c": (C, [P]),
         "pbt_last_launch_count": (I64, [P]),

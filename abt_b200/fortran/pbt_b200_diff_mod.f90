@@ -86,7 +86,33 @@ module pbt_b200_diff_mod
             type(pbt_output_params), intent(inout) :: params
             real(c_double), intent(out) :: mueller(*), mueller_1d(*)
         end function
+        integer(c_int) function pbt_beamlist_writer_open(path, theta, ntheta, phi, nphi, nverts, &
+                                                         face_off, face_vi, nfaces, lambda, w) &
+                                                         bind(C, name="pbt_beamlist_writer_open")
+            import :: c_int, c_char, c_double, c_int64_t, c_ptr
+            character(kind=c_char), dimension(*), intent(in) :: path
+            real(c_double), intent(in) :: theta(*), phi(*)
+            integer(c_int64_t), value :: ntheta, nphi, nverts, nfaces
+            integer(c_int64_t), intent(in) :: face_off(*), face_vi(*)
+            real(c_double), value :: lambda
+            type(c_ptr), intent(out) :: w
+        end function
+        integer(c_int) function pbt_beamlist_writer_add(w, beam, nbeam, ext, next, verts, params_in) &
+                                                        bind(C, name="pbt_beamlist_writer_add")
+            import :: c_int, c_int64_t, c_double, c_ptr, pbt_outbeam, pbt_output_params
+            type(c_ptr), value :: w
+            type(pbt_outbeam), intent(in) :: beam(*), ext(*)
+            integer(c_int64_t), value :: nbeam, next
+            real(c_double), intent(in) :: verts(*)
+            type(pbt_output_params), intent(in) :: params_in
+        end function
+        integer(c_int) function pbt_beamlist_writer_close(w) bind(C, name="pbt_beamlist_writer_close")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: w
+        end function
     end interface
+
+    type(c_ptr), save :: pbt_dump = c_null_ptr
 
     contains
 
@@ -199,6 +225,49 @@ module pbt_b200_diff_mod
                        face_off, face_vi, int(geometry%nf, c_int64_t), theta_vals, &
                        int(size(theta_vals), c_int64_t), phi_vals, int(size(phi_vals), c_int64_t), &
                        lambda, fast, amplC), 'pbt_diffraction_c')
+    end subroutine
+
+    ! Beam-list dump: open once before the orientation loop, call
+    ! pbt_dump_orientation beside diff_main (src/pbt_seq_mod.f90:212) with the
+    ! same outbeam lists and the rotated geometry, close after the loop.  The
+    ! file replays through pbt_diff_batch_c (abt_b200.beamlist in Python).
+    subroutine pbt_dump_open(path, job_params, geometry)
+        character(len=*), intent(in) :: path
+        type(job_parameters_type), intent(in) :: job_params
+        type(geometry_type), intent(in) :: geometry
+        integer(c_int64_t), allocatable :: face_off(:), face_vi(:)
+        call pack_faces(geometry, face_off, face_vi)
+        call pbt_check(pbt_beamlist_writer_open(trim(path) // c_null_char, job_params%theta_vals, &
+                       int(size(job_params%theta_vals), c_int64_t), job_params%phi_vals, &
+                       int(size(job_params%phi_vals), c_int64_t), int(size(geometry%v, 1), c_int64_t), &
+                       face_off, face_vi, int(geometry%nf, c_int64_t), job_params%la, pbt_dump), &
+                       'pbt_beamlist_writer_open')
+    end subroutine
+
+    subroutine pbt_dump_orientation(beam_outbeam_tree, beam_outbeam_tree_counter, &
+                                    ext_diff_outbeam_tree, geometry, params_in)
+        type(outbeamtype), dimension(:), allocatable, intent(in) :: beam_outbeam_tree
+        integer(8), intent(in) :: beam_outbeam_tree_counter
+        type(outbeamtype), dimension(:), allocatable, intent(in) :: ext_diff_outbeam_tree
+        type(geometry_type), intent(in) :: geometry
+        type(pbt_output_params), intent(in) :: params_in   ! abs, geo_cross_sec, energies
+        type(pbt_outbeam), allocatable :: pb(:), pe(:)
+        integer(8) :: j, next
+        next = size(ext_diff_outbeam_tree, 1)
+        allocate(pb(max(1_8, beam_outbeam_tree_counter)), pe(max(1_8, next)))
+        do j = 1, beam_outbeam_tree_counter
+            call pack_outbeam(beam_outbeam_tree(j), pb(j))
+        end do
+        do j = 1, next
+            call pack_outbeam(ext_diff_outbeam_tree(j), pe(j))
+        end do
+        call pbt_check(pbt_beamlist_writer_add(pbt_dump, pb, int(beam_outbeam_tree_counter, c_int64_t), &
+                       pe, int(next, c_int64_t), geometry%v, params_in), 'pbt_beamlist_writer_add')
+    end subroutine
+
+    subroutine pbt_dump_close()
+        call pbt_check(pbt_beamlist_writer_close(pbt_dump), 'pbt_beamlist_writer_close')
+        pbt_dump = c_null_ptr
     end subroutine
 
 end module pbt_b200_diff_mod

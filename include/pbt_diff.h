@@ -253,6 +253,38 @@ int pbt_set_plan(pbt_ctx *ctx, int32_t variant, int32_t bins_per_thread, int64_t
  * Resets the record. */
 int pbt_kernel_time_ms(pbt_ctx *ctx, double *total_ms, int64_t *nlaunch);
 
+/* ---------------------------------------------------------------------------
+ * Beam-list files (no counterpart in the reference): the outbeam lists that
+ * the tracer hands to diff_main (src/pbt_seq_mod.f90:212), one orientation
+ * after another, saved for replay through pbt_diff_batch_c.  Host-only.
+ * Writer: open with the far-field grid and the particle topology, add one
+ * orientation per call (its outbeams, external-diffraction outbeams, rotated
+ * vertices v(nverts,3) and params_in record), close.  Reader: the whole file
+ * in host memory; pbt_beamlist_arrays gives pointers in pbt_diff_batch_c's
+ * layout (orientation-major outbeams with offsets, norient vertex blocks,
+ * norient params records), valid until pbt_beamlist_free.  A damaged,
+ * truncated or foreign file fails with PBT_EINVAL (magic, version, counts
+ * and a checksum are verified). */
+typedef struct pbt_beamlist_writer pbt_beamlist_writer;
+typedef struct pbt_beamlist pbt_beamlist;
+int pbt_beamlist_writer_open(const char *path, const double *theta, int64_t ntheta,
+                             const double *phi, int64_t nphi, int64_t nverts,
+                             const int64_t *face_off, const int64_t *face_vi, int64_t nfaces,
+                             double lambda, pbt_beamlist_writer **out);
+int pbt_beamlist_writer_add(pbt_beamlist_writer *w, const pbt_outbeam *beam, int64_t nbeam,
+                            const pbt_outbeam *ext, int64_t next, const double *verts,
+                            const pbt_output_params *params_in);
+int pbt_beamlist_writer_close(pbt_beamlist_writer *w);
+int pbt_beamlist_read(const char *path, pbt_beamlist **out);
+/* counts: norient, nverts, nfaces, nface_vi, ntheta, nphi, nbeam_total, next_total */
+int pbt_beamlist_info(const pbt_beamlist *bl, int64_t counts[8], double *lambda);
+int pbt_beamlist_arrays(const pbt_beamlist *bl, const double **theta, const double **phi,
+                        const int64_t **face_off, const int64_t **face_vi, const double **verts,
+                        const int64_t **beam_off, const pbt_outbeam **beam,
+                        const int64_t **ext_off, const pbt_outbeam **ext,
+                        const pbt_output_params **params_in);
+int pbt_beamlist_free(pbt_beamlist *bl);
+
 #ifdef __cplusplus
 }
 #endif
