@@ -117,6 +117,7 @@ int grid_prepare(pbt_ctx *ctx, const double *theta, int64_t ntheta, const double
         !memcmp(g.phi.data(), phi, nphi * sizeof(double)))
         return PBT_OK;
     g.valid = false;
+    g.fast_tile = 0;
     g.theta.assign(theta, theta + ntheta);
     g.phi.assign(phi, phi + nphi);
     int64_t nb = ntheta * nphi;

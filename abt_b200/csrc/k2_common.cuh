@@ -26,11 +26,28 @@ struct __align__(16) K2Rec {
 };
 static_assert(sizeof(K2Rec) == 176, "K2Rec must be 176 bytes");
 
-// Per-record field-of-view test data (is_fast_diff only): prop0 and cos(fov).
+// Per-record field-of-view test data (is_fast_diff only): prop0 and cos(fov)
+// for the per-bin test; fovm = fov + a parallax margin with its cosine and
+// sine for the per-tile cull (a tile whose cone lies beyond fovm is skipped).
+// When the FP32 per-bin test is within tol of the threshold the FP64 test of
+// the reference (facet centre com, prop0, cos(fov)) decides, with the same
+// rounding as the FP64 drop-in.
 struct __align__(16) K2Fov {
     float p0[3];
     float cos_fov;
+    float cos_fovm, sin_fovm, fovm, tol;
+    double com[3], p0d[3], cos_fovd, pad;
 };
+static_assert(sizeof(K2Fov) == 96, "K2Fov must be 96 bytes");
+
+// Cone of a bin tile (is_fast_diff only): unit centre direction and the
+// largest angle psi of a tile bin from it.
+struct __align__(16) K2Cone {
+    float c[3];
+    float psi;
+    float cos_psi, sin_psi, pad[2];
+};
+static_assert(sizeof(K2Cone) == 32, "K2Cone must be 32 bytes");
 
 }  // namespace pbt
 

@@ -57,7 +57,23 @@ struct BinDev {
     double ux, uy, uz;  // unit bin direction, FP64
     float fx, fy, fz;   // same, FP32
     float hx, hy, hz;   // direction of the (phi_i, theta_i) bin used by the forward bodge
+    int64_t bin;        // bin index
 };
+
+// The field-of-view test of the FP64 drop-in for bin `bin` (src/diff_mod.f90:593-603):
+// x1 = X - com, dot(x1/r1, prop0) >= cos(fov), each operation rounded once.
+__device__ __forceinline__ bool fov_exact(const K2Fov &f, const double *__restrict__ xyz, int64_t nb,
+                                       int64_t bin) {
+    const double x1 = __dadd_rn(xyz[bin], -f.com[0]);
+    const double y1 = __dadd_rn(xyz[nb + bin], -f.com[1]);
+    const double z1 = __dadd_rn(xyz[2 * nb + bin], -f.com[2]);
+    const double r1 =
+        __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x1, x1), __dmul_rn(y1, y1)), __dmul_rn(z1, z1)));
+    const double v0 = __ddiv_rn(x1, r1), v1 = __ddiv_rn(y1, r1), v2 = __ddiv_rn(z1, r1);
+    const double d = __dadd_rn(__dadd_rn(__dmul_rn(v0, f.p0d[0]), __dmul_rn(v1, f.p0d[1])),
+                               __dmul_rn(v2, f.p0d[2]));
+    return !(d < f.cos_fovd);
+}
 
 // ---------------------------------------------------------------- set-up
 
@@ -226,6 +242,24 @@ __global__ void k2_setup_kernel(RefSrc S, int64_t nrefs, const double *__restric
             fv.p0[1] = (float)prop0[1];
             fv.p0[2] = (float)prop0[2];
             fv.cos_fov = (float)cos(fov);
+            // the per-bin test uses the direction from the facet centre: it is
+            // within |c|/R of the direction from the origin; 2|c|/R + 1e-5 rad
+            // also covers the FP32 rounding of both tests
+            const double cn = sqrt(fr.com[0] * fr.com[0] + fr.com[1] * fr.com[1] +
+                                   fr.com[2] * fr.com[2]);
+            const double fovm = fov + 2.0 * cn / kFarR + 1e-5;
+            fv.fovm = (float)fovm;
+            fv.cos_fovm = (float)cos(fovm);
+            fv.sin_fovm = (float)sin(fovm);
+            // FP32 test error: second-order parallax (< 3 |c/R|^2) and rounding (< 8e-7)
+            const double e2 = (cn / kFarR) * (cn / kFarR);
+            fv.tol = (float)(3.0 * e2 + 8e-7);
+            for (int c = 0; c < 3; c++) {
+                fv.com[c] = fr.com[c];
+                fv.p0d[c] = prop0[c];
+            }
+            fv.cos_fovd = cos(fov);
+            fv.pad = 0.0;
             fovs[r0 + t] = fv;
         }
     }
@@ -367,7 +401,7 @@ struct K2MainArgs {
 template <int BPT, bool FAST>
 __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const BinDev (&bd)[BPT],
                                           const bool (&valid)[BPT], float (&acc)[BPT][8], float k,
-                                          float hkR) {
+                                          float hkR, const double *__restrict__ xyz, int64_t nb) {
     const double kc0 = r.kc[0], kc1 = r.kc[1], kc2 = r.kc[2];
 #pragma unroll
     for (int q = 0; q < BPT; q++) {
@@ -397,7 +431,9 @@ __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const
             const float dy = fmaf(B.fy, opa, -r.eps[1]);
             const float dz = fmaf(B.fz, opa, -r.eps[2]);
             const float dp = fmaf(dz, fv->p0[2], fmaf(dy, fv->p0[1], dx * fv->p0[0]));
-            use = use && !(dp < fv->cos_fov);
+            bool in = !(dp < fv->cos_fov);
+            if (use && fabsf(dp - fv->cos_fov) < fv->tol) in = fov_exact(*fv, xyz, nb, B.bin);
+            use = use && in;
         }
         // aperture integral
         const float kxx = fmaf(-k, kx, r.kp[0]);
@@ -514,6 +550,7 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
             const int64_t o = valid[q] ? bin[q] : 0;
             const double X = P.xyz[o], Y = P.xyz[P.nb + o], Zc = P.xyz[2 * P.nb + o];
             const double ir = 1.0 / sqrt(X * X + Y * Y + Zc * Zc);
+            bd[q].bin = o;
             bd[q].ux = X * ir;
             bd[q].uy = Y * ir;
             bd[q].uz = Zc * ir;
@@ -560,7 +597,7 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
             const K2Fov *fv = FAST ? P.fovs + rbeg + c * K2_CH : nullptr;
             for (int j = 0; j < n; j++)
                 k2_record<BPT, FAST>(sbuf[st][j], FAST ? fv + j : nullptr, bd, valid, acc, P.k,
-                                     P.hkR);
+                                     P.hkR, P.xyz, P.nb);
 #pragma unroll
             for (int q = 0; q < BPT; q++)
 #pragma unroll
@@ -608,6 +645,7 @@ struct BinPk {
     double ux, uy, uz;     // unit bin direction, FP64
     float2 fx, fy, fz;     // same, broadcast FP32 pairs
     float2 hx, hy, hz;     // forward-bodge bin direction, broadcast pairs
+    int64_t bin;           // bin index
 };
 
 // sin(h)/h (h >= 0) with one shared reciprocal: rh = 1/max(h, 0.5)
@@ -685,7 +723,7 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
 template <bool FAST>
 __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const BinPk &B,
                                         float2 (&acc)[8], float2 nk, float2 hkR, bool lo_ok,
-                                        bool hi_ok) {
+                                        bool hi_ok, const double *__restrict__ xyz, int64_t nb) {
     // far-field phase per facet: FP64 k u.c, reduced mod 2 pi
     float2 rf;
     {
@@ -715,8 +753,11 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
         const K2Fov &fa = fv[0], &fb = fv[1];
         const float dpx = fmaf(dz.x, fa.p0[2], fmaf(dy.x, fa.p0[1], dx.x * fa.p0[0]));
         const float dpy = fmaf(dz.y, fb.p0[2], fmaf(dy.y, fb.p0[1], dx.y * fb.p0[0]));
-        ok_x = ok_x && !(dpx < fa.cos_fov);
-        ok_y = ok_y && !(dpy < fb.cos_fov);
+        bool in_x = !(dpx < fa.cos_fov), in_y = !(dpy < fb.cos_fov);
+        if (ok_x && fabsf(dpx - fa.cos_fov) < fa.tol) in_x = fov_exact(fa, xyz, nb, B.bin);
+        if (ok_y && fabsf(dpy - fb.cos_fov) < fb.tol) in_y = fov_exact(fb, xyz, nb, B.bin);
+        ok_x = ok_x && in_x;
+        ok_y = ok_y && in_y;
     }
     // aperture integral
     const float2 kxx = fma2(nk, kx, P.kp[0]);
@@ -810,9 +851,20 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
 
 constexpr int K2P_CH = 32;  // record pairs per shared-memory stage (64 records)
 
+// The record's per-bin test passes no bin of the tile when the angle between
+// prop0 and the tile centre exceeds fovm + psi (fovm includes the parallax
+// and rounding margin); compared through cosines with a further 1e-6 margin.
+__device__ __forceinline__ bool cone_culled(const K2Fov &f, const K2Cone &t) {
+    if (!(f.fovm + t.psi < 3.14159f)) return false;
+    const float d = fmaf(f.p0[2], t.c[2], fmaf(f.p0[1], t.c[1], f.p0[0] * t.c[0]));
+    return d < fmaf(f.cos_fovm, t.cos_psi, -f.sin_fovm * t.sin_psi) - 1e-6f;
+}
+
 struct K2PkArgs {
     const K2Pair *pairs;
     const K2Fov *fovs;
+    const int *perm;        // is_fast_diff: tile-major bin order (-1: padding)
+    const K2Cone *cones;    // is_fast_diff: cone of each tile
     const int64_t *seg_rec;
     const int64_t *item_pre;
     int64_t nseg;
@@ -829,10 +881,11 @@ struct K2PkArgs {
 };
 
 template <int BPT, bool FAST>
-__global__ void __launch_bounds__(K2_THREADS) k2_main_pk_kernel(K2PkArgs P) {
+__global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 1) k2_main_pk_kernel(K2PkArgs P) {
     __shared__ __align__(128) K2Pair sbuf[K2_NST][K2P_CH];
     __shared__ __align__(8) uint64_t bars[K2_NST];
     __shared__ long long s_item;
+    __shared__ unsigned s_keep[2];  // is_fast_diff: records of the stage not culled for the tile
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int s = 0; s < K2_NST; s++) mbar_init(smem_u32(&bars[s]), 1);
@@ -866,11 +919,13 @@ __global__ void __launch_bounds__(K2_THREADS) k2_main_pk_kernel(K2PkArgs P) {
         int64_t bin[BPT];
 #pragma unroll
         for (int q = 0; q < BPT; q++) {
-            bin[q] = tile * TILE + q * K2_THREADS + tid;
-            valid[q] = bin[q] < P.nb;
+            const int64_t li = tile * TILE + q * K2_THREADS + tid;
+            bin[q] = FAST ? (int64_t)P.perm[li] : li;
+            valid[q] = FAST ? bin[q] >= 0 : bin[q] < P.nb;
             const int64_t o = valid[q] ? bin[q] : 0;
             const double X = P.xyz[o], Y = P.xyz[P.nb + o], Zc = P.xyz[2 * P.nb + o];
             const double ir = 1.0 / sqrt(X * X + Y * Y + Zc * Zc);
+            bd[q].bin = o;
             bd[q].ux = X * ir;
             bd[q].uy = Y * ir;
             bd[q].uz = Zc * ir;
@@ -889,6 +944,8 @@ __global__ void __launch_bounds__(K2_THREADS) k2_main_pk_kernel(K2PkArgs P) {
         for (int q = 0; q < BPT; q++)
 #pragma unroll
             for (int c = 0; c < 8; c++) acc64[q][c] = 0.0;
+        K2Cone cone;
+        if (FAST) cone = P.cones[tile];
         // record pairs [p0, p1) cover records [rbeg, rend)
         const int64_t p0 = rbeg >> 1, p1 = (rend + 1) >> 1;
         const int64_t npair = p1 - p0;
@@ -919,13 +976,31 @@ __global__ void __launch_bounds__(K2_THREADS) k2_main_pk_kernel(K2PkArgs P) {
             // only the item's first pair (odd rbeg) and last pair (odd rend) are partial
             const int j_lo = (c == 0 && (rbeg & 1)) ? 0 : -1;
             const int j_hi = (c == nchunk - 1 && (rend & 1)) ? n - 1 : -1;
+            if (FAST) {
+                // the tile cull of the stage's 2n records, one per thread of
+                // warps 0 and 1: a record whose field of view misses the whole
+                // tile adds nothing
+                if (tid < 64) {
+                    const bool keep =
+                        tid < 2 * n && !cone_culled(P.fovs[2 * (p0 + c * K2P_CH) + tid], cone);
+                    const unsigned m = __ballot_sync(0xffffffffu, keep);
+                    if ((tid & 31) == 0) s_keep[tid >> 5] = m;
+                }
+                __syncthreads();
+            }
             for (int j = 0; j < n; j++) {
-                const bool lo_ok = j != j_lo, hi_ok = j != j_hi;
+                bool lo_ok = j != j_lo, hi_ok = j != j_hi;
                 const K2Fov *fv = FAST ? P.fovs + 2 * (p0 + c * K2P_CH + j) : nullptr;
+                if (FAST) {
+                    const unsigned m = s_keep[j >> 4] >> (2 * (j & 15));
+                    lo_ok = lo_ok && (m & 1u);
+                    hi_ok = hi_ok && (m & 2u);
+                    if (!lo_ok && !hi_ok) continue;  // uniform over the CTA
+                }
 #pragma unroll
                 for (int q = 0; q < BPT; q++)
                     k2_pair<FAST>(sbuf[st][j], fv, bd[q], acc[q], nk, hkR, lo_ok && valid[q],
-                                  hi_ok && valid[q]);
+                                  hi_ok && valid[q], P.xyz, P.nb);
             }
 #pragma unroll
             for (int q = 0; q < BPT; q++)
@@ -1336,12 +1411,98 @@ int k2_launch_pk(pbt_ctx *ctx, cudaStream_t st, const K2PkArgs &A) {
     return PBT_OK;
 }
 
+// One warp per tile: unit centre of the tile's bin directions and the
+// largest angle of a bin from it (FP64).
+__global__ void k2_cone_kernel(const int *__restrict__ perm, int64_t ntiles, int64_t tile,
+                               const double *__restrict__ xyz, int64_t nb, K2Cone *__restrict__ cones) {
+    const int64_t t = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= ntiles) return;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int64_t i = lane; i < tile; i += 32) {
+        const int o = perm[t * tile + i];
+        if (o < 0) continue;
+        const double X = xyz[o], Y = xyz[nb + o], Z = xyz[2 * nb + o];
+        const double ir = 1.0 / sqrt(X * X + Y * Y + Z * Z);
+        sx += X * ir;
+        sy += Y * ir;
+        sz += Z * ir;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, off);
+        sy += __shfl_xor_sync(0xffffffffu, sy, off);
+        sz += __shfl_xor_sync(0xffffffffu, sz, off);
+    }
+    const double sn = sqrt(sx * sx + sy * sy + sz * sz);
+    // a tile whose directions cancel gets psi > pi: never culled
+    const bool ok = sn > 1e-9;
+    const double cx = ok ? sx / sn : 0.0, cy = ok ? sy / sn : 0.0, cz = ok ? sz / sn : 1.0;
+    double dmin = 1.0;
+    for (int64_t i = lane; i < tile; i += 32) {
+        const int o = perm[t * tile + i];
+        if (o < 0) continue;
+        const double X = xyz[o], Y = xyz[nb + o], Z = xyz[2 * nb + o];
+        const double ir = 1.0 / sqrt(X * X + Y * Y + Z * Z);
+        dmin = fmin(dmin, (X * cx + Y * cy + Z * cz) * ir);
+    }
+    for (int off = 16; off > 0; off >>= 1) dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, off));
+    if (lane == 0) {
+        const double psi = ok ? acos(fmax(-1.0, fmin(1.0, dmin))) + 1e-6 : 4.0;
+        K2Cone c;
+        c.c[0] = (float)cx;
+        c.c[1] = (float)cy;
+        c.c[2] = (float)cz;
+        c.psi = (float)psi;
+        c.cos_psi = (float)cos(psi);
+        c.sin_psi = (float)sin(psi);
+        c.pad[0] = c.pad[1] = 0.0f;
+        cones[t] = c;
+    }
+}
+
+// is_fast_diff tiles of `tile` bins: blocks of (tile/16) theta x 16 phi bins,
+// so that a tile spans a small solid angle; cached with the bin grid.
+int k2_fast_tiles(pbt_ctx *ctx, cudaStream_t st, int64_t tile) {
+    GridCache &g = ctx->grid;
+    if (g.fast_tile == tile) return PBT_OK;
+    const int64_t nphi = (int64_t)g.phi.size(), ntheta = (int64_t)g.theta.size();
+    const int64_t bp = 16, bt = tile / bp;
+    const int64_t ntb = (ntheta + bt - 1) / bt, npb = (nphi + bp - 1) / bp;
+    const int64_t ntiles = ntb * npb;
+    std::vector<int> perm((size_t)(ntiles * tile), -1);
+    for (int64_t a = 0; a < ntb; a++)
+        for (int64_t b = 0; b < npb; b++) {
+            const int64_t t = a * npb + b;
+            int64_t i = 0;
+            for (int64_t j = a * bt; j < std::min(ntheta, (a + 1) * bt); j++)
+                for (int64_t q = b * bp; q < std::min(nphi, (b + 1) * bp); q++)
+                    perm[(size_t)(t * tile + i++)] = (int)(q + nphi * j);
+        }
+    PBT_TRY(g.fast_perm.ensure(perm.size() * sizeof(int)));
+    PBT_TRY(g.fast_cone.ensure((size_t)ntiles * sizeof(K2Cone)));
+    PBT_CUDA_TRY(cudaMemcpyAsync(g.fast_perm.p, perm.data(), perm.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, st));
+    k2_cone_kernel<<<(unsigned)((ntiles + 3) / 4), 128, 0, st>>>(
+        g.fast_perm.as<int>(), ntiles, tile, g.xyz.as<double>(), g.nb, g.fast_cone.as<K2Cone>());
+    ctx->launches++;
+    PBT_CUDA_TRY(cudaGetLastError());
+    PBT_CUDA_TRY(cudaStreamSynchronize(st));  // perm (pageable) and cones ready before caching
+    g.fast_tile = tile;
+    g.fast_ntiles = ntiles;
+    return PBT_OK;
+}
+
 int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, int64_t no,
                  double lambda, int fast_diff, const K2Plan &plan, float *ws, int64_t *seg_rec,
                  int64_t *item_pre, unsigned long long *counter) {
     const GridCache &g = ctx->grid;
     const int64_t tile = (int64_t)K2_THREADS * plan.bpt;
-    const int64_t ntiles = (g.nb + tile - 1) / tile;
+    int64_t ntiles = (g.nb + tile - 1) / tile;
+    const bool cull = fast_diff && plan.variant == 1;
+    if (cull) {
+        PBT_TRY(k2_fast_tiles(ctx, st, tile));
+        ntiles = g.fast_ntiles;
+    }
     k2_plan_kernel<<<1, 32, 0, st>>>(S.start, S.refbase, S.beam_off, o0, no, plan.rpi, ntiles,
                                      seg_rec, item_pre, counter);
     ctx->launches++;
@@ -1368,6 +1529,8 @@ int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, in
         K2PkArgs B;
         B.pairs = S.pairs;
         B.fovs = S.fovs;
+        B.perm = cull ? g.fast_perm.as<int>() : nullptr;
+        B.cones = cull ? g.fast_cone.as<K2Cone>() : nullptr;
         B.seg_rec = seg_rec;
         B.item_pre = item_pre;
         B.nseg = A.nseg;

@@ -86,6 +86,10 @@ struct GridCache {
     DevBuf thtab;                    // sin(theta) | cos(theta) (ntheta each), libm values
     DevBuf wbin;                     // simpne weights w_phi(i) * w_theta(j) * sin(theta_j)  (nb)
     DevBuf wphi;                     // simpne weights over phi (nphi)
+    // is_fast_diff bin tiles: (theta x phi) blocks of fast_tile bins
+    int64_t fast_tile = 0, fast_ntiles = 0;
+    DevBuf fast_perm;                // tile-major bin indices (int32, -1 = padding)
+    DevBuf fast_cone;                // K2Cone per tile
     bool valid = false;
 };
 

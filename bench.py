@@ -65,6 +65,8 @@ def parse():
                     help="orientations of the rough-column orientation average (0: skip)")
     ap.add_argument("--orient-fp64", type=int, default=16,
                     help="orientations timed with the FP64 drop-in and used for the error")
+    ap.add_argument("--fast-diff", type=int, default=1,
+                    help="1: also time the workload with is_fast_diff (field-of-view tile cull)")
     ap.add_argument("--adjoint-facets", type=int, default=20000,
                     help="facet sample for the adjoint / forward kernel-time ratio (0: skip)")
     return ap.parse_args()
@@ -402,6 +404,29 @@ def main():
 
     if args.orient > 0 and rank == 0:
         extra["orientation_average"] = orientation_average(ctx, args)
+
+    # -fast_diff: the same workload with the field-of-view test (fov = 8 lambda / d);
+    # error against the FP64 drop-in with is_fast_diff on the first 20,000 facets
+    if args.fast_diff and rank == 0:
+        ctx.diff_main(beam[:64], None, geo, th, ph, LAM, is_fast_diff=True, precision="fp32")
+        ctx.set_kernel_timing(True)
+        ctx.kernel_time_ms()
+        flush.zero_()
+        ctx.diff_main(beam, None, geo, th, ph, LAM, is_fast_diff=True, precision="fp32")
+        kf_ms, _ = ctx.kernel_time_ms()
+        ctx.set_kernel_timing(False)
+        sub = beam[:20000]
+        from tests.helpers import mueller_rel_err
+        a32 = ctx.diff_main(sub, None, geo, th, ph, LAM, is_fast_diff=True, precision="fp32")
+        a64 = ctx.diff_main(sub, None, geo, th, ph, LAM, is_fast_diff=True, precision="fp64")
+        m32, _, _ = ctx.finalise(a32[0], a32[1], th, ph, LAM, pin[0])
+        m64, _, _ = ctx.finalise(a64[0], a64[1], th, ph, LAM, pin[0])
+        extra["fast_diff"] = {"kernel_ms": kf_ms, "value": work / (kf_ms / 1e3), "unit": UNIT,
+                              "speedup_vs_full_kernel": (kern_ms / max(kern_n, 1)) / kf_ms,
+                              "max_rel_mueller_err_vs_fp64_fast_20000_facets":
+                                  mueller_rel_err(m32, m64, 1e-6),
+                              "cull": "records whose field of view misses a 8x16 (theta x phi) "
+                                      "bin tile are skipped for that tile"}
 
     # FP32 error against the FP64 drop-in on the full workload
     if not args.no_error_check:

@@ -86,3 +86,24 @@ def test_batch_fp32_vs_fp64(ctx, scaling):
         assert abs(f[2][n] - r[2][n]) <= TOL_PARAM * abs(r[2][n]), n
         np.testing.assert_allclose(f[3][n], r[3][n], rtol=TOL_PARAM, err_msg=n)
     np.testing.assert_allclose(f[3]["back_scatt"], r[3]["back_scatt"], rtol=1e-4)
+
+
+@pytest.mark.gpu
+def test_fp32_fast_diff_tile_cull(ctx):
+    """is_fast_diff on beam lists with small fields of view: the FP32 kernel
+    skips whole (theta x phi) tiles outside a facet's cone; the result must
+    still match the FP64 drop-in, which tests every bin."""
+    geo, beam, _ = W.synthetic_beam_list(n_beams=30, facets_per_beam=40, seed=7)
+    # narrow and wide cones, and external diffraction (a hemisphere each)
+    beam["fov"] *= np.repeat(np.linspace(0.1, 2.0, 30), 40)
+    ext = beam[::40].copy()
+    ext["prop_out"] = (0.0, 0.0, -1.0)
+    th, ph = abt_b200.make_angles([0, 180], [1]), abt_b200.make_angles([0, 358], [2])
+    a32 = ctx.diff_main(beam, ext, geo, th, ph, LAM, is_fast_diff=True, precision="fp32")
+    a64 = ctx.diff_main(beam, ext, geo, th, ph, LAM, is_fast_diff=True, precision="fp64")
+    assert mueller_rel_err(_mueller(*a32), _mueller(*a64)) <= TOL_MU
+    # the cull must not change the per-bin masking: compare against no culling
+    ctx.set_plan(0, 1, 2048)   # the one-record kernel has no tile cull
+    a32n = ctx.diff_main(beam, ext, geo, th, ph, LAM, is_fast_diff=True, precision="fp32")
+    ctx.set_plan(-1)
+    assert mueller_rel_err(_mueller(*a32), _mueller(*a32n)) <= 1e-5
