@@ -881,7 +881,7 @@ struct K2PkArgs {
 };
 
 template <int BPT, bool FAST>
-__global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 1) k2_main_pk_kernel(K2PkArgs P) {
+__global__ void __launch_bounds__(K2_THREADS, (BPT == 1 && FAST) ? 4 : 0) k2_main_pk_kernel(K2PkArgs P) {
     __shared__ __align__(128) K2Pair sbuf[K2_NST][K2P_CH];
     __shared__ __align__(8) uint64_t bars[K2_NST];
     __shared__ long long s_item;

@@ -67,6 +67,8 @@ def parse():
                     help="orientations timed with the FP64 drop-in and used for the error")
     ap.add_argument("--fast-diff", type=int, default=1,
                     help="1: also time the workload with is_fast_diff (field-of-view tile cull)")
+    ap.add_argument("--diff-orient", type=int, default=64,
+                    help="orientations of the differentiation workload (0: skip)")
     ap.add_argument("--adjoint-facets", type=int, default=20000,
                     help="facet sample for the adjoint / forward kernel-time ratio (0: skip)")
     return ap.parse_args()
@@ -195,6 +197,90 @@ def orientation_average(ctx, args):
             "max_rel_mueller_err_vs_fp64": mueller_rel_err(f32[0], f64[0], 1e-6),
             "max_rel_param_err_vs_fp64": perr,
             "api": "pbt_diff_batch_c (host pointers), wall clock"}
+
+
+def differentiation(ctx, args):
+    """Gradients of the Mueller loss for a Gaussian-rough hexagonal plate
+    (r 8 um, L 4 um, sigma 0.05 um, 20,808 triangles; stand-in beam lists),
+    --diff-orient orientations, 181 theta x 90 phi: the target is the FP32
+    forward of the geometry with N(0, 0.02^2) um vertex noise; each orientation
+    runs the FP32 forward and the adjoint through torch.autograd.  On the first
+    orientation the gradient is checked against FP64 central differences
+    (h = 1e-5 um) of the loss of the FP64 drop-in."""
+    import torch
+
+    import abt_b200
+    from abt_b200 import autograd as AG
+    from abt_b200 import workloads as W
+    geo = W.hex_prism(8.0, 4.0, n_side=34, n_len=17, roughness=0.05, seed=4)
+    th = abt_b200.make_angles([0, 180], [1])
+    ph = abt_b200.make_angles([0, 356], [4])
+    rng = np.random.default_rng(4)
+    eul = W.uniform_euler(rng, args.diff_orient)
+    noise = rng.normal(0.0, 0.02, size=geo["verts"].shape)
+    fwd_ms = adj_ms = wall = 0.0
+    nrec = []
+    fd = None
+    for i, (a, b, c) in enumerate(eul):
+        R = W.euler_rotation(a, b, c)
+        V, beam, ext, _ = W.standin_orientation(geo, R, rng, n_internal=(0, 2))
+        nrec.append(len(beam) + len(ext))
+        tb, te = ctx.diff_main(beam, ext, dict(geo, verts=(geo["verts"] + noise) @ R.T), th, ph,
+                               LAM, precision="fp32")
+        t11, t12 = AG.mueller11_12(torch.from_numpy(tb), torch.from_numpy(te), LAM)
+        g = dict(geo, verts=V)
+        Vg = torch.tensor(V, requires_grad=True)
+        ab = torch.tensor(beam["ampl"], requires_grad=True)
+        ae = torch.tensor(ext["ampl"], requires_grad=True)
+        ctx.set_kernel_timing(True)
+        ctx.kernel_time_ms()
+        t0 = time.perf_counter()
+        afb, afe = AG.far_field(ctx, Vg, ab, ae, beam, ext, g, th, ph, LAM)
+        f_ms, _ = ctx.kernel_time_ms()
+        m11, m12 = AG.mueller11_12(afb, afe, LAM)
+        AG.mueller_loss(m11, m12, t11, t12, th).backward()
+        wall += time.perf_counter() - t0
+        a_ms, _ = ctx.kernel_time_ms()
+        ctx.set_kernel_timing(False)
+        if i > 0:  # the first orientation warms up
+            fwd_ms += f_ms
+            adj_ms += a_ms
+        if i == 0:
+            def loss64(Vm, bm=beam, em=ext):
+                x, y = ctx.diff_main(bm, em, dict(geo, verts=Vm), th, ph, LAM, precision="fp64")
+                p, q = AG.mueller11_12(torch.from_numpy(x), torch.from_numpy(y), LAM)
+                return float(AG.mueller_loss(p, q, t11, t12, th))
+            gV = Vg.grad.numpy()
+            used = np.unique(geo["face_vi"].reshape(-1, 3)[beam["fi"][:2000] - 1]) - 1
+            picks = [(int(v), k) for v in rng.choice(used, 4, replace=False) for k in range(3)]
+            h = 1e-5
+            errs = []
+            for v, k in picks:
+                Vp, Vm = V.copy(), V.copy()
+                Vp[v, k] += h
+                Vm[v, k] -= h
+                errs.append(abs((loss64(Vp) - loss64(Vm)) / (2 * h) - gV[v, k]))
+            gb = ab.grad.numpy()
+            aerr = []
+            for j in (0, len(beam) // 2):
+                bp, bm = beam.copy(), beam.copy()
+                bp["ampl"][j, 2] += 1e-6
+                bm["ampl"][j, 2] -= 1e-6
+                aerr.append(abs((loss64(V, bp) - loss64(V, bm)) / 2e-6 - gb[j, 2]))
+            fd = {"h_um": h, "vertex_coords": len(picks),
+                  "max_abs_err_over_max_grad_vertex": float(max(errs) / np.abs(gV).max()),
+                  "ampl_components": len(aerr),
+                  "max_abs_err_over_max_grad_ampl": float(max(aerr) / np.abs(gb).max())}
+    n = max(1, args.diff_orient - 1)
+    return {"workload": "rough hexagonal plate r 8 um, L 4 um, sigma 0.05 um (20,808 triangles), "
+                        "stand-in beam lists, %d orientations, 181 theta x 90 phi, target from "
+                        "0.02 um vertex noise" % args.diff_orient,
+            "records_per_orientation": [int(min(nrec)), int(np.mean(nrec)), int(max(nrec))],
+            "forward_kernel_ms_per_orientation": fwd_ms / n,
+            "adjoint_kernel_ms_per_orientation": adj_ms / n,
+            "adjoint_over_forward": adj_ms / fwd_ms if fwd_ms > 0 else None,
+            "gradient_wall_ms_per_orientation": wall * 1e3 / args.diff_orient,
+            "fd_check_first_orientation": fd}
 
 
 def cpu_baseline(geo, beam, th, ph, seconds, nthreads):
@@ -404,6 +490,9 @@ def main():
 
     if args.orient > 0 and rank == 0:
         extra["orientation_average"] = orientation_average(ctx, args)
+
+    if args.diff_orient > 0 and rank == 0:
+        extra["differentiation"] = differentiation(ctx, args)
 
     # -fast_diff: the same workload with the field-of-view test (fov = 8 lambda / d);
     # error against the FP64 drop-in with is_fast_diff on the first 20,000 facets
