@@ -67,6 +67,8 @@ def parse():
                     help="orientations timed with the FP64 drop-in and used for the error")
     ap.add_argument("--fast-diff", type=int, default=1,
                     help="1: also time the workload with is_fast_diff (field-of-view tile cull)")
+    ap.add_argument("--large-orient", type=int, default=2,
+                    help="orientations of the large absorbing column timed (0: skip)")
     ap.add_argument("--diff-orient", type=int, default=64,
                     help="orientations of the differentiation workload (0: skip)")
     ap.add_argument("--adjoint-facets", type=int, default=20000,
@@ -197,6 +199,71 @@ def orientation_average(ctx, args):
             "max_rel_mueller_err_vs_fp64": mueller_rel_err(f32[0], f64[0], 1e-6),
             "max_rel_param_err_vs_fp64": perr,
             "api": "pbt_diff_batch_c (host pointers), wall clock"}
+
+
+def large_case(ctx, args):
+    """The large-column workload: smooth hexagonal column r 50 um, L 100 um
+    triangulated to 2 um^2 facets (22,500 triangles), stand-in beam lists of
+    10-30 outgoing beams per facet (~460,000 outbeams per orientation), 1441
+    theta x 720 phi (1,037,520 bins).  --large-orient orientations are averaged
+    by one FP32 batch; the FP64 drop-in rate is sampled on 4,000 facets and
+    the error taken on a 10 % facet sample of the first orientation."""
+    import abt_b200
+    from abt_b200 import workloads as W
+    from tests.helpers import mueller_rel_err
+    geo = W.hex_prism(50.0, 100.0, n_side=25, n_len=50, roughness=0.0, seed=5)
+    th = abt_b200.make_angles([0, 180], [0.125])
+    ph = abt_b200.make_angles([0, 359.5], [0.5])
+    nb = len(th) * len(ph)
+    rng = np.random.default_rng(5)
+    eul = W.uniform_euler(rng, args.large_orient)
+    Vs, beams, exts = [], [], []
+    pin = np.zeros(args.large_orient, dtype=abt_b200.PARAMS_DTYPE)
+    for i, (a, b, c) in enumerate(eul):
+        V, beam, ext, gcs = W.standin_orientation(geo, W.euler_rotation(a, b, c), rng,
+                                                  n_internal=(10, 30))
+        Vs.append(V)
+        beams.append(beam)
+        exts.append(ext)
+        pin[i] = abt_b200.params(geo_cross_sec=gcs)
+    F = np.array([len(b) + len(e) for b, e in zip(beams, exts)])
+    ctx.diff_batch(beams[:1], [exts[0][:64]], Vs[:1], geo, th, ph, LAM, pin[:1], precision="fp32")
+    ctx.set_kernel_timing(True)
+    ctx.kernel_time_ms()
+    t0 = time.perf_counter()
+    ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp32")
+    t32 = time.perf_counter() - t0
+    k_ms, k_n = ctx.kernel_time_ms()
+    # FP64 drop-in rate on 4,000 facets over the full grid
+    sub = beams[0][:4000]
+    ctx.kernel_time_ms()
+    ctx.diff_main(sub, None, dict(geo, verts=Vs[0]), th, ph, LAM, precision="fp64")
+    k64_ms, _ = ctx.kernel_time_ms()
+    ctx.set_kernel_timing(False)
+    r64 = len(sub) * nb / (k64_ms / 1e3)
+    # error on a 10 % sample of the first orientation's outbeams
+    sb = beams[0][::10]
+    se = exts[0][::10]
+    g0 = dict(geo, verts=Vs[0])
+    a32 = ctx.diff_main(sb, se, g0, th, ph, LAM, precision="fp32")
+    a64 = ctx.diff_main(sb, se, g0, th, ph, LAM, precision="fp64")
+    m32, _, p32 = ctx.finalise(a32[0], a32[1], th, ph, LAM, pin[0])
+    m64, _, p64 = ctx.finalise(a64[0], a64[1], th, ph, LAM, pin[0])
+    work = float(F.sum()) * nb
+    return {"workload": "smooth hexagonal column r 50 um, L 100 um, 2 um^2 triangles (22,500), "
+                        "stand-in beam lists (10-30 outgoing beams per facet), %d orientations, "
+                        "1441 theta x 720 phi" % args.large_orient,
+            "outbeams_per_orientation": [int(F.min()), int(F.mean()), int(F.max())], "bins": nb,
+            "fp32_batched_s": t32, "fp32_orientations_per_s": args.large_orient / t32,
+            "fp32_facet_bin_per_s": work / t32, "fp32_kernel_ms": k_ms,
+            "fp32_kernel_facet_bin_per_s": work / (k_ms / 1e3),
+            "fp64_dropin_facet_bin_per_s": r64,
+            "fp64_dropin_orientations_per_s_extrapolated": r64 / (float(F.mean()) * nb),
+            "speedup_fp32_batched_vs_fp64_dropin": (work / t32) / r64,
+            "max_rel_mueller_err_vs_fp64_10pct_sample": mueller_rel_err(m32, m64, 1e-6),
+            "max_rel_param_err_vs_fp64_10pct_sample": max(
+                abs(float(p32[n]) - float(p64[n])) / abs(float(p64[n]))
+                for n in ("scatt", "ext", "asymmetry"))}
 
 
 def differentiation(ctx, args):
@@ -493,6 +560,8 @@ def main():
 
     if args.diff_orient > 0 and rank == 0:
         extra["differentiation"] = differentiation(ctx, args)
+    if args.large_orient > 0 and rank == 0:
+        extra["large_column"] = large_case(ctx, args)
 
     # -fast_diff: the same workload with the field-of-view test (fov = 8 lambda / d);
     # error against the FP64 drop-in with is_fast_diff on the first 20,000 facets
