@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch plan instead of tuning it on a 20,000-facet sample")
     ap.add_argument("--no-graph", action="store_true",
                     help="enqueue each step through the C ABI instead of replaying a CUDA graph")
     ap.add_argument("--orient", type=int, default=1024,
@@ -442,6 +444,14 @@ def main():
         diff_batch_dev(ctx, stream.cuda_stream, 1, d_beam, boff, d_ext, eoff, d_verts, nverts,
                        geo["face_off"], d_fvi, th, ph, LAM, d_pin, d_mu, d_m1, d_pav, d_pper)
 
+    # launch plan (variant x bins per thread x records per item) tuned on a sample
+    plan = {"plan": "default (1, 1, 2048)"}
+    if not args.no_tune:
+        from abt_b200.tune import tune
+        best, times = tune(ctx, beam, geo, th, ph, LAM, sample_facets=20000)
+        plan = {"plan": list(best), "candidates_kernel_ms_20000_facets":
+                {"%d,%d,%d" % k: round(v, 3) for k, v in times.items()}}
+
     # the step: one replay of the batch captured as a CUDA graph (the capture
     # runs the batch once); --no-graph enqueues it through the C ABI instead
     graph = None
@@ -640,7 +650,8 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "256 MB buffer written before every step, inside the timed region",
                        "step": "CUDA graph replay of pbt_diff_batch_dev_c" if not args.no_graph
-                               else "pbt_diff_batch_dev_c"},
+                               else "pbt_diff_batch_dev_c",
+                       "launch_plan": plan},
             "orientations_per_s": world * 1e3 / ms_step,
             "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof,
             "cpu_baseline": cpu}
