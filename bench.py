@@ -128,6 +128,21 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
+def max_over_ranks(dist, ms, device):
+    """The slowest rank's time (all ranks take part; dist None: one process)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(world, work_per_rank, ms_step):
+    """Whole-job throughput of `world` replicas: all ranks' units over the slowest time."""
+    return world * work_per_rank / (ms_step / 1e3)
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -498,12 +513,9 @@ def main():
     ms_total = e0.elapsed_time(e1)
     if graph is not None:
         graph.close()
-    if dist is not None:
-        t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(dist, ms_total, dev)
     ms_step = ms_total / args.steps
-    value = world * work / (ms_step / 1e3)
+    value = replicas_value(world, work, ms_step)
 
     extra = {}
     # end to end through the host C ABI with pinned host buffers
