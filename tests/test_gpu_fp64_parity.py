@@ -153,3 +153,20 @@ def test_batch_fp64_matches_oracle_loop(ctx):
     got = np.array([pav[n] for n in abt_b200.PARAM_NAMES])
     sel = [i for i, n in enumerate(abt_b200.PARAM_NAMES) if n not in ("beam_energy_out", "ext_energy_out")]
     np.testing.assert_allclose(got[sel], rp[sel], rtol=TOL_AMPL)
+
+
+def test_diffraction_concurrent_callers(ctx):
+    """The -memory path calls diffraction from OpenMP threads
+    (src/beam_loop_mod.f90:1935-1967): concurrent callers on one context get
+    the same grids as serial calls."""
+    from concurrent.futures import ThreadPoolExecutor
+    rng = np.random.default_rng(12)
+    th, ph = grids()[0]
+    geo = mixed_polygon_geometry(rng)
+    obs = outbeams(16, rng, len(geo["face_off"]) - 1)
+    serial = [ctx.diffraction(obs[i:i + 1], geo, th, ph, LAM) for i in range(len(obs))]
+    with ThreadPoolExecutor(max_workers=8) as ex:
+        conc = list(ex.map(lambda i: ctx.diffraction(obs[i:i + 1], geo, th, ph, LAM),
+                           range(len(obs))))
+    for a, b in zip(serial, conc):
+        assert np.array_equal(a, b)
