@@ -12,7 +12,8 @@ There is no CPU fallback: importing the compute entry points requires the
 built library (python abt_b200/build.py).
 """
 from ._lib import OUTBEAM_DTYPE, PARAMS_DTYPE, PARAM_NAMES, PbtError  # noqa: F401
-from .diff import Context, PI_REF, make_angles, make_geometry, params, params_dict  # noqa: F401
+from .diff import (Context, PI_REF, make_angles, make_far_field_bins, make_geometry, params,  # noqa: F401
+                   params_dict)
 
 __all__ = ["Context", "OUTBEAM_DTYPE", "PARAMS_DTYPE", "PARAM_NAMES", "PbtError", "PI_REF",
-           "make_angles", "make_geometry", "params", "params_dict"]
+           "make_angles", "make_far_field_bins", "make_geometry", "params", "params_dict"]

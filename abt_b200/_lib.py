@@ -39,7 +39,8 @@ EXPORTS = ("pbt_ctx_create", "pbt_ctx_destroy", "pbt_last_error_string", "pbt_ve
            "pbt_diff_adjoint_c", "pbt_diff_batch_dev_graph_c", "pbt_graph_launch_c",
            "pbt_graph_kernel_count", "pbt_graph_destroy_c", "pbt_beamlist_writer_open",
            "pbt_beamlist_writer_add", "pbt_beamlist_writer_close", "pbt_beamlist_read",
-           "pbt_beamlist_info", "pbt_beamlist_arrays", "pbt_beamlist_free")
+           "pbt_beamlist_info", "pbt_beamlist_arrays", "pbt_beamlist_free",
+           "pbt_make_far_field_bins_c")
 
 
 class PbtError(RuntimeError):
@@ -87,6 +88,7 @@ def lib():
         "pbt_beamlist_info": (C, [P, P, P]),
         "pbt_beamlist_arrays": (C, [P] + [P] * 10),
         "pbt_beamlist_free": (C, [P]),
+        "pbt_make_far_field_bins_c": (C, [P, I64, P, I64, P, P, P]),
         "pbt_graph_kernel_count": (I64, [P]),
         "pbt_graph_destroy_c": (C, [P]),
         "pbt_last_launch_count": (I64, [P]),

@@ -109,6 +109,20 @@ static void simpne_weights(const double *x, int64_t ntab, double *w) {
     panel(ntab - 3, x1, x2, x3, x3 * x3 - x2 * x2, x3 * x3 * x3 - x2 * x2 * x2, x3 - x2);
 }
 
+// make_far_field_bins (src/diff_mod.f90:827-855) in meshgrid order, phi fastest
+// (:846-853): X = R (sin t cos p, sin t sin p, -cos t), R = 1e6, libm values.
+void far_field_bins(const double *theta, int64_t ntheta, const double *phi, int64_t nphi,
+                    double *x, double *y, double *z) {
+    const double r = kFarR;
+    for (int64_t j = 0; j < ntheta; j++)
+        for (int64_t i = 0; i < nphi; i++) {
+            const int64_t o = i + nphi * j;
+            x[o] = r * sin(theta[j]) * cos(phi[i]);
+            y[o] = r * sin(theta[j]) * sin(phi[i]);
+            z[o] = -(r * cos(theta[j]));
+        }
+}
+
 int grid_prepare(pbt_ctx *ctx, const double *theta, int64_t ntheta, const double *phi,
                  int64_t nphi, cudaStream_t st) {
     GridCache &g = ctx->grid;
@@ -137,16 +151,8 @@ int grid_prepare(pbt_ctx *ctx, const double *theta, int64_t ntheta, const double
             g.back_i = i;
         }
     }
-    // make_far_field_bins with meshgrid order (phi fastest), src/diff_mod.f90:846-853
     std::vector<double> xyz(3 * nb), pt(2 * nphi), tt(2 * ntheta), wb(nb), wph(nphi), wth(ntheta);
-    const double r = kFarR;
-    for (int64_t j = 0; j < ntheta; j++)
-        for (int64_t i = 0; i < nphi; i++) {
-            int64_t o = i + nphi * j;
-            xyz[o] = r * sin(theta[j]) * cos(phi[i]);
-            xyz[nb + o] = r * sin(theta[j]) * sin(phi[i]);
-            xyz[2 * nb + o] = -(r * cos(theta[j]));
-        }
+    far_field_bins(theta, ntheta, phi, nphi, xyz.data(), xyz.data() + nb, xyz.data() + 2 * nb);
     for (int64_t i = 0; i < nphi; i++) {
         pt[i] = cos(phi[i]);
         pt[nphi + i] = sin(phi[i]);
@@ -279,3 +285,14 @@ int k1_build_facets(const pbt_outbeam *obs, int64_t n, double fov_override, cons
 }
 
 }  // namespace pbt
+
+extern "C" int pbt_make_far_field_bins_c(const double *theta, int64_t ntheta, const double *phi,
+                                         int64_t nphi, double *xfar, double *yfar, double *zfar) {
+    pbt::clear_error();
+    if (!theta || !phi || !xfar || !yfar || !zfar || ntheta < 1 || nphi < 1) {
+        pbt::set_error("make_far_field_bins: NULL array or empty angle list");
+        return PBT_EINVAL;
+    }
+    pbt::far_field_bins(theta, ntheta, phi, nphi, xfar, yfar, zfar);
+    return PBT_OK;
+}

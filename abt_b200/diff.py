@@ -51,6 +51,17 @@ def make_angles(vals_deg, splits_deg):
     return a * PI_REF / 180.0
 
 
+def make_far_field_bins(theta, phi):
+    """make_far_field_bins (src/diff_mod.f90:827-855) -> (xfar, yfar, zfar),
+    each (nphi, ntheta) in Fortran order (pbt_make_far_field_bins_c)."""
+    theta = np.ascontiguousarray(theta, dtype=np.float64)
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    out = [np.zeros((len(phi), len(theta)), order="F") for _ in range(3)]
+    check(_lib.lib().pbt_make_far_field_bins_c(ptr(theta), len(theta), ptr(phi), len(phi),
+                                               *[o.ctypes.data for o in out]))
+    return tuple(out)
+
+
 def make_geometry(verts, faces):
     """Geometry dict from (nverts,3) vertices and a list of 1-based vertex index lists."""
     verts = np.asarray(verts, dtype=np.float64)

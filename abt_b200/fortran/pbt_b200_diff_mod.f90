@@ -106,6 +106,13 @@ module pbt_b200_diff_mod
             real(c_double), intent(in) :: verts(*)
             type(pbt_output_params), intent(in) :: params_in
         end function
+        integer(c_int) function pbt_make_far_field_bins_c(theta, ntheta, phi, nphi, x, y, z) &
+                                                          bind(C, name="pbt_make_far_field_bins_c")
+            import :: c_int, c_int64_t, c_double
+            real(c_double), intent(in) :: theta(*), phi(*)
+            integer(c_int64_t), value :: ntheta, nphi
+            real(c_double), intent(out) :: x(*), y(*), z(*)
+        end function
         integer(c_int) function pbt_beamlist_writer_close(w) bind(C, name="pbt_beamlist_writer_close")
             import :: c_int, c_ptr
             type(c_ptr), value :: w
@@ -225,6 +232,19 @@ module pbt_b200_diff_mod
                        face_off, face_vi, int(geometry%nf, c_int64_t), theta_vals, &
                        int(size(theta_vals), c_int64_t), phi_vals, int(size(phi_vals), c_int64_t), &
                        lambda, fast, amplC), 'pbt_diffraction_c')
+    end subroutine
+
+    ! same argument list as make_far_field_bins, src/diff_mod.f90:827-836
+    subroutine make_far_field_bins(x, y, z, theta_vals, phi_vals)
+        real(8), dimension(:,:), allocatable, intent(out) :: x, y, z
+        real(8), dimension(:), allocatable, intent(in) :: theta_vals
+        real(8), dimension(:), allocatable, intent(in) :: phi_vals
+        integer(8) :: nphi, ntheta
+        nphi = size(phi_vals, 1)
+        ntheta = size(theta_vals, 1)
+        allocate(x(nphi, ntheta), y(nphi, ntheta), z(nphi, ntheta))
+        call pbt_check(pbt_make_far_field_bins_c(theta_vals, int(ntheta, c_int64_t), phi_vals, &
+                       int(nphi, c_int64_t), x, y, z), 'pbt_make_far_field_bins_c')
     end subroutine
 
     ! Beam-list dump: open once before the orientation loop, call

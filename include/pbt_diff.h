@@ -98,6 +98,13 @@ int pbt_diffraction_c(pbt_ctx *ctx, const pbt_outbeam *outbeam, const double *ve
                       int64_t nfaces, const double *theta, int64_t ntheta, const double *phi,
                       int64_t nphi, double lambda, int32_t is_fast_diff, double *amplC);
 
+/* make_far_field_bins, src/diff_mod.f90:827-855: the far-field points
+ * X = R (sin t cos p, sin t sin p, -cos t), R = 1e6, for every (phi, theta),
+ * written as xfar/yfar/zfar(nphi, ntheta) column-major (phi fastest), with the
+ * platform libm as the reference computes them.  Host only. */
+int pbt_make_far_field_bins_c(const double *theta, int64_t ntheta, const double *phi,
+                              int64_t nphi, double *xfar, double *yfar, double *zfar);
+
 /* pbt_diffraction_c for callers that cannot let a library allocate memory.
  * No counterpart in the reference.  Programs whose device memory is reserved
  * up front by their own pool allocator, or that may allocate nothing after

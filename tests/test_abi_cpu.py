@@ -99,3 +99,19 @@ def test_hex_prism_is_closed_and_outward():
     # outward: normals point away from the centre
     c = geo["verts"][geo["face_vi"] - 1].reshape(-1, 3, 3).mean(1)
     assert ((n * c).sum(1) > 0).all()
+
+
+def test_make_far_field_bins_matches_oracle():
+    """make_far_field_bins through the C ABI (host only) equals the oracle's
+    restatement bit for bit (both use the platform libm)."""
+    import abt_b200
+    from oracle import oracle as O
+    th = abt_b200.make_angles([0, 2, 10, 180], [0.5, 2, 10])
+    ph = abt_b200.make_angles([0, 350], [10])
+    x, y, z = abt_b200.make_far_field_bins(th, ph)
+    ref = O.far_field_bins(th, ph)
+    assert x.shape == (len(ph), len(th))
+    for a, r in zip((x, y, z), ref):
+        assert np.array_equal(a.ravel(order="F"), r)
+    with pytest.raises(abt_b200.PbtError):
+        abt_b200.make_far_field_bins(th[:0], ph)
