@@ -674,3 +674,15 @@ extern "C" int pbt_diff_adjoint_c(pbt_ctx *ctx, const pbt_outbeam *beam, int64_t
                       lambda, is_fast_diff ? 1 : 0, grad_ampl_far_beam, grad_ampl_far_ext_diff,
                       grad_verts, grad_beam_ampl, grad_ext_ampl);
 }
+
+// Failure-detection self-test: a device wait that nothing completes must end
+// by itself within limit_ms and come back as PBT_ETIMEOUT with the context
+// still usable.
+extern "C" int pbt_selftest_bounded_wait_c(pbt_ctx *ctx, int32_t limit_ms) {
+    API_ENTER(ctx);
+    if (limit_ms < 1 || limit_ms > 5000) {
+        set_error("self-test limit must be 1..5000 ms");
+        return PBT_EINVAL;
+    }
+    return k2_wait_selftest(ctx, st, (uint64_t)limit_ms * 1000000ull);
+}

@@ -364,10 +364,13 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_
         "l"(src), "r"(bytes), "r"(bar)
         : "memory");
 }
-// Bounded wait on an mbarrier phase: false after ~2 s.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Bounded wait on an mbarrier phase: false after limit_ns of global time or
+// 2^26 polls, whichever comes first.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
+                                          uint64_t limit_ns = kWaitLimitNs) {
     uint64_t t0 = 0;
-    for (uint32_t it = 0;; ++it) {
+    for (uint32_t it = 0; it < (1u << 26); ++it) {
         uint32_t ok;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -376,8 +379,9 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
             : "memory");
         if (ok) return true;
         if (it == 0) t0 = gtimer();
-        else if ((it & 255) == 0 && gtimer() - t0 > 2000000000ull) return false;
+        else if ((it & 255) == 0 && gtimer() - t0 > limit_ns) return false;
     }
+    return false;
 }
 
 struct K2MainArgs {
@@ -580,12 +584,14 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
             }
         }
         bool timed_out = false;
+        int64_t c_out = 0;
         for (int64_t c = 0; c < nchunk; c++) {
             const int st = (int)(c % K2_NST);
             const bool ok = mbar_wait(smem_u32(&bars[st]), parity[st]);
             parity[st] ^= 1u;
             if (__syncthreads_or(!ok)) {
                 timed_out = true;
+                c_out = c;
                 break;
             }
             const int n = (int)min((int64_t)K2_CH, nrec - c * K2_CH);
@@ -612,7 +618,14 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
             }
         }
         if (timed_out) {
-            if (tid == 0) atomicOr(P.err, 4);
+            if (tid == 0) {
+                atomicOr(P.err, 4);
+                // bounded wait for this CTA's bulk copies still in flight
+                for (int64_t c2 = c_out; c2 < min(nchunk, c_out + K2_NST); c2++) {
+                    const int s2 = (int)(c2 % K2_NST);
+                    mbar_wait(smem_u32(&bars[s2]), c2 == c_out ? parity[s2] ^ 1u : parity[s2]);
+                }
+            }
             return;
         }
         float *out = P.ws + seg * 8 * P.nb;
@@ -959,12 +972,14 @@ __global__ void __launch_bounds__(K2_THREADS, (BPT == 1 && FAST) ? 4 : 0) k2_mai
             }
         }
         bool timed_out = false;
+        int64_t c_out = 0;
         for (int64_t c = 0; c < nchunk; c++) {
             const int st = (int)(c % K2_NST);
             const bool ok = mbar_wait(smem_u32(&bars[st]), (parity >> st) & 1u);
             parity ^= 1u << st;
             if (__syncthreads_or(!ok)) {
                 timed_out = true;
+                c_out = c;
                 break;
             }
             const int n = (int)min((int64_t)K2P_CH, npair - c * K2P_CH);
@@ -1017,7 +1032,15 @@ __global__ void __launch_bounds__(K2_THREADS, (BPT == 1 && FAST) ? 4 : 0) k2_mai
             }
         }
         if (timed_out) {
-            if (tid == 0) atomicOr(P.err, 4);
+            if (tid == 0) {
+                atomicOr(P.err, 4);
+                // bounded wait for this CTA's bulk copies still in flight
+                for (int64_t c2 = c_out; c2 < min(nchunk, c_out + K2_NST); c2++) {
+                    const int s2 = (int)(c2 % K2_NST);
+                    const uint32_t ph = (parity >> s2) & 1u;
+                    mbar_wait(smem_u32(&bars[s2]), c2 == c_out ? ph ^ 1u : ph);
+                }
+            }
             return;
         }
         float *out = P.ws + seg * 8 * P.nb;
@@ -1561,6 +1584,31 @@ int64_t max_face_nv(const int64_t *h_face_off, int64_t nfaces) {
 }
 
 }  // namespace
+
+namespace {
+// One CTA waits on an mbarrier that nothing arrives at: the bounded wait must
+// give up after limit_ns and raise the timeout flag.
+__global__ void k2_wait_selftest_kernel(uint64_t limit_ns, int *__restrict__ err) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&bar), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const bool ok = mbar_wait(smem_u32(&bar), 0u, limit_ns);
+    if (threadIdx.x == 0 && !ok) atomicOr(err, 4);
+}
+}  // namespace
+
+int k2_wait_selftest(pbt_ctx *ctx, cudaStream_t st, uint64_t limit_ns) {
+    PBT_TRY(ctx->d_misc.ensure(64));
+    int *d_err = ctx->d_misc.as<int>();
+    PBT_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    k2_wait_selftest_kernel<<<1, 32, 0, st>>>(limit_ns, d_err);
+    ctx->launches = 1;
+    PBT_CUDA_TRY(cudaGetLastError());
+    return k2_check_err(ctx, st, d_err);
+}
 
 int k2_check_err(pbt_ctx *ctx, cudaStream_t st, const int *d_err) {
     int h = 0;

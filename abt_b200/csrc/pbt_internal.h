@@ -178,6 +178,8 @@ int k2_diff_main_impl(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *d_beam, 
                       const int64_t *d_face_vi, int64_t nfaces, double lambda, int fast_diff,
                       double *d_afb, double *d_afe);
 int k2_check_err(pbt_ctx *ctx, cudaStream_t st, const int *d_err);
+// Launches a bounded wait that nothing completes (the failure-detection self-test).
+int k2_wait_selftest(pbt_ctx *ctx, cudaStream_t st, uint64_t limit_ns);
 int totals_divide_device(pbt_ctx *ctx, DevTotals &T, cudaStream_t st, int64_t num_orients,
                          double *d_mu, double *d_m1, double *d_p);
 int validate_outbeams(const pbt_outbeam *obs, int64_t n, int64_t nfaces, const char *what);

@@ -135,6 +135,11 @@ class Context:
         check(_lib.lib().pbt_set_plan(self._h, int(variant), int(bins_per_thread),
                                       int(records_per_item)))
 
+    def selftest_bounded_wait(self, limit_ms=200):
+        """pbt_selftest_bounded_wait_c: a device wait that nothing completes must
+        give up by itself; raises PbtError(PBT_ETIMEOUT) as designed."""
+        check(_lib.lib().pbt_selftest_bounded_wait_c(self._h, int(limit_ms)))
+
     def kernel_time_ms(self):
         """(total ms, launches) of the far-field kernels timed since the last call."""
         t = ctypes.c_double()

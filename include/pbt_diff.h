@@ -292,6 +292,12 @@ int pbt_beamlist_arrays(const pbt_beamlist *bl, const double **theta, const doub
                         const pbt_output_params **params_in);
 int pbt_beamlist_free(pbt_beamlist *bl);
 
+/* Failure-detection self-test (no counterpart in the reference): launches a
+ * device wait on an mbarrier that nothing completes, bounded like every wait of
+ * the far-field kernels; it gives up after limit_ms (1..5000) and the call
+ * returns PBT_ETIMEOUT, leaving the context usable. */
+int pbt_selftest_bounded_wait_c(pbt_ctx *ctx, int32_t limit_ms);
+
 #ifdef __cplusplus
 }
 #endif

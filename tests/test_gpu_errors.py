@@ -77,3 +77,52 @@ def test_context_survives_errors(ctx):
     th, ph, geo, ob = _inputs()
     afb, afe = ctx.diff_main(ob, None, geo, th, ph, LAM)
     assert np.isfinite(afb).all() and np.abs(afb).max() > 0
+
+
+def test_bounded_wait_times_out_and_context_survives(ctx):
+    """Failure detection without a GPU fault: a device wait that nothing
+    completes ends by itself within its limit and is reported as
+    PBT_ETIMEOUT; the next compute call on the same context succeeds."""
+    import time
+    t0 = time.perf_counter()
+    with pytest.raises(abt_b200.PbtError) as e:
+        ctx.selftest_bounded_wait(200)
+    assert e.value.status == abt_b200._lib.PBT_ETIMEOUT
+    assert time.perf_counter() - t0 < 5.0
+    rng = np.random.default_rng(3)
+    geo = one_triangle()
+    th, ph = abt_b200.make_angles([0, 180], [10]), abt_b200.make_angles([0, 350], [10])
+    afb, _ = ctx.diff_main(outbeams(2, rng, 1), None, geo, th, ph, 0.532, precision="fp32")
+    assert np.isfinite(afb).all() and np.abs(afb).max() > 0
+
+
+def test_fp32_face_vertex_limit(ctx):
+    """The FP32 path fans faces of up to 16 vertices; a 20-gon is refused with
+    PBT_EINVAL there, while the FP64 drop-in takes it."""
+    n = 20
+    a = np.arange(n) * 2 * np.pi / n
+    verts = np.stack([np.cos(a), np.sin(a), np.zeros(n)], 1) + np.array([3.0, -2.0, 1.0])
+    geo = abt_b200.make_geometry(verts, [list(range(1, n + 1))])
+    rng = np.random.default_rng(4)
+    ob = outbeams(1, rng, 1)
+    th, ph = abt_b200.make_angles([0, 180], [10]), abt_b200.make_angles([0, 350], [10])
+    a64, _ = ctx.diff_main(ob, None, geo, th, ph, 0.532, precision="fp64")
+    assert np.isfinite(a64).all()
+    with pytest.raises(PbtError) as e:
+        ctx.diff_main(ob, None, geo, th, ph, 0.532, precision="fp32")
+    assert e.value.status == PBT_EINVAL
+
+
+def test_ragged_batch_with_empty_orientations(ctx):
+    """Orientations with no outbeams at all, or no external diffraction, in a
+    batch: FP32 matches the FP64 drop-in."""
+    from abt_b200 import workloads as W
+    from tests.helpers import mueller_rel_err
+    geo, Vs, beams, exts, pin = W.rough_column_orientations(4, seed=41, n_side=2, n_len=3,
+                                                            m_range=(0, 2))
+    beams[1] = beams[1][:0]
+    exts[2] = exts[2][:0]
+    th, ph = abt_b200.make_angles([0, 180], [4]), abt_b200.make_angles([0, 356], [4])
+    r32 = ctx.diff_batch(beams, exts, Vs, geo, th, ph, 0.532, pin, precision="fp32")
+    r64 = ctx.diff_batch(beams, exts, Vs, geo, th, ph, 0.532, pin, precision="fp64")
+    assert mueller_rel_err(r32[0], r64[0]) <= 1e-4
