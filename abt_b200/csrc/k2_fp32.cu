@@ -1003,19 +1003,26 @@ __global__ void __launch_bounds__(K2_THREADS, (BPT == 1 && FAST) ? 4 : 0) k2_mai
                 }
                 __syncthreads();
             }
-            for (int j = 0; j < n; j++) {
+            auto pair_step = [&](int j) {
                 bool lo_ok = j != j_lo, hi_ok = j != j_hi;
                 const K2Fov *fv = FAST ? P.fovs + 2 * (p0 + c * K2P_CH + j) : nullptr;
                 if (FAST) {
                     const unsigned m = s_keep[j >> 4] >> (2 * (j & 15));
                     lo_ok = lo_ok && (m & 1u);
                     hi_ok = hi_ok && (m & 2u);
-                    if (!lo_ok && !hi_ok) continue;  // uniform over the CTA
+                    if (!lo_ok && !hi_ok) return;  // uniform over the CTA
                 }
 #pragma unroll
                 for (int q = 0; q < BPT; q++)
                     k2_pair<FAST>(sbuf[st][j], fv, bd[q], acc[q], nk, hkR, lo_ok && valid[q],
                                   hi_ok && valid[q], P.xyz, P.nb);
+            };
+            if (FAST) {
+                // two pairs per iteration: with most pairs culled, the loop overhead shows
+#pragma unroll 2
+                for (int j = 0; j < n; j++) pair_step(j);
+            } else {
+                for (int j = 0; j < n; j++) pair_step(j);
             }
 #pragma unroll
             for (int q = 0; q < BPT; q++)
