@@ -40,7 +40,7 @@ EXPORTS = ("pbt_ctx_create", "pbt_ctx_destroy", "pbt_last_error_string", "pbt_ve
            "pbt_graph_kernel_count", "pbt_graph_destroy_c", "pbt_beamlist_writer_open",
            "pbt_beamlist_writer_add", "pbt_beamlist_writer_close", "pbt_beamlist_read",
            "pbt_beamlist_info", "pbt_beamlist_arrays", "pbt_beamlist_free",
-           "pbt_make_far_field_bins_c", "pbt_selftest_bounded_wait_c")
+           "pbt_make_far_field_bins_c", "pbt_selftest_bounded_wait_c", "pbt_diff_batch_list_c")
 
 
 class PbtError(RuntimeError):
@@ -90,6 +90,8 @@ def lib():
         "pbt_beamlist_free": (C, [P]),
         "pbt_make_far_field_bins_c": (C, [P, I64, P, I64, P, P, P]),
         "pbt_selftest_bounded_wait_c": (C, [P, I32]),
+        "pbt_diff_batch_list_c": (C, [P, I64, P, P, P, P, P, I64, P, P, I64, P, I64, P, I64, D,
+                                      I32, I32, I32, P, P, P, P, P]),
         "pbt_graph_kernel_count": (I64, [P]),
         "pbt_graph_destroy_c": (C, [P]),
         "pbt_last_launch_count": (I64, [P]),

@@ -136,8 +136,9 @@ int upload_geometry(pbt_ctx *ctx, cudaStream_t st, const double *verts, int64_t 
     char *b = ctx->d_in.as<char>();
     PBT_CUDA_TRY(cudaMemcpyAsync(b + o_fo, face_off, (nfaces + 1) * 8, cudaMemcpyHostToDevice, st));
     PBT_CUDA_TRY(cudaMemcpyAsync(b + o_fv, face_vi, nvi * 8, cudaMemcpyHostToDevice, st));
-    PBT_CUDA_TRY(cudaMemcpyAsync(b + o_v, verts, (size_t)norient * 3 * nverts * 8,
-                                 cudaMemcpyHostToDevice, st));
+    if (verts)  // else the caller copies the orientations' blocks
+        PBT_CUDA_TRY(cudaMemcpyAsync(b + o_v, verts, (size_t)norient * 3 * nverts * 8,
+                                     cudaMemcpyHostToDevice, st));
     G.face_off = (const int64_t *)(b + o_fo);
     G.face_vi = (const int64_t *)(b + o_fv);
     G.verts = (const double *)(b + o_v);
@@ -372,25 +373,53 @@ int batch_common_checks(pbt_ctx *ctx, int64_t norient, const int64_t *beam_off,
 
 }  // namespace
 
-extern "C" int pbt_diff_batch_c(pbt_ctx *ctx, int64_t norient, const pbt_outbeam *beam,
-                                const int64_t *beam_off, const pbt_outbeam *ext,
-                                const int64_t *ext_off, const double *verts, int64_t nverts,
-                                const int64_t *face_off, const int64_t *face_vi, int64_t nfaces,
-                                const double *theta, int64_t ntheta, const double *phi,
-                                int64_t nphi, double lambda, int32_t is_fast_diff, int32_t scaling,
-                                int32_t precision, const pbt_output_params *params_in,
-                                double *mueller_avg, double *mueller_1d_avg,
-                                pbt_output_params *params_avg,
-                                pbt_output_params *params_per_orient) {
-    API_ENTER(ctx);
+namespace {
+
+// The host batch over per-orientation arrays: beams[o] (boff[o+1]-boff[o]
+// records), exts[o], verts[o] (nverts x 3, column-major).  Both host batch
+// entry points land here; consecutive orientations whose arrays are adjacent
+// in memory are copied in one piece.
+struct HostRuns {
+    const pbt_outbeam *const *beam;
+    const pbt_outbeam *const *ext;
+    const double *const *verts;
+    const int64_t *boff, *eoff;
+};
+
+// Copies orientations [o0, o1) of one kind into consecutive device records.
+int copy_lists(const pbt_outbeam *const *src, const int64_t *off, int64_t o0, int64_t o1,
+               pbt_outbeam *dst, cudaStream_t s) {
+    int64_t o = o0;
+    while (o < o1) {
+        const pbt_outbeam *p = src[o];
+        int64_t n = off[o + 1] - off[o], e = o + 1;
+        while (e < o1 && src[e] == p + n) {
+            n += off[e + 1] - off[e];
+            e++;
+        }
+        if (n) PBT_CUDA_TRY(cudaMemcpyAsync(dst + (off[o] - off[o0]), p, n * sizeof(pbt_outbeam),
+                                            cudaMemcpyHostToDevice, s));
+        o = e;
+    }
+    return PBT_OK;
+}
+
+int host_batch(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const HostRuns &H, int64_t nverts,
+               const int64_t *face_off, const int64_t *face_vi, int64_t nfaces,
+               const double *theta, int64_t ntheta, const double *phi, int64_t nphi,
+               double lambda, int32_t is_fast_diff, int32_t scaling, int32_t precision,
+               const pbt_output_params *params_in, double *mueller_avg, double *mueller_1d_avg,
+               pbt_output_params *params_avg, pbt_output_params *params_per_orient) {
+    const int64_t *beam_off = H.boff, *ext_off = H.eoff;
     PBT_TRY(batch_common_checks(ctx, norient, beam_off, ext_off, face_off, nfaces, theta, ntheta,
                                 phi, nphi, lambda, precision, mueller_avg, mueller_1d_avg,
                                 params_avg, params_in));
-    PBT_TRY(validate_geometry(verts, nverts, face_off, face_vi, nfaces));
-    for (int64_t o = 1; o < norient; o++)
-        PBT_TRY(validate_geometry(verts + o * 3 * nverts, nverts, face_off, face_vi, nfaces));
-    PBT_TRY(validate_outbeams(beam, beam_off[norient], nfaces, "beam"));
-    PBT_TRY(validate_outbeams(ext, ext_off[norient], nfaces, "external diffraction"));
+    for (int64_t o = 0; o < norient; o++) {
+        PBT_TRY(validate_geometry(H.verts[o], nverts, face_off, face_vi, nfaces));
+        PBT_TRY(validate_outbeams(H.beam[o], beam_off[o + 1] - beam_off[o], nfaces, "beam"));
+        PBT_TRY(validate_outbeams(H.ext[o], ext_off[o + 1] - ext_off[o], nfaces,
+                                  "external diffraction"));
+    }
     PBT_TRY(grid_prepare(ctx, theta, ntheta, phi, nphi, st));
     PBT_TRY(check_grid_ready(ctx));
     const int64_t nb = ctx->grid.nb;
@@ -405,10 +434,10 @@ extern "C" int pbt_diff_batch_c(pbt_ctx *ctx, int64_t norient, const pbt_outbeam
         double *d_afb = ctx->d_out.as<double>(), *d_afe = d_afb + 8 * nb;
         double *d_mu = ctx->d_mu.as<double>(), *d_m1 = d_mu + 16 * nb, *d_p = d_m1 + 16 * ntheta;
         for (int64_t o = 0; o < norient; o++) {
-            PBT_TRY(fp64_diff_main_device(ctx, st, beam + beam_off[o], beam_off[o + 1] - beam_off[o],
-                                          ext + ext_off[o], ext_off[o + 1] - ext_off[o],
-                                          verts + o * 3 * nverts, nverts, face_off, face_vi, nfaces,
-                                          lambda, is_fast_diff ? 1 : 0, d_afb, d_afe));
+            PBT_TRY(fp64_diff_main_device(ctx, st, H.beam[o], beam_off[o + 1] - beam_off[o],
+                                          H.ext[o], ext_off[o + 1] - ext_off[o], H.verts[o],
+                                          nverts, face_off, face_vi, nfaces, lambda,
+                                          is_fast_diff ? 1 : 0, d_afb, d_afe));
             PBT_TRY(k3_finalise(ctx, st, d_afb, d_afe, lambda, scaling ? 1 : 0, &params_in[o], d_mu,
                                 d_m1, d_p, &T));
             if (params_per_orient)
@@ -423,29 +452,123 @@ extern "C" int pbt_diff_batch_c(pbt_ctx *ctx, int64_t norient, const pbt_outbeam
         PBT_CUDA_TRY(cudaStreamSynchronize(st));
         return PBT_OK;
     }
-    // FP32 batched path: stage inputs, run on the device, fetch outputs
+    // FP32 batched path.  The orientations go in runs of about an eighth of the
+    // outbeams each: run k+1's outbeams are copied on the copy stream into one
+    // of two slots while run k computes on the compute stream.
     GeoDev G;
-    PBT_TRY(upload_geometry(ctx, st, verts, nverts, norient, face_off, face_vi, nfaces, G));
+    {
+        const bool contiguous = [&] {
+            for (int64_t o = 1; o < norient; o++)
+                if (H.verts[o] != H.verts[0] + o * 3 * nverts) return false;
+            return true;
+        }();
+        PBT_TRY(upload_geometry(ctx, st, contiguous ? H.verts[0] : nullptr, nverts, norient,
+                                face_off, face_vi, nfaces, G));
+        if (!contiguous)
+            for (int64_t o = 0; o < norient; o++)
+                PBT_CUDA_TRY(cudaMemcpyAsync(const_cast<double *>(G.verts) + o * 3 * nverts,
+                                             H.verts[o], 3 * nverts * 8, cudaMemcpyHostToDevice, st));
+    }
     const size_t ob = sizeof(pbt_outbeam);
     const int64_t nbt = beam_off[norient], net = ext_off[norient];
-    const size_t o_b = 0, o_e = al((nbt + 1) * ob), o_pi = al(o_e + (net + 1) * ob),
-                 o_pp = al(o_pi + norient * sizeof(pbt_output_params)),
+    std::vector<int64_t> run{0};
+    {
+        const int64_t target = std::max<int64_t>((nbt + net) / 8, 262144);
+        int64_t acc = 0;
+        for (int64_t o = 0; o < norient; o++) {
+            acc += (beam_off[o + 1] - beam_off[o]) + (ext_off[o + 1] - ext_off[o]);
+            if (acc >= target && o + 1 < norient) {
+                run.push_back(o + 1);
+                acc = 0;
+            }
+        }
+        run.push_back(norient);
+    }
+    const int64_t nrun = (int64_t)run.size() - 1;
+    int64_t mb = 0, me = 0, mo = 0;
+    for (int64_t k = 0; k < nrun; k++) {
+        mb = std::max(mb, beam_off[run[k + 1]] - beam_off[run[k]]);
+        me = std::max(me, ext_off[run[k + 1]] - ext_off[run[k]]);
+        mo = std::max(mo, run[k + 1] - run[k]);
+    }
+    const int nslot = nrun > 1 ? 2 : 1;
+    size_t o_slot[2][2], off = 0;
+    for (int i = 0; i < nslot; i++) {
+        o_slot[i][0] = off;
+        off = al(off + (mb + 1) * ob);
+        o_slot[i][1] = off;
+        off = al(off + (me + 1) * ob);
+    }
+    const size_t o_pi = off, o_pp = al(o_pi + norient * sizeof(pbt_output_params)),
                  o_mu = al(o_pp + norient * sizeof(pbt_output_params)),
                  o_m1 = al(o_mu + 16 * nb * 8), o_pa = al(o_m1 + 16 * ntheta * 8),
                  o_end = al(o_pa + sizeof(pbt_output_params));
     PBT_TRY(ctx->d_fac.ensure(o_end));
     char *b = ctx->d_fac.as<char>();
-    pbt_outbeam *d_beam = (pbt_outbeam *)(b + o_b), *d_ext = (pbt_outbeam *)(b + o_e);
     pbt_output_params *d_pin = (pbt_output_params *)(b + o_pi), *d_pp = (pbt_output_params *)(b + o_pp),
                       *d_pa = (pbt_output_params *)(b + o_pa);
     double *d_mu = (double *)(b + o_mu), *d_m1 = (double *)(b + o_m1);
-    if (nbt) PBT_CUDA_TRY(cudaMemcpyAsync(d_beam, beam, nbt * ob, cudaMemcpyHostToDevice, st));
-    if (net) PBT_CUDA_TRY(cudaMemcpyAsync(d_ext, ext, net * ob, cudaMemcpyHostToDevice, st));
     PBT_CUDA_TRY(cudaMemcpyAsync(d_pin, params_in, norient * sizeof(pbt_output_params),
                                  cudaMemcpyHostToDevice, st));
-    PBT_TRY(k2_batch_impl(ctx, st, norient, d_beam, beam_off, d_ext, ext_off, G.verts, nverts,
-                          face_off, G.face_off, G.face_vi, nfaces, lambda, is_fast_diff ? 1 : 0,
-                          scaling ? 1 : 0, d_pin, d_mu, d_m1, d_pa, d_pp, 1));
+    cudaStream_t cs = st;
+    if (nrun > 1) {
+        if (!ctx->copy_stream)
+            PBT_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; i++) {
+            if (!ctx->up_ev[i]) PBT_CUDA_TRY(cudaEventCreateWithFlags(&ctx->up_ev[i], cudaEventDisableTiming));
+            if (!ctx->done_ev[i]) PBT_CUDA_TRY(cudaEventCreateWithFlags(&ctx->done_ev[i], cudaEventDisableTiming));
+        }
+        cs = ctx->copy_stream;
+        try {
+            if (ctx->h_gather.size() < (size_t)(mb + me + 2) * ob) ctx->h_gather.resize((size_t)(mb + me + 2) * ob);
+        } catch (...) {
+            set_error("batch: out of host memory for the gather buffer");
+            return PBT_ENOMEM;
+        }
+        // the slots (and the buffers before them) may still be read by earlier work on st
+        PBT_CUDA_TRY(cudaEventRecord(ctx->done_ev[0], st));
+        PBT_CUDA_TRY(cudaStreamWaitEvent(cs, ctx->done_ev[0], 0));
+    }
+    K2Batch B;
+    PBT_TRY(k2_batch_begin(ctx, st, norient, mo, d_pp, B));
+    std::vector<int64_t> hbo(mo + 1), heo(mo + 1);
+    for (int64_t k = 0; k < nrun; k++) {
+        const int slot = (int)(k % nslot);
+        const int64_t o0 = run[k], no = run[k + 1] - run[k];
+        const int64_t b0 = beam_off[o0], e0 = ext_off[o0];
+        const int64_t nbk = beam_off[o0 + no] - b0, nek = ext_off[o0 + no] - e0;
+        pbt_outbeam *d_beam = (pbt_outbeam *)(b + o_slot[slot][0]);
+        pbt_outbeam *d_ext = (pbt_outbeam *)(b + o_slot[slot][1]);
+        if (nrun > 1) {
+            // gather the run on the host (threads), then one copy per kind; the
+            // copy returns once the host buffer is staged, so one buffer serves
+            char *hb = ctx->h_gather.data();
+            pbt_outbeam *hbeam = (pbt_outbeam *)hb, *hext = (pbt_outbeam *)(hb + mb * ob);
+#pragma omp parallel for schedule(dynamic, 8)
+            for (int64_t o = o0; o < o0 + no; o++) {
+                const int64_t nbo = beam_off[o + 1] - beam_off[o], neo = ext_off[o + 1] - ext_off[o];
+                if (nbo) memcpy(hbeam + (beam_off[o] - b0), H.beam[o], nbo * ob);
+                if (neo) memcpy(hext + (ext_off[o] - e0), H.ext[o], neo * ob);
+            }
+            if (k >= 2) PBT_CUDA_TRY(cudaStreamWaitEvent(cs, ctx->done_ev[slot], 0));
+            if (nbk) PBT_CUDA_TRY(cudaMemcpyAsync(d_beam, hbeam, nbk * ob, cudaMemcpyHostToDevice, cs));
+            if (nek) PBT_CUDA_TRY(cudaMemcpyAsync(d_ext, hext, nek * ob, cudaMemcpyHostToDevice, cs));
+            PBT_CUDA_TRY(cudaEventRecord(ctx->up_ev[slot], cs));
+            PBT_CUDA_TRY(cudaStreamWaitEvent(st, ctx->up_ev[slot], 0));
+        } else {
+            if (nbk) PBT_TRY(copy_lists(H.beam, beam_off, o0, o0 + no, d_beam, cs));
+            if (nek) PBT_TRY(copy_lists(H.ext, ext_off, o0, o0 + no, d_ext, cs));
+        }
+        for (int64_t q = 0; q <= no; q++) {
+            hbo[q] = beam_off[o0 + q] - b0;
+            heo[q] = ext_off[o0 + q] - e0;
+        }
+        PBT_TRY(k2_batch_add(ctx, st, B, o0, no, d_beam, hbo.data(), d_ext, heo.data(),
+                             G.verts + o0 * 3 * nverts, nverts, face_off, G.face_off, G.face_vi,
+                             nfaces, lambda, is_fast_diff ? 1 : 0, scaling ? 1 : 0, d_pin));
+        if (nrun > 1) PBT_CUDA_TRY(cudaEventRecord(ctx->done_ev[slot], st));
+    }
+    PBT_TRY(k2_batch_finish(ctx, st, B, d_pin, d_mu, d_m1, d_pa, 1));
     PBT_CUDA_TRY(cudaMemcpyAsync(mueller_avg, d_mu, 16 * nb * 8, cudaMemcpyDeviceToHost, st));
     PBT_CUDA_TRY(cudaMemcpyAsync(mueller_1d_avg, d_m1, 16 * ntheta * 8, cudaMemcpyDeviceToHost, st));
     PBT_CUDA_TRY(cudaMemcpyAsync(params_avg, d_pa, sizeof(pbt_output_params), cudaMemcpyDeviceToHost,
@@ -455,6 +578,70 @@ extern "C" int pbt_diff_batch_c(pbt_ctx *ctx, int64_t norient, const pbt_outbeam
                                      cudaMemcpyDeviceToHost, st));
     PBT_CUDA_TRY(cudaStreamSynchronize(st));
     return PBT_OK;
+}
+
+}  // namespace
+
+extern "C" int pbt_diff_batch_c(pbt_ctx *ctx, int64_t norient, const pbt_outbeam *beam,
+                                const int64_t *beam_off, const pbt_outbeam *ext,
+                                const int64_t *ext_off, const double *verts, int64_t nverts,
+                                const int64_t *face_off, const int64_t *face_vi, int64_t nfaces,
+                                const double *theta, int64_t ntheta, const double *phi,
+                                int64_t nphi, double lambda, int32_t is_fast_diff, int32_t scaling,
+                                int32_t precision, const pbt_output_params *params_in,
+                                double *mueller_avg, double *mueller_1d_avg,
+                                pbt_output_params *params_avg,
+                                pbt_output_params *params_per_orient) {
+    API_ENTER(ctx);
+    if (norient < 1 || !verts) {
+        set_error(norient < 1 ? "norient must be >= 1" : "batch: verts must not be NULL");
+        return PBT_EINVAL;
+    }
+    PBT_TRY(check_offsets(beam_off, norient, "beam"));
+    PBT_TRY(check_offsets(ext_off, norient, "ext"));
+    std::vector<const pbt_outbeam *> pb(norient), pe(norient);
+    std::vector<const double *> pv(norient);
+    for (int64_t o = 0; o < norient; o++) {
+        pb[o] = beam ? beam + beam_off[o] : nullptr;
+        pe[o] = ext ? ext + ext_off[o] : nullptr;
+        pv[o] = verts + o * 3 * nverts;
+    }
+    const HostRuns H{pb.data(), pe.data(), pv.data(), beam_off, ext_off};
+    return host_batch(ctx, st, norient, H, nverts, face_off, face_vi, nfaces, theta, ntheta, phi,
+                      nphi, lambda, is_fast_diff, scaling, precision, params_in, mueller_avg,
+                      mueller_1d_avg, params_avg, params_per_orient);
+}
+
+extern "C" int pbt_diff_batch_list_c(pbt_ctx *ctx, int64_t norient,
+                                     const pbt_outbeam *const *beams, const int64_t *nbeam,
+                                     const pbt_outbeam *const *exts, const int64_t *next,
+                                     const double *const *verts, int64_t nverts,
+                                     const int64_t *face_off, const int64_t *face_vi,
+                                     int64_t nfaces, const double *theta, int64_t ntheta,
+                                     const double *phi, int64_t nphi, double lambda,
+                                     int32_t is_fast_diff, int32_t scaling, int32_t precision,
+                                     const pbt_output_params *params_in, double *mueller_avg,
+                                     double *mueller_1d_avg, pbt_output_params *params_avg,
+                                     pbt_output_params *params_per_orient) {
+    API_ENTER(ctx);
+    if (norient < 1 || !beams || !nbeam || !exts || !next || !verts) {
+        set_error(norient < 1 ? "norient must be >= 1" : "batch: NULL list argument");
+        return PBT_EINVAL;
+    }
+    std::vector<int64_t> boff(norient + 1, 0), eoff(norient + 1, 0);
+    for (int64_t o = 0; o < norient; o++) {
+        if (nbeam[o] < 0 || next[o] < 0 || !verts[o]) {
+            set_error("batch: orientation %lld has a negative count or NULL vertices",
+                      (long long)(o + 1));
+            return PBT_EINVAL;
+        }
+        boff[o + 1] = boff[o] + nbeam[o];
+        eoff[o + 1] = eoff[o] + next[o];
+    }
+    const HostRuns H{beams, exts, verts, boff.data(), eoff.data()};
+    return host_batch(ctx, st, norient, H, nverts, face_off, face_vi, nfaces, theta, ntheta, phi,
+                      nphi, lambda, is_fast_diff, scaling, precision, params_in, mueller_avg,
+                      mueller_1d_avg, params_avg, params_per_orient);
 }
 
 namespace {

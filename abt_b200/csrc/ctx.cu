@@ -196,13 +196,22 @@ extern "C" int pbt_ctx_destroy(pbt_ctx *ctx) {
         DevBuf *bufs[] = {&ctx->d_fac, &ctx->d_edge, &ctx->d_out,  &ctx->d_mu,
                           &ctx->d_m1,  &ctx->d_misc, &ctx->d_in,   &ctx->d_rec,
                           &ctx->d_ws,  &ctx->d_scan, &ctx->d_items, &ctx->grid.xyz, &ctx->grid.phitab,
-                          &ctx->grid.thtab, &ctx->grid.wbin, &ctx->grid.wphi};
+                          &ctx->grid.thtab, &ctx->grid.wbin, &ctx->grid.wphi,
+                          &ctx->grid.fast_perm, &ctx->grid.fast_cone};
         for (DevBuf *b : bufs) b->release();
         ctx->tot.release();
         ctx->btot.release();
         ctx->h_stage.release();
         for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
         if (ctx->stage_ev) cudaEventDestroy(ctx->stage_ev);
+        for (int i = 0; i < 2; i++) {
+            if (ctx->up_ev[i]) cudaEventDestroy(ctx->up_ev[i]);
+            if (ctx->done_ev[i]) cudaEventDestroy(ctx->done_ev[i]);
+        }
+        if (ctx->copy_stream) {
+            cudaStreamSynchronize(ctx->copy_stream);
+            cudaStreamDestroy(ctx->copy_stream);
+        }
         cudaStreamDestroy(ctx->stream);
     }
     delete ctx;

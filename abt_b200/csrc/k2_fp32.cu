@@ -1294,12 +1294,6 @@ namespace {
 // K2Pair records, 0 = one facet per step over K2Rec records.  bpt = bins per
 // thread, rpi = facet records per work item.  PBT_K2_PLAN="variant,bpt,rpi"
 // overrides the default (used by the tuner).
-struct K2Plan {
-    int variant = 1;
-    int bpt = 1;
-    int64_t rpi = 2048;
-};
-
 K2Plan k2_plan_for(const pbt_ctx *ctx) {
     K2Plan p;
     if (ctx->plan_variant >= 0) {
@@ -1636,8 +1630,117 @@ int k2_check_err(pbt_ctx *ctx, cudaStream_t st, const int *d_err) {
     return PBT_OK;
 }
 
-// Batched FP32 orientation average.  h_beam_off / h_ext_off / h_face_off are
-// host arrays; every other array is device memory.
+// Batched FP32 orientation average in three steps: begin (the orientation
+// sums and per-orientation results for norient orientations), add (a run of
+// orientations [o0, o0+no): record set-up, the far-field sum and the
+// epilogue into the sums), finish (averages and phi integrals).
+// h_beam_off / h_ext_off (relative to the run) and h_face_off are host arrays;
+// every other array is device memory.
+namespace {
+__global__ void k2_err_fold_kernel(const int *__restrict__ run_err, int *__restrict__ total) {
+    if (threadIdx.x == 0 && *run_err) atomicOr(total, *run_err);
+}
+}  // namespace
+
+int k2_batch_begin(pbt_ctx *ctx, cudaStream_t st, int64_t norient, int64_t max_run,
+                   const pbt_output_params *d_params_per, K2Batch &B) {
+    const GridCache &g = ctx->grid;
+    const int64_t nb = g.nb;
+    B.norient = norient;
+    B.plan = k2_plan_for(ctx);
+    // orientation chunks of the workspace, capped at 8 GiB
+    const size_t per_orient = (size_t)2 * 8 * nb * sizeof(float);
+    const size_t cap = (size_t)8 << 30;
+    B.wchunk = std::max<int64_t>(1, std::min<int64_t>(max_run, (int64_t)(cap / per_orient)));
+    const int64_t chunk = B.wchunk;
+    // d_ws: workspace | mu_sum | per-orient red (6) | bs | scale (2) | per-orient params | seg/items
+    const size_t o_ws = 0, o_mu = align_up(o_ws + chunk * per_orient),
+                 o_red = align_up(o_mu + 16 * nb * 8), o_bs = align_up(o_red + 6 * norient * 8),
+                 o_sc = align_up(o_bs + norient * 8), o_pp = align_up(o_sc + 2 * norient * 8),
+                 o_seg = align_up(o_pp + norient * sizeof(pbt_output_params)),
+                 o_it = align_up(o_seg + (2 * chunk + 1) * 8), o_cnt = align_up(o_it + (2 * chunk + 1) * 8),
+                 o_err = align_up(o_cnt + 64), o_end = align_up(o_err + 64);
+    PBT_TRY(ctx->d_ws.ensure(o_end));
+    char *base = ctx->d_ws.as<char>();
+    B.err = (int *)(base + o_err);
+    PBT_CUDA_TRY(cudaMemsetAsync(B.err, 0, sizeof(int), st));
+    B.ws = (float *)(base + o_ws);
+    B.mu_sum = (double *)(base + o_mu);
+    B.redo = (double *)(base + o_red);
+    B.bs = (double *)(base + o_bs);
+    B.scale = (double *)(base + o_sc);
+    B.pp = d_params_per ? const_cast<pbt_output_params *>(d_params_per) : (pbt_output_params *)(base + o_pp);
+    B.seg_rec = (int64_t *)(base + o_seg);
+    B.item_pre = (int64_t *)(base + o_it);
+    B.counter = (unsigned long long *)(base + o_cnt);
+    PBT_CUDA_TRY(cudaMemsetAsync(B.mu_sum, 0, 16 * nb * 8, st));
+    PBT_CUDA_TRY(cudaMemsetAsync(B.redo, 0, 6 * norient * 8, st));
+    PBT_CUDA_TRY(cudaMemsetAsync(B.bs, 0, norient * 8, st));
+    PBT_CUDA_TRY(cudaMemsetAsync(B.scale, 0, 2 * norient * 8, st));
+    return PBT_OK;
+}
+
+int k2_batch_add(pbt_ctx *ctx, cudaStream_t st, K2Batch &B, int64_t o0, int64_t no,
+                 const pbt_outbeam *d_beam, const int64_t *h_beam_off, const pbt_outbeam *d_ext,
+                 const int64_t *h_ext_off, const double *d_verts, int64_t nverts,
+                 const int64_t *h_face_off, const int64_t *d_face_off, const int64_t *d_face_vi,
+                 int64_t nfaces, double lambda, int fast_diff, int scaling,
+                 const pbt_output_params *d_params_in) {
+    const GridCache &g = ctx->grid;
+    const int64_t nb = g.nb, nphi = (int64_t)g.phi.size(), ntheta = (int64_t)g.theta.size();
+    K2Setup S;
+    PBT_TRY(k2_prepare(ctx, st, no, d_beam, h_beam_off, d_ext, h_ext_off, d_verts, nverts,
+                       d_face_off, d_face_vi, nfaces, max_face_nv(h_face_off, nfaces), lambda,
+                       fast_diff, B.plan.variant, S));
+    const double waveno = 2.0 * kPiRef / lambda;
+    const double *phitab = g.phitab.as<double>(), *sth = g.thtab.as<double>(), *cth = sth + ntheta;
+    (void)sth;
+    const int64_t back_bin = 0 + nphi * g.back_i;
+    const int eb = 256;
+    const unsigned egrid = (unsigned)((nb + eb - 1) / eb);
+    for (int64_t l0 = 0; l0 < no; l0 += B.wchunk) {
+        const int64_t n = std::min(B.wchunk, no - l0);
+        PBT_TRY(k2_run_chunk(ctx, st, S, l0, n, lambda, fast_diff, B.plan, B.ws, B.seg_rec,
+                             B.item_pre, B.counter));
+        const int64_t og = o0 + l0;  // global orientation of the workspace's first slot
+        if (scaling) {
+            k2_scatt_be_kernel<<<egrid, eb, 0, st>>>(B.ws, n, og, nb, nphi, phitab, waveno,
+                                                     g.wbin.as<double>(), B.scale);
+            k2_scale_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(B.scale, d_params_in, og, n);
+            ctx->launches += 2;
+        }
+        k2_epi_kernel<<<egrid, eb, 0, st>>>(B.ws, n, og, nb, nphi, phitab, cth, waveno,
+                                            g.wbin.as<double>(), back_bin, scaling ? B.scale : nullptr,
+                                            B.mu_sum, B.redo, B.bs);
+        ctx->launches++;
+        PBT_CUDA_TRY(cudaGetLastError());
+    }
+    // the run's error flags (its set-up buffer is reused by the next run)
+    k2_err_fold_kernel<<<1, 32, 0, st>>>(S.err, B.err);
+    ctx->launches++;
+    PBT_CUDA_TRY(cudaGetLastError());
+    return PBT_OK;
+}
+
+int k2_batch_finish(pbt_ctx *ctx, cudaStream_t st, K2Batch &B, const pbt_output_params *d_params_in,
+                    double *d_mueller_avg, double *d_m1d_avg, pbt_output_params *d_params_avg,
+                    int check_errors) {
+    const GridCache &g = ctx->grid;
+    const int64_t nb = g.nb, nphi = (int64_t)g.phi.size(), ntheta = (int64_t)g.theta.size();
+    const int64_t norient = B.norient;
+    k2_final_kernel<<<(unsigned)((norient + 127) / 128), 128, 0, st>>>(B.redo, B.bs, d_params_in,
+                                                                       norient, B.pp);
+    k2_param_avg_kernel<<<1, 32, 0, st>>>(B.pp, norient, d_params_avg);
+    k2_mu_avg_kernel<<<(unsigned)((16 * nb + 255) / 256), 256, 0, st>>>(
+        B.mu_sum, 16 * nb, 1.0 / (double)norient, (double)norient, d_mueller_avg);
+    k2_phi_int_kernel<<<(unsigned)((16 * ntheta + 127) / 128), 128, 0, st>>>(
+        d_mueller_avg, g.wphi.as<double>(), nphi, ntheta, d_m1d_avg);
+    ctx->launches += 4;
+    PBT_CUDA_TRY(cudaGetLastError());
+    if (check_errors) PBT_TRY(k2_check_err(ctx, st, B.err));
+    return PBT_OK;
+}
+
 int k2_batch_impl(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam *d_beam,
                   const int64_t *h_beam_off, const pbt_outbeam *d_ext, const int64_t *h_ext_off,
                   const double *d_verts, int64_t nverts, const int64_t *h_face_off,
@@ -1645,68 +1748,13 @@ int k2_batch_impl(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outb
                   double lambda, int fast_diff, int scaling, const pbt_output_params *d_params_in,
                   double *d_mueller_avg, double *d_m1d_avg, pbt_output_params *d_params_avg,
                   pbt_output_params *d_params_per, int check_errors) {
-    const GridCache &g = ctx->grid;
-    const int64_t nb = g.nb, nphi = (int64_t)g.phi.size(), ntheta = (int64_t)g.theta.size();
-    const K2Plan plan = k2_plan_for(ctx);
-    K2Setup S;
-    PBT_TRY(k2_prepare(ctx, st, norient, d_beam, h_beam_off, d_ext, h_ext_off, d_verts, nverts,
-                       d_face_off, d_face_vi, nfaces, max_face_nv(h_face_off, nfaces), lambda,
-                       fast_diff, plan.variant, S));
-    // orientation chunks sized to a workspace cap
-    const size_t per_orient = (size_t)2 * 8 * nb * sizeof(float);
-    const size_t cap = (size_t)8 << 30;
-    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(norient, (int64_t)(cap / per_orient)));
-    // d_ws: workspace | mu_sum | per-orient red (6) | bs | scale (2) | per-orient params | seg/items
-    const size_t o_ws = 0, o_mu = align_up(o_ws + chunk * per_orient),
-                 o_red = align_up(o_mu + 16 * nb * 8), o_bs = align_up(o_red + 6 * norient * 8),
-                 o_sc = align_up(o_bs + norient * 8), o_pp = align_up(o_sc + 2 * norient * 8),
-                 o_seg = align_up(o_pp + norient * sizeof(pbt_output_params)),
-                 o_it = align_up(o_seg + (2 * chunk + 1) * 8), o_cnt = align_up(o_it + (2 * chunk + 1) * 8),
-                 o_end = align_up(o_cnt + 64);
-    PBT_TRY(ctx->d_ws.ensure(o_end));
-    char *base = ctx->d_ws.as<char>();
-    float *ws = (float *)(base + o_ws);
-    double *mu_sum = (double *)(base + o_mu), *redo = (double *)(base + o_red),
-           *bs = (double *)(base + o_bs), *scale = (double *)(base + o_sc);
-    pbt_output_params *pp = d_params_per ? d_params_per : (pbt_output_params *)(base + o_pp);
-    int64_t *seg_rec = (int64_t *)(base + o_seg), *item_pre = (int64_t *)(base + o_it);
-    unsigned long long *counter = (unsigned long long *)(base + o_cnt);
-    PBT_CUDA_TRY(cudaMemsetAsync(mu_sum, 0, 16 * nb * 8, st));
-    PBT_CUDA_TRY(cudaMemsetAsync(redo, 0, 6 * norient * 8, st));
-    PBT_CUDA_TRY(cudaMemsetAsync(bs, 0, norient * 8, st));
-    PBT_CUDA_TRY(cudaMemsetAsync(scale, 0, 2 * norient * 8, st));
-    const double waveno = 2.0 * kPiRef / lambda;
-    const double *phitab = g.phitab.as<double>(), *sth = g.thtab.as<double>(), *cth = sth + ntheta;
-    const int64_t back_bin = 0 + nphi * g.back_i;
-    const int eb = 256;
-    const unsigned egrid = (unsigned)((nb + eb - 1) / eb);
-    for (int64_t o0 = 0; o0 < norient; o0 += chunk) {
-        const int64_t no = std::min(chunk, norient - o0);
-        PBT_TRY(k2_run_chunk(ctx, st, S, o0, no, lambda, fast_diff, plan, ws, seg_rec, item_pre,
-                             counter));
-        if (scaling) {
-            k2_scatt_be_kernel<<<egrid, eb, 0, st>>>(ws, no, o0, nb, nphi, phitab, waveno,
-                                                     g.wbin.as<double>(), scale);
-            k2_scale_kernel<<<(unsigned)((no + 127) / 128), 128, 0, st>>>(scale, d_params_in, o0, no);
-            ctx->launches += 2;
-        }
-        k2_epi_kernel<<<egrid, eb, 0, st>>>(ws, no, o0, nb, nphi, phitab, cth, waveno,
-                                            g.wbin.as<double>(), back_bin, scaling ? scale : nullptr,
-                                            mu_sum, redo, bs);
-        ctx->launches++;
-        PBT_CUDA_TRY(cudaGetLastError());
-    }
-    k2_final_kernel<<<(unsigned)((norient + 127) / 128), 128, 0, st>>>(redo, bs, d_params_in,
-                                                                       norient, pp);
-    k2_param_avg_kernel<<<1, 32, 0, st>>>(pp, norient, d_params_avg);
-    k2_mu_avg_kernel<<<(unsigned)((16 * nb + 255) / 256), 256, 0, st>>>(
-        mu_sum, 16 * nb, 1.0 / (double)norient, (double)norient, d_mueller_avg);
-    k2_phi_int_kernel<<<(unsigned)((16 * ntheta + 127) / 128), 128, 0, st>>>(
-        d_mueller_avg, g.wphi.as<double>(), nphi, ntheta, d_m1d_avg);
-    ctx->launches += 4;
-    PBT_CUDA_TRY(cudaGetLastError());
-    if (check_errors) PBT_TRY(k2_check_err(ctx, st, S.err));
-    return PBT_OK;
+    K2Batch B;
+    PBT_TRY(k2_batch_begin(ctx, st, norient, norient, d_params_per, B));
+    PBT_TRY(k2_batch_add(ctx, st, B, 0, norient, d_beam, h_beam_off, d_ext, h_ext_off, d_verts,
+                         nverts, h_face_off, d_face_off, d_face_vi, nfaces, lambda, fast_diff,
+                         scaling, d_params_in));
+    return k2_batch_finish(ctx, st, B, d_params_in, d_mueller_avg, d_m1d_avg, d_params_avg,
+                           check_errors);
 }
 
 // FP32 diff_main: one orientation, amplitude grids in the reference layout.

@@ -110,6 +110,10 @@ struct pbt_ctx {
     int device = 0;
     std::mutex mu;
     cudaStream_t stream = nullptr;   // internal stream of the host-pointer entry points
+    cudaStream_t copy_stream = nullptr;       // uploads of the next orientation run (batch)
+    cudaEvent_t up_ev[2] = {nullptr, nullptr};    // run uploaded into slot i
+    cudaEvent_t done_ev[2] = {nullptr, nullptr};  // compute done with slot i
+    std::vector<char> h_gather;                // host gather buffer of one batch run
     pbt::GridCache grid;
     // scratch (grow-only)
     pbt::DevBuf d_fac, d_edge, d_out, d_mu, d_m1, d_misc, d_in, d_rec, d_ws, d_scan, d_items;
@@ -163,6 +167,33 @@ int totals_add_device(pbt_ctx *ctx, DevTotals &T, cudaStream_t st, const double 
 
 // Batched FP32 path.  h_beam_off / h_ext_off / h_face_off are host arrays,
 // every other pointer is device memory.
+// Batched FP32 average in steps (k2_batch_impl = begin + one add + finish).
+struct K2Plan {
+    int variant = 1;   // 0: one record per step, 1: two records packed (FP32x2)
+    int bpt = 1;       // bins per thread
+    int64_t rpi = 2048;  // facet records per work item
+};
+struct K2Batch {
+    int64_t norient = 0, wchunk = 1;
+    K2Plan plan;
+    float *ws = nullptr;
+    double *mu_sum = nullptr, *redo = nullptr, *bs = nullptr, *scale = nullptr;
+    pbt_output_params *pp = nullptr;
+    int64_t *seg_rec = nullptr, *item_pre = nullptr;
+    unsigned long long *counter = nullptr;
+    int *err = nullptr;
+};
+int k2_batch_begin(pbt_ctx *ctx, cudaStream_t st, int64_t norient, int64_t max_run,
+                   const pbt_output_params *d_params_per, K2Batch &B);
+int k2_batch_add(pbt_ctx *ctx, cudaStream_t st, K2Batch &B, int64_t o0, int64_t no,
+                 const pbt_outbeam *d_beam, const int64_t *h_beam_off, const pbt_outbeam *d_ext,
+                 const int64_t *h_ext_off, const double *d_verts, int64_t nverts,
+                 const int64_t *h_face_off, const int64_t *d_face_off, const int64_t *d_face_vi,
+                 int64_t nfaces, double lambda, int fast_diff, int scaling,
+                 const pbt_output_params *d_params_in);
+int k2_batch_finish(pbt_ctx *ctx, cudaStream_t st, K2Batch &B, const pbt_output_params *d_params_in,
+                    double *d_mueller_avg, double *d_m1d_avg, pbt_output_params *d_params_avg,
+                    int check_errors);
 int k2_batch_impl(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam *d_beam,
                   const int64_t *h_beam_off, const pbt_outbeam *d_ext, const int64_t *h_ext_off,
                   const double *d_verts, int64_t nverts, const int64_t *h_face_off,

@@ -254,30 +254,36 @@ class Context:
         params_in: PARAMS_DTYPE array of length norient.
         Returns (mueller_avg, mueller_1d_avg, params_avg, params_per_orient)."""
         norient = len(beams)
-        # a single orientation is passed without a copy (keeps pinned buffers pinned)
-        beam = _ob(beams[0] if norient == 1 else np.concatenate(beams))
-        ext = _ob(exts[0] if norient == 1 else np.concatenate(exts))
-        boff = np.zeros(norient + 1, dtype=np.int64)
-        boff[1:] = np.cumsum([len(b) for b in beams])
-        eoff = np.zeros(norient + 1, dtype=np.int64)
-        eoff[1:] = np.cumsum([len(e) for e in exts])
+        if len(exts) != norient or len(verts_per_orient) != norient:
+            raise ValueError("beams, exts and verts_per_orient need one entry per orientation")
+        # each orientation's arrays go to the library as they are (no host-side
+        # gather; pinned arrays stay pinned): pbt_diff_batch_list_c
+        bl = [_ob(b) for b in beams]
+        el = [_ob(e) for e in exts]
+        vl = [np.asfortranarray(v, dtype=np.float64) for v in verts_per_orient]
+        nverts = vl[0].shape[0]
+        if any(v.shape != (nverts, 3) for v in vl):
+            raise ValueError("every orientation needs a (nverts, 3) vertex array")
         _, fo, fv = _geo(geometry)
-        nverts = np.asarray(verts_per_orient[0]).shape[0]
-        flat = [np.asfortranarray(v, dtype=np.float64).ravel(order="F") for v in verts_per_orient]
-        V = flat[0] if norient == 1 else np.concatenate(flat)
         theta = np.ascontiguousarray(theta, dtype=np.float64)
         phi = np.ascontiguousarray(phi, dtype=np.float64)
         pin = np.ascontiguousarray(params_in, dtype=PARAMS_DTYPE)
-        mu = np.zeros((len(phi), len(theta), 16), order="F")
-        mu1 = np.zeros((len(theta), 16), order="F")
+        mu = np.empty((len(phi), len(theta), 16), order="F")
+        mu1 = np.empty((len(theta), 16), order="F")
         pav = np.zeros((), dtype=PARAMS_DTYPE)
         pper = np.zeros(norient, dtype=PARAMS_DTYPE)
-        check(_lib.lib().pbt_diff_batch_c(self._h, norient, ptr(beam), ptr(boff), ptr(ext),
-                                          ptr(eoff), ptr(V), nverts, ptr(fo), ptr(fv), len(fo) - 1,
-                                          ptr(theta), len(theta), ptr(phi), len(phi), float(lam),
-                                          int(bool(is_fast_diff)), int(bool(scaling)),
-                                          _PREC[precision], ptr(pin), mu.ctypes.data,
-                                          mu1.ctypes.data, pav.ctypes.data, pper.ctypes.data))
+        VP = ctypes.c_void_p * norient
+        pb = VP(*[ptr(b) for b in bl])
+        pe = VP(*[ptr(e) for e in el])
+        pv = VP(*[v.ctypes.data for v in vl])
+        nbm = np.array([len(b) for b in bl], dtype=np.int64)
+        nex = np.array([len(e) for e in el], dtype=np.int64)
+        check(_lib.lib().pbt_diff_batch_list_c(
+            self._h, norient, ctypes.cast(pb, ctypes.c_void_p), nbm.ctypes.data,
+            ctypes.cast(pe, ctypes.c_void_p), nex.ctypes.data, ctypes.cast(pv, ctypes.c_void_p),
+            nverts, ptr(fo), ptr(fv), len(fo) - 1, ptr(theta), len(theta), ptr(phi), len(phi),
+            float(lam), int(bool(is_fast_diff)), int(bool(scaling)), _PREC[precision], ptr(pin),
+            mu.ctypes.data, mu1.ctypes.data, pav.ctypes.data, pper.ctypes.data))
         return mu, mu1, pav, pper
 
 

@@ -215,7 +215,7 @@ def orientation_average(ctx, args):
             "speedup_fp32_batched_vs_fp64_dropin": t64 / t32,
             "max_rel_mueller_err_vs_fp64": mueller_rel_err(f32[0], f64[0], 1e-6),
             "max_rel_param_err_vs_fp64": perr,
-            "api": "pbt_diff_batch_c (host pointers), wall clock"}
+            "api": "pbt_diff_batch_list_c (host pointers, one array per orientation), wall clock"}
 
 
 def large_case(ctx, args):
@@ -535,7 +535,7 @@ def main():
     d2h = 16 * nb * 8 + 16 * len(th) * 8 + 2 * pin.nbytes
     e2e = {"value": world * work / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3,
-           "api": "pbt_diff_batch_c (host pointers, pinned)"}
+           "api": "pbt_diff_batch_list_c (host pointers, pinned)"}
 
     # reference-exact FP64 drop-in rate on a facet sample
     if args.fp64_facets > 0:

@@ -195,6 +195,22 @@ int pbt_diff_batch_c(pbt_ctx *ctx, int64_t norient, const pbt_outbeam *beam,
                      double *mueller_avg, double *mueller_1d_avg, pbt_output_params *params_avg,
                      pbt_output_params *params_per_orient);
 
+/* Same as pbt_diff_batch_c with each orientation in its own host arrays (no
+ * counterpart in the reference; its orientation loop keeps one outbeam tree
+ * per orientation): beams[o] holds nbeam[o] records, exts[o] next[o] records
+ * (a NULL pointer is allowed for a zero count), verts[o] the orientation's
+ * v(nverts,3).  The arrays are copied to the device as they are, without a
+ * host-side gather. */
+int pbt_diff_batch_list_c(pbt_ctx *ctx, int64_t norient, const pbt_outbeam *const *beams,
+                          const int64_t *nbeam, const pbt_outbeam *const *exts,
+                          const int64_t *next, const double *const *verts, int64_t nverts,
+                          const int64_t *face_off, const int64_t *face_vi, int64_t nfaces,
+                          const double *theta, int64_t ntheta, const double *phi, int64_t nphi,
+                          double lambda, int32_t is_fast_diff, int32_t scaling, int32_t precision,
+                          const pbt_output_params *params_in, double *mueller_avg,
+                          double *mueller_1d_avg, pbt_output_params *params_avg,
+                          pbt_output_params *params_per_orient);
+
 /* Same as pbt_diff_batch_c with the bulk arrays already in device memory of
  * the context's device: beam, ext, verts, face_vi, params_in and all outputs
  * are device pointers; beam_off, ext_off, face_off, theta and phi are host

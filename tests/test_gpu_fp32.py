@@ -107,3 +107,44 @@ def test_fp32_fast_diff_tile_cull(ctx):
     a32n = ctx.diff_main(beam, ext, geo, th, ph, LAM, is_fast_diff=True, precision="fp32")
     ctx.set_plan(-1)
     assert mueller_rel_err(_mueller(*a32), _mueller(*a32n)) <= 1e-5
+
+
+def test_batch_runs_overlap_uploads(ctx):
+    """A host batch large enough to be split into runs (uploads of run k+1
+    overlap run k) gives the FP64 drop-in's average; a bad face index in a late
+    run is still reported."""
+    geo, Vs, beams, exts, pin = W.rough_column_orientations(40, seed=51, m_range=(20, 24))
+    assert sum(len(b) + len(e) for b, e in zip(beams, exts)) > 3 * 262144 // 2
+    th, ph = abt_b200.make_angles([0, 180], [10]), abt_b200.make_angles([0, 350], [10])
+    r32 = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp32")
+    r64 = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp64")
+    assert mueller_rel_err(r32[0], r64[0]) <= TOL_MU
+    for n in ("scatt", "ext", "asymmetry"):
+        assert abs(float(r32[2][n]) - float(r64[2][n])) <= TOL_PARAM * abs(float(r64[2][n]))
+
+
+def test_contiguous_batch_entry_matches_list_entry(ctx):
+    """pbt_diff_batch_c (one gathered array, CSR offsets) and
+    pbt_diff_batch_list_c (one array per orientation) give the same average."""
+    import ctypes
+    from abt_b200 import _lib
+    geo, Vs, beams, exts, pin = W.rough_column_orientations(5, seed=61, n_side=2, n_len=3,
+                                                            m_range=(0, 3))
+    th, ph = abt_b200.make_angles([0, 180], [5]), abt_b200.make_angles([0, 350], [10])
+    mu_l, m1_l, pav_l, _ = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp32")
+    beam = np.concatenate(beams)
+    ext = np.concatenate(exts)
+    boff = np.concatenate([[0], np.cumsum([len(b) for b in beams])]).astype(np.int64)
+    eoff = np.concatenate([[0], np.cumsum([len(e) for e in exts])]).astype(np.int64)
+    V = np.concatenate([np.asfortranarray(v).ravel(order="F") for v in Vs])
+    mu = np.empty((len(ph), len(th), 16), order="F")
+    m1 = np.empty((len(th), 16), order="F")
+    pav = np.zeros((), dtype=abt_b200.PARAMS_DTYPE)
+    fo, fv = geo["face_off"], geo["face_vi"]
+    _lib.check(_lib.lib().pbt_diff_batch_c(
+        ctx.handle, len(beams), beam.ctypes.data, boff.ctypes.data, ext.ctypes.data,
+        eoff.ctypes.data, V.ctypes.data, Vs[0].shape[0], fo.ctypes.data, fv.ctypes.data,
+        len(fo) - 1, th.ctypes.data, len(th), ph.ctypes.data, len(ph), LAM, 0, 0, 1,
+        pin.ctypes.data, mu.ctypes.data, m1.ctypes.data, pav.ctypes.data, None))
+    assert mueller_rel_err(mu, mu_l) <= 1e-5
+    assert abs(float(pav["scatt"]) - float(pav_l["scatt"])) <= 1e-6 * abs(float(pav_l["scatt"]))
