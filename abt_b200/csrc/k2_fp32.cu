@@ -1612,6 +1612,7 @@ int k2_wait_selftest(pbt_ctx *ctx, cudaStream_t st, uint64_t limit_ns) {
 }
 
 int k2_check_err(pbt_ctx *ctx, cudaStream_t st, const int *d_err) {
+    (void)ctx;
     int h = 0;
     PBT_CUDA_TRY(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     PBT_CUDA_TRY(cudaStreamSynchronize(st));
