@@ -662,14 +662,21 @@ struct BinPk {
 };
 
 // sin(h)/h (h >= 0) with one shared reciprocal: rh = 1/max(h, 0.5)
+// The series is evaluated only when a lane of the warp needs it: small gaps
+// occur near a facet's specular and forward directions, so whole warps of
+// neighbouring bins mostly skip it.  Every lane of the warp calls this.
 __device__ __forceinline__ float2 sinc_pk(float2 h, float2 rh) {
-    const float2 h2 = mul2(h, h);
-    const float2 p = fma2(h2, fma2(h2, fma2(h2, fma2(h2, bc2(2.7557319e-6f), bc2(-1.9841270e-4f)),
-                                            bc2(8.3333333e-3f)),
-                                   bc2(-1.6666667e-1f)),
-                          bc2(1.0f));
-    const float2 q = mul2(make_float2(__sinf(h.x), __sinf(h.y)), rh);
-    return sel2(h.x < 0.5f, h.y < 0.5f, p, q);
+    float2 q = mul2(make_float2(__sinf(h.x), __sinf(h.y)), rh);
+    const bool sx = h.x < 0.5f, sy = h.y < 0.5f;
+    if (__any_sync(0xffffffffu, sx || sy)) {
+        const float2 h2 = mul2(h, h);
+        const float2 p = fma2(h2, fma2(h2, fma2(h2, fma2(h2, bc2(2.7557319e-6f), bc2(-1.9841270e-4f)),
+                                                bc2(8.3333333e-3f)),
+                                       bc2(-1.6666667e-1f)),
+                              bc2(1.0f));
+        q = sel2(sx, sy, p, q);
+    }
+    return q;
 }
 
 // Second divided difference of e^{ix} at the three phases of each lane.
