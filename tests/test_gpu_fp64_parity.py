@@ -170,3 +170,22 @@ def test_diffraction_concurrent_callers(ctx):
                            range(len(obs))))
     for a, b in zip(serial, conc):
         assert np.array_equal(a, b)
+
+
+def test_diff_main_config_sized_hex_column(ctx):
+    """The plain-method configuration at its own size: a hexagonal column
+    (r 5 um, L 10 um, 0.26 um^2 triangles: 1,764 facets), Euler (30, 40, 10),
+    stand-in outbeams (~3,500), 181 theta x 180 phi; the FP64 drop-in against
+    the oracle (OpenMP facet loop, as the reference runs it)."""
+    import os
+    rng = np.random.default_rng(1)
+    th = abt_b200.make_angles([0, 180], [1])
+    ph = abt_b200.make_angles([0, 358], [2])
+    geo = W.hex_prism(5.0, 10.0, n_side=7, n_len=14)
+    R = W.euler_rotation(*np.radians([30, 40, 10]))
+    V, beam, ext, _ = W.standin_orientation(geo, R, rng, n_internal=(0, 3))
+    g2 = dict(geo, verts=V)
+    afb, afe = ctx.diff_main(beam, ext, g2, th, ph, LAM)
+    rfb, rfe = O.diff_main(th, ph, LAM, g2, beam, ext, nthreads=os.cpu_count() or 1)
+    assert rel_err(afb, rfb) <= TOL_AMPL
+    assert rel_err(afe, rfe) <= TOL_AMPL
