@@ -66,7 +66,8 @@ struct __align__(16) K2Pair {
     float2 hkz_cf, hicf, hkxky_cf;
     float2 inc[3];
     float2 vx[3], vy[3];
-    float2 amp[8];
+    float2 amp[8];   // the amplitude columns in the circular basis: u+_1, u-_1, u+_2, u-_2
+                     // (u+- = a1c +- i a2c of K2Rec::amp), re/im
 };
 static_assert(sizeof(K2Pair) == 352, "K2Pair must be 352 bytes");
 

@@ -227,14 +227,22 @@ __global__ void k2_setup_kernel(RefSrc S, int64_t nrefs, const double *__restric
         rec.hkz_cf = (float)(-0.5 * fr.prop2[2] * cf);
         rec.hicf = (float)(0.5 / cf);
         rec.hkxky_cf = (float)(0.5 * fr.prop2[0] * Ky * cf);
+        double am[8];  // (2 i A / lambda) sign ampl: (1,1),(2,1),(1,2),(2,2) re/im
         for (int q = 0; q < 4; q++) {
-            rec.amp[2 * q] = (float)(-cpre * ob->ampl[2 * q + 1]);
-            rec.amp[2 * q + 1] = (float)(cpre * ob->ampl[2 * q]);
+            am[2 * q] = -cpre * ob->ampl[2 * q + 1];
+            am[2 * q + 1] = cpre * ob->ampl[2 * q];
         }
-        if (pairs)
+        for (int q = 0; q < 8; q++) rec.amp[q] = (float)am[q];
+        if (pairs) {
+            // the packed kernel works on the columns in the circular basis
+            // u+ = a1c + i a2c, u- = a1c - i a2c (formed in FP64)
+            const double uc[8] = {am[0] - am[3], am[1] + am[2], am[0] + am[3], am[1] - am[2],
+                                  am[4] - am[7], am[5] + am[6], am[4] + am[7], am[5] - am[6]};
+            for (int q = 0; q < 8; q++) rec.amp[q] = (float)uc[q];
             store_pair_half(pairs, r0 + t, rec);
-        else
+        } else {
             recs[r0 + t] = rec;
+        }
         if (fast_diff) {
             K2Fov fv;
             const double fov = kind ? kPiRef / 2.0 : ob->fov;
@@ -844,28 +852,25 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     }
     const float2 A = fma2(p, d, mul2(rr, e));
     const float2 Bc = fma2(p, e, neg2(mul2(rr, d)));
-    const float2 nB = neg2(Bc);
-    float2 G[8];
-    G[0] = fma2(A, P.amp[0], mul2(Bc, P.amp[2]));
-    G[1] = fma2(A, P.amp[1], mul2(Bc, P.amp[3]));
-    G[2] = fma2(A, P.amp[2], mul2(nB, P.amp[0]));
-    G[3] = fma2(A, P.amp[3], mul2(nB, P.amp[1]));
-    G[4] = fma2(A, P.amp[4], mul2(Bc, P.amp[6]));
-    G[5] = fma2(A, P.amp[5], mul2(Bc, P.amp[7]));
-    G[6] = fma2(A, P.amp[6], mul2(nB, P.amp[4]));
-    G[7] = fma2(A, P.amp[7], mul2(nB, P.amp[5]));
+    // [[A, B], [-B, A]] is diagonal in the circular basis: with z = A - iB the
+    // columns' u+ take z, their u- take conj(z).  q+ = g z, q- = g conj(z).
+    const float2 gyB = mul2(gy, Bc), gxB = mul2(gx, Bc);
+    float2 qpr = fma2(gx, A, gyB), qmr = fma2(gx, A, neg2(gyB));
+    float2 qpi = fma2(gy, A, neg2(gxB)), qmi = fma2(gy, A, gxB);
     if (FAST || !lo_ok || !hi_ok) {
         // a lane outside the item or outside the field of view adds nothing
-        gx = sel2(ok_x, ok_y, gx, bc2(0.0f));
-        gy = sel2(ok_x, ok_y, gy, bc2(0.0f));
-#pragma unroll
-        for (int c = 0; c < 8; c++) G[c] = sel2(ok_x, ok_y, G[c], bc2(0.0f));
+        qpr = sel2(ok_x, ok_y, qpr, bc2(0.0f));
+        qmr = sel2(ok_x, ok_y, qmr, bc2(0.0f));
+        qpi = sel2(ok_x, ok_y, qpi, bc2(0.0f));
+        qmi = sel2(ok_x, ok_y, qmi, bc2(0.0f));
     }
-    const float2 ngy = neg2(gy);
+    // acc: (U+ col 1, U- col 1, U+ col 2, U- col 2), re/im
 #pragma unroll
     for (int c = 0; c < 4; c++) {
-        acc[2 * c] = fma2(gx, G[2 * c], fma2(ngy, G[2 * c + 1], acc[2 * c]));
-        acc[2 * c + 1] = fma2(gx, G[2 * c + 1], fma2(gy, G[2 * c], acc[2 * c + 1]));
+        const float2 qr = (c & 1) ? qmr : qpr, qi = (c & 1) ? qmi : qpi;
+        const float2 ur = P.amp[2 * c], ui = P.amp[2 * c + 1];
+        acc[2 * c] = fma2(qr, ur, fma2(neg2(qi), ui, acc[2 * c]));
+        acc[2 * c + 1] = fma2(qr, ui, fma2(qi, ur, acc[2 * c + 1]));
     }
 }
 
@@ -1060,9 +1065,16 @@ __global__ void __launch_bounds__(K2_THREADS, (BPT == 1 && FAST) ? 4 : 0) k2_mai
         float *out = P.ws + seg * 8 * P.nb;
 #pragma unroll
         for (int q = 0; q < BPT; q++)
-            if (valid[q])
+            if (valid[q]) {
+                // back from the circular basis: a1 = (U+ + U-)/2, a2 = -i (U+ - U-)/2
+                const double *u = acc64[q];
+                const double lin[8] = {0.5 * (u[0] + u[2]), 0.5 * (u[1] + u[3]),
+                                       0.5 * (u[1] - u[3]), 0.5 * (u[2] - u[0]),
+                                       0.5 * (u[4] + u[6]), 0.5 * (u[5] + u[7]),
+                                       0.5 * (u[5] - u[7]), 0.5 * (u[6] - u[4])};
 #pragma unroll
-                for (int cc = 0; cc < 8; cc++) atomicAdd(out + cc * P.nb + bin[q], (float)acc64[q][cc]);
+                for (int cc = 0; cc < 8; cc++) atomicAdd(out + cc * P.nb + bin[q], (float)lin[cc]);
+            }
     }
 }
 
