@@ -383,7 +383,7 @@ def cpu_baseline(geo, beam, th, ph, seconds, nthreads):
     t0 = time.perf_counter()
     O.diff_main(th, ph, LAM, geo, beam[:n2], ext, nthreads=nthreads)
     dt = time.perf_counter() - t0
-    return {"value": n2 * nb / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+    return {"value": n2 * nb / dt, "unit": UNIT, "cores": O.openmp_threads(nthreads), "kind": "port",
             "sample": "%d facets x %d bins (first facets of the workload), %.1f s" % (n2, nb, dt)}
 
 

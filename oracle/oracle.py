@@ -48,6 +48,8 @@ def lib():
         L.oracle_make_angles.restype = I64
         L.oracle_make_angles.argtypes = [P, P, I64, P, I64]
         L.oracle_deg_to_rad.argtypes = [P, I64]
+        L.oracle_openmp.restype = ctypes.c_int
+        L.oracle_openmp.argtypes = []
         L.oracle_simpne.restype = D
         L.oracle_simpne.argtypes = [I64, P, P, I64]
         L.oracle_diff_main_flat.restype = ctypes.c_int
@@ -96,6 +98,12 @@ def _geom(geometry):
     fo = np.ascontiguousarray(geometry["face_off"], dtype=np.int64)
     fv = np.ascontiguousarray(geometry["face_vi"], dtype=np.int64)
     return v, fo, fv
+
+
+def openmp_threads(nthreads):
+    """Threads oracle_diff_main_omp really uses for a request of nthreads:
+    nthreads when the library was built with OpenMP, else 1."""
+    return nthreads if lib().oracle_openmp() else 1
 
 
 def diff_main(theta, phi, lam, geometry, beam, ext, is_fast_diff=False, nthreads=0):

@@ -464,6 +464,16 @@ int oracle_diff_main(const or_grid *g, const or_geom *geo,
     return rc;
 }
 
+/* 1 when the library was compiled with OpenMP (the threaded loop below runs
+ * on nthreads threads), 0 when it was compiled without (one thread). */
+int oracle_openmp(void) {
+#ifdef _OPENMP
+    return 1;
+#else
+    return 0;
+#endif
+}
+
 /* The reference's multithreaded loop shape (src/diff_mod.f90:739-816):
  * OpenMP worksharing over outbeams, each thread computing one outbeam's full
  * grid and adding it under a critical section.  Used only as the timed CPU
