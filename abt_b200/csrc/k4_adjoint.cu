@@ -58,11 +58,14 @@ enum {
 };
 
 // packed accumulator pairs: (TKX_j, TKY_j) and (WU_i0, WU_i1)
-enum { P_TK = 0, P_WU01 = 3, K4_NPAIR = 6 };
+// and the two Karczewski-Wolf bin sums (sum ee_bar s, sum X) that the
+// record's constants scale into A_P2 at the end
+enum { P_TK = 0, P_WU01 = 3, P_KW = 6, K4_NPAIR = 7 };
 
 struct K4Rec {
     double kc[3];
     float eps[3], b, R[9], ea[3], kp[2], p2[3], cf, icf, inc[3], xa[3], ya[3], amp[8];
+    float kw1, kw2, hicf;  // -p2z cf / 2, p2x p2y cf / 2, icf / 2
 };
 
 // Per-bin input in HBM: the unit bin direction in FP64, 32 B (two 16-byte
@@ -76,13 +79,15 @@ struct Bin4 {
     double ux, uy, uz;
     float fx, fy, fz;
     int64_t o;     // bin index
-    float2 G[4];   // cotangent of S' (pre-T, common phase removed) for the record's kind
+    float2 G[4];   // cotangent of S' (pre-T, common phase removed) for the record's kind,
+                   // circular basis of the columns: H+_1, H-_1, H+_2, H-_2
     float2 Gm[4];  // -i G
 };
 
 __device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 
 __device__ __forceinline__ float rcp4(float x) {
@@ -91,23 +96,27 @@ __device__ __forceinline__ float rcp4(float x) {
     return r;
 }
 
-// sinc(h) and sinc'(h) for h >= 0, branch-free: series below 0.5, else
-// sin(h)/h and (cos h - sinc h)/h with rh = 1/max(h, 0.5).
-__device__ __forceinline__ void sinc_d(float h, float rh, float &sc, float &dsc) {
-    const float h2 = h * h;
-    const float ps = fmaf(h2, fmaf(h2, fmaf(h2, fmaf(h2, 2.7557319e-6f, -1.9841270e-4f), 8.3333333e-3f),
-                                   -1.6666667e-1f),
-                          1.0f);
-    // d/dh (sin h / h) = -h/3 + h^3/30 - h^5/840 + h^7/45360
-    const float pd = h * fmaf(h2, fmaf(h2, fmaf(h2, 2.2045855e-5f, -1.1904762e-3f), 3.3333333e-2f),
-                              -0.33333333f);
+// sinc(h) and sinc'(h) for h >= 0: series below 0.5, else sin(h)/h and
+// (cos h - sinc h)/h with rh = 1/max(h, 0.5).  series (warp-uniform) is false
+// when no lane of the warp has an argument below 0.5; the polynomials are
+// then skipped.
+__device__ __forceinline__ void sinc_d(float h, float rh, bool series, float &sc, float &dsc) {
     float s, c;
     __sincosf(h, &s, &c);
-    const float qs = s * rh;
-    const float qd = (c - qs) * rh;
-    const bool small = h < 0.5f;
-    sc = small ? ps : qs;
-    dsc = small ? pd : qd;
+    sc = s * rh;
+    dsc = (c - sc) * rh;
+    if (series) {
+        const float h2 = h * h;
+        const float ps = fmaf(
+            h2, fmaf(h2, fmaf(h2, fmaf(h2, 2.7557319e-6f, -1.9841270e-4f), 8.3333333e-3f), -1.6666667e-1f),
+            1.0f);
+        // d/dh (sin h / h) = -h/3 + h^3/30 - h^5/840 + h^7/45360
+        const float pd =
+            h * fmaf(h2, fmaf(h2, fmaf(h2, 2.2045855e-5f, -1.1904762e-3f), 3.3333333e-2f), -0.33333333f);
+        const bool small = h < 0.5f;
+        sc = small ? ps : sc;
+        dsc = small ? pd : dsc;
+    }
 }
 
 // g = second divided difference of e^{ix} at t0, t1, t2, and dg/dlo, dg/dhi
@@ -129,8 +138,10 @@ __device__ __forceinline__ void dd_grad(float t0, float t1, float t2, float2 &g,
         const float r = rcp4(p12 * Dg);
         const float rD = Dg * r, iD = p12 * r;
         float sc1, dsc1, sc2, dsc2;
-        sinc_d(h1, a2 * rD, sc1, dsc1);
-        sinc_d(h2, a1 * rD, sc2, dsc2);
+        // the lanes that reach here vote; a lane that needs the series is among them
+        const bool series = __any_sync(__activemask(), fminf(h1, h2) < 0.5f);
+        sinc_d(h1, a2 * rD, series, sc1, dsc1);
+        sinc_d(h2, a1 * rD, series, sc2, dsc2);
         // E = i e^{ic} sinc(h) = sc n with n = i e^{ic} = (-s, c); dE/dc = i E = sc (i n),
         // i n = (-c, -s); dE/dh = dsc n.  g = (E2 - E1) / D,
         // dg/dlo = (g - (iE1 - H1)/2) / D, dg/dhi = ((iE2 + H2)/2 - g) / D
@@ -231,7 +242,6 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     for (int j = 0; j < 3; j++) t[j] = fmaf(kyy, r.ya[j], fmaf(kxx, r.xa[j], ph));
     float2 g, dlo, dhi;
     dd_grad(t[0], t[1], t[2], g, dlo, dhi);
-    const float Kx = r.p2[0], Ky = r.p2[1], Kz = r.p2[2], cf = r.cf, rcf = r.icf;
     const bool yclamp = !(fabsf(ky) <= 0.999999f);
     const float kyc = fminf(fmaxf(ky, -0.999999f), 0.999999f);
     const float traw = fmaf(kx, kx, kz * kz);
@@ -240,8 +250,10 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const float rs = rsqrtf(tt), s = tt * rs;
     const float kyrs = kyc * rs;
     const float m[3] = {-kx * kyrs, s, -kz * kyrs};
-    const float dd = fmaf(-0.5f * Kz * cf, s, -0.5f * kz * rs * rcf);
-    const float ee = fmaf(0.5f * Kx * Ky * cf, s, -0.5f * kx * kyc * rs * rcf);
+    // dd = -Kz cf s / 2 - kz icf / (2 s), ee = Kx Ky cf s / 2 - kx ky icf / (2 s)
+    const float e = rs * r.hicf, kxkyc = kx * kyc;
+    const float dd = fmaf(r.kw1, s, -kz * e);
+    const float ee = fmaf(r.kw2, s, -kxkyc * e);
     const float kc3[3] = {kx, kyc, kz};
     const float dinc = fmaf(r.inc[2], kz, fmaf(r.inc[1], kyc, r.inc[0] * kx));
     const bool bodge = !(fabsf(dinc) < 0.999f);
@@ -282,33 +294,32 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
         rr = fmaf(hc[2], ev[2], fmaf(hc[1], ev[1], hc[0] * ev[0]));
     }
     const float A = fmaf(pp, dd, rr * ee), Bm = fmaf(pp, ee, -rr * dd);
-    // W = [[A, B], [-B, A]] amp' ; complex order (1,1),(2,1),(1,2),(2,2)
-    const float2 *a = reinterpret_cast<const float2 *>(r.amp);
-    const float2 A2 = bc2(A), B2 = bc2(Bm), nB2 = bc2(-Bm);
-    float2 W[4];
-    W[0] = fma2(A2, a[0], mul2(B2, a[1]));
-    W[1] = fma2(A2, a[1], mul2(nB2, a[0]));
-    W[2] = fma2(A2, a[2], mul2(B2, a[3]));
-    W[3] = fma2(A2, a[3], mul2(nB2, a[2]));
-    // backward.  C = g W:  g_bar = sum G conj(W) = sum (Re W) G + (Im W)(-i G),
-    // W_bar = G conj(g) = (Re g) G + (Im g)(-i G)
-    float2 gb = make_float2(0, 0);
-    float2 Wb[4];
-    const float2 gx2 = bc2(g.x), gy2 = bc2(g.y);
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-        gb = fma2(bc2(W[c].x), B.G[c], fma2(bc2(W[c].y), B.Gm[c], gb));
-        Wb[c] = fma2(gx2, B.G[c], mul2(gy2, B.Gm[c]));
+    // W = [[A, B], [-B, A]] amp' is diagonal in the circular basis:
+    // W1j +- i W2j = z+- u+-_j with z+ = A - iB, z- = A + iB.  With the cotangent
+    // H+-_j of the same basis and S+- = sum_j H+-_j conj(u+-_j):
+    //   g_bar = conj(z+) S+ + conj(z-) S- = A (S+ + S-) + i B (S+ - S-)
+    //   A_bar = Re conj(g) (S+ + S-),  B_bar = Im conj(g) (S- - S+)
+    //   u+-_j_bar = H+-_j conj(g z+-)
+    const float2 *u = reinterpret_cast<const float2 *>(r.amp);
+    // H conj(u) = Re(u) H + Im(u) (-i H)
+    const float2 Sp = fma2(bc2(u[0].x), B.G[0], fma2(bc2(u[0].y), B.Gm[0],
+                           fma2(bc2(u[2].x), B.G[2], mul2(bc2(u[2].y), B.Gm[2]))));
+    const float2 Sn = fma2(bc2(u[1].x), B.G[1], fma2(bc2(u[1].y), B.Gm[1],
+                           fma2(bc2(u[3].x), B.G[3], mul2(bc2(u[3].y), B.Gm[3]))));
+    const float2 Ss = add2(Sp, Sn), Sd = sub2(Sp, Sn);
+    const float2 gb = make_float2(fmaf(A, Ss.x, -Bm * Sd.y), fmaf(A, Ss.y, Bm * Sd.x));
+    const float Ab = fmaf(g.x, Ss.x, g.y * Ss.y);
+    const float Bb = fmaf(g.y, Sd.x, -g.x * Sd.y);
+    {
+        const float gyB = g.y * Bm, gyA = g.y * A;
+        // conj(g z+) and conj(g z-); H w = Re(w) H - Im(w) (-i H)
+        const float wpr = fmaf(g.x, A, gyB), wpi = fmaf(g.x, Bm, -gyA);
+        const float wnr = fmaf(g.x, A, -gyB), wni = fmaf(-g.x, Bm, -gyA);
+        accA[0] = fma2(bc2(wpr), B.G[0], fma2(bc2(-wpi), B.Gm[0], accA[0]));
+        accA[1] = fma2(bc2(wnr), B.G[1], fma2(bc2(-wni), B.Gm[1], accA[1]));
+        accA[2] = fma2(bc2(wpr), B.G[2], fma2(bc2(-wpi), B.Gm[2], accA[2]));
+        accA[3] = fma2(bc2(wnr), B.G[3], fma2(bc2(-wni), B.Gm[3], accA[3]));
     }
-    // A_bar = Re sum conj(W_bar) dW/dA, B_bar likewise ; amp'_bar = M^T W_bar
-    const float2 pa = fma2(Wb[0], a[0], fma2(Wb[1], a[1], fma2(Wb[2], a[2], mul2(Wb[3], a[3]))));
-    const float2 pb = sub2(fma2(Wb[0], a[1], mul2(Wb[2], a[3])), fma2(Wb[1], a[0], mul2(Wb[3], a[2])));
-    const float Ab = pa.x + pa.y;
-    const float Bb = pb.x + pb.y;
-    accA[0] = fma2(A2, Wb[0], fma2(nB2, Wb[1], accA[0]));
-    accA[1] = fma2(B2, Wb[0], fma2(A2, Wb[1], accA[1]));
-    accA[2] = fma2(A2, Wb[2], fma2(nB2, Wb[3], accA[2]));
-    accA[3] = fma2(B2, Wb[2], fma2(A2, Wb[3], accA[3]));
     // A = pp dd + rr ee, B = pp ee - rr dd
     const float ppb = fmaf(Ab, dd, Bb * ee), rrb = fmaf(Ab, ee, -Bb * dd);
     const float ddb = fmaf(Ab, pp, -Bb * rr), eeb = fmaf(Ab, rr, Bb * pp);
@@ -372,18 +383,21 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
         kycb += qb[1];
         kzb += qb[2];
     }
-    // Karczewski-Wolf dd, ee as above
-    kxb += eeb * (-0.5f * kyrs * rcf);
-    kycb += eeb * (-0.5f * kx * rs * rcf);
-    kzb += ddb * (-0.5f * rs * rcf);
-    const float rs2 = rs * rs;
-    const float sb = sbm + ddb * fmaf(-0.5f * Kz, cf, 0.5f * kz * rs2 * rcf) +
-                     eeb * fmaf(0.5f * Kx * Ky, cf, 0.5f * kx * kyc * rs2 * rcf);
-    const float cfb = ddb * fmaf(-0.5f * Kz, s, 0.5f * kz * rs * rcf * rcf) +
-                      eeb * fmaf(0.5f * Kx * Ky, s, 0.5f * kx * kyc * rs * rcf * rcf);
-    acc[A_P2 + 2] += ddb * (-0.5f * cf * s);
-    acc[A_P2 + 0] += eeb * (0.5f * Ky * cf * s);
-    acc[A_P2 + 1] += eeb * (0.5f * Kx * cf * s) + cfb * Ky * cf * cf * cf;
+    // Karczewski-Wolf dd, ee as above.  With X = (dd_bar kz + ee_bar kx ky) e:
+    //   s_bar += kw1 dd_bar + kw2 ee_bar + X / s
+    //   p2_bar: z -cf/2 dd_bar s, x Ky cf/2 ee_bar s,
+    //           y Kx cf/2 ee_bar s + Ky cf^2 (kw1 dd_bar s + kw2 ee_bar s + X)
+    // (cf = 1/sqrt(1 - Ky^2)); the bin sums of dd_bar s, ee_bar s and X are
+    // scaled by the record's constants after the loop.
+    const float dde = ddb * e, eee = eeb * e;
+    kxb = fmaf(-eee, kyc, kxb);
+    kycb = fmaf(-eee, kx, kycb);
+    kzb -= dde;
+    const float X = fmaf(dde, kz, eee * kxkyc);
+    const float sb = sbm + fmaf(ddb, r.kw1, fmaf(eeb, r.kw2, rs * X));
+    acc[A_P2 + 2] = fmaf(ddb, s, acc[A_P2 + 2]);
+    accP[P_KW].x = fmaf(eeb, s, accP[P_KW].x);
+    accP[P_KW].y += X;
     if (!floored) {
         const float ttb = 0.5f * sb * rs;  // s = sqrt(tt)
         kxb = fmaf(2.0f * kx, ttb, kxb);
@@ -395,13 +409,15 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const float tlo = fmaf(gb.x, dlo.x, gb.y * dlo.y), thi = fmaf(gb.x, dhi.x, gb.y * dhi.y);
     const float phb = fmaf(gb.y, g.x, -gb.x * g.y);
     const float tmid = phb - tlo - thi;
-    const int rk[3] = {(t[1] < t[0]) + (t[2] < t[0]), (t[0] <= t[1]) + (t[2] < t[1]),
-                       (t[0] <= t[2]) + (t[1] <= t[2])};
+    // rank 0 (lowest) / 2 (highest) of each t_j, ties broken by index
+    const bool c01 = t[1] < t[0], c02 = t[2] < t[0], c12 = t[2] < t[1];
+    const bool is_lo[3] = {!c01 && !c02, c01 && !c12, c02 && c12};
+    const bool is_hi[3] = {c01 && c02, !c01 && c12, !c02 && !c12};
     float kxxb = 0.0f, kyyb = 0.0f;
     const float2 kk2 = make_float2(kxx, kyy);
 #pragma unroll
     for (int j = 0; j < 3; j++) {
-        const float tb = rk[j] == 0 ? tlo : (rk[j] == 1 ? tmid : thi);
+        const float tb = is_lo[j] ? tlo : (is_hi[j] ? thi : tmid);
         kxxb = fmaf(tb, r.xa[j], kxxb);
         kyyb = fmaf(tb, r.ya[j], kyyb);
         accP[P_TK + j] = fma2(bc2(tb), kk2, accP[P_TK + j]);
@@ -409,8 +425,8 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     // kxx = k p2x - k kx ; kyy = k p2y - k ky
     kxb = fmaf(-k, kxxb, kxb);
     kyb = fmaf(-k, kyyb, kyb);
-    acc[A_P2 + 0] = fmaf(k, kxxb, acc[A_P2 + 0]);
-    acc[A_P2 + 1] = fmaf(k, kyyb, acc[A_P2 + 1]);
+    acc[A_P2 + 0] += kxxb;  // times k after the loop
+    acc[A_P2 + 1] += kyyb;
     const float kb3[3] = {kxb, kyb, kzb};
     float ab, bb;
     dir4_back(r, d, kb3, B.fx, B.fy, B.fz, acc, accP, ab, bb);
@@ -486,10 +502,15 @@ __global__ void __launch_bounds__(K4_WARPS * 32, MINB) k4_adjoint_kernel(
         for (int c = 0; c < 4; c++) B.Gm[c] = make_float2(B.G[c].y, -B.G[c].x);
         k4_eval<FAST>(r, B, k, hkR, iRf, cosfov, p0, bins, nphi, theta_i, acc, accA, accP);
     }
+    // amplitude sums back from the circular basis: a1j_bar = u+_j_bar + u-_j_bar,
+    // a2j_bar = i (u-_j_bar - u+_j_bar)
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        acc[A_AMP + 2 * q] = accA[q].x;
-        acc[A_AMP + 2 * q + 1] = accA[q].y;
+    for (int j = 0; j < 2; j++) {
+        const float2 up = accA[2 * j], un = accA[2 * j + 1];
+        acc[A_AMP + 4 * j] = up.x + un.x;
+        acc[A_AMP + 4 * j + 1] = up.y + un.y;
+        acc[A_AMP + 4 * j + 2] = up.y - un.y;
+        acc[A_AMP + 4 * j + 3] = un.x - up.x;
     }
 #pragma unroll
     for (int j = 0; j < 3; j++) {
@@ -497,6 +518,15 @@ __global__ void __launch_bounds__(K4_WARPS * 32, MINB) k4_adjoint_kernel(
         acc[A_TKY + j] = accP[P_TK + j].y;
         acc[A_WU + 3 * j] += accP[P_WU01 + j].x;
         acc[A_WU + 3 * j + 1] += accP[P_WU01 + j].y;
+    }
+    {
+        // A_P2 held (sum kxx_bar, sum kyy_bar, sum dd_bar s) and P_KW (sum ee_bar s, sum X)
+        const float cf = r.cf, Kx = r.p2[0], Ky = r.p2[1];
+        const float q1 = acc[A_P2 + 2], q2 = accP[P_KW].x, q3 = accP[P_KW].y;
+        acc[A_P2 + 0] = fmaf(k, acc[A_P2 + 0], 0.5f * Ky * cf * q2);
+        acc[A_P2 + 1] = fmaf(k, acc[A_P2 + 1],
+                             fmaf(0.5f * Kx * cf, q2, Ky * cf * cf * fmaf(r.kw1, q1, fmaf(r.kw2, q2, q3))));
+        acc[A_P2 + 2] = -0.5f * cf * q1;
     }
 #pragma unroll
     for (int q = 0; q < K4_NACC; q++) {
@@ -541,9 +571,12 @@ __global__ void k4_prep_kernel(const double *__restrict__ gafb, const double *__
         const double o21r = gr[1] * T11 + gr[3] * T12, o21i = gi[1] * T11 + gi[3] * T12;
         const double o12r = gr[0] * T21 + gr[2] * T22, o12i = gi[0] * T21 + gi[2] * T22;
         const double o22r = gr[1] * T21 + gr[3] * T22, o22i = gi[1] * T21 + gi[3] * T22;
+        // in the circular basis of the columns: H+-_j = (G1j +- i G2j) / 2
         float4 *dst = gbin + (kd * nb + o) * 2;
-        dst[0] = make_float4((float)o11r, (float)o11i, (float)o21r, (float)o21i);
-        dst[1] = make_float4((float)o12r, (float)o12i, (float)o22r, (float)o22i);
+        dst[0] = make_float4((float)(0.5 * (o11r - o21i)), (float)(0.5 * (o11i + o21r)),
+                             (float)(0.5 * (o11r + o21i)), (float)(0.5 * (o11i - o21r)));
+        dst[1] = make_float4((float)(0.5 * (o12r - o22i)), (float)(0.5 * (o12i + o22r)),
+                             (float)(0.5 * (o12r + o22i)), (float)(0.5 * (o12i - o22r)));
     }
 }
 
@@ -626,9 +659,24 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
         r.kp[1] = (float)(k * fr.prop2[1]);
         r.cf = (float)(1.0 / sqrt(1.0 - fr.prop2[1] * fr.prop2[1]));
         r.icf = (float)sqrt(1.0 - fr.prop2[1] * fr.prop2[1]);
-        for (int c = 0; c < 4; c++) {
-            r.amp[2 * c] = (float)(-cpre * ob.ampl[2 * c + 1]);
-            r.amp[2 * c + 1] = (float)(cpre * ob.ampl[2 * c]);
+        {
+            const double cfd = 1.0 / sqrt(1.0 - fr.prop2[1] * fr.prop2[1]);
+            r.kw1 = (float)(-0.5 * fr.prop2[2] * cfd);
+            r.kw2 = (float)(0.5 * fr.prop2[0] * fr.prop2[1] * cfd);
+            r.hicf = (float)(0.5 * sqrt(1.0 - fr.prop2[1] * fr.prop2[1]));
+        }
+        {
+            // amp' = (2 i A / lambda) sign ampl in the order (1,1),(2,1),(1,2),(2,2),
+            // stored as the columns in the circular basis u+-_j = a1j +- i a2j:
+            // u+_1, u-_1, u+_2, u-_2
+            double am[8];
+            for (int c = 0; c < 4; c++) {
+                am[2 * c] = -cpre * ob.ampl[2 * c + 1];
+                am[2 * c + 1] = cpre * ob.ampl[2 * c];
+            }
+            const double uc[8] = {am[0] - am[3], am[1] + am[2], am[0] + am[3], am[1] - am[2],
+                                  am[4] - am[7], am[5] + am[6], am[4] + am[7], am[5] - am[6]};
+            for (int c = 0; c < 8; c++) r.amp[c] = (float)uc[c];
         }
         h.As = As;
         h.sign = fr.sign;
