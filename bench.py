@@ -190,6 +190,8 @@ def orientation_average(ctx, args):
     k32_ms, k32_n = ctx.kernel_time_ms()
     # FP32 and FP64 on the first k orientations
     f32 = ctx.diff_batch(beams[:k], exts[:k], Vs[:k], geo, th, ph, LAM, pin[:k], precision="fp32")
+    # one untimed FP64 orientation first: the steady state of a per-orientation loop
+    ctx.diff_batch(beams[:1], exts[:1], Vs[:1], geo, th, ph, LAM, pin[:1], precision="fp64")
     ctx.kernel_time_ms()
     t0 = time.perf_counter()
     f64 = ctx.diff_batch(beams[:k], exts[:k], Vs[:k], geo, th, ph, LAM, pin[:k], precision="fp64")
