@@ -202,27 +202,57 @@ def facet_normals_areas(verts, face_off, face_vi):
     return n / (2 * a[:, None]), a
 
 
-def standin_orientation(geometry, R, rng, lam=LAMBDA, n_internal=(0, 6), rbi=1.31):
-    """A beam list standing in for one orientation of the tracer: the particle
-    rotated by R, lit from +z along (0,0,-1).  External diffraction: one
-    outbeam per lit facet along the incidence direction (as
-    src/beam_loop_mod.f90:602-608 emits them).  Beam outbeams: every facet
-    emits 0..n reflected/refracted outgoing beams with Fresnel-like scalar
-    amplitudes (uneven counts per orientation, like the tracer's output).
-    Returns (rotated vertices, beam, ext, params_in record)."""
-    V = geometry["verts"] @ R.T
-    fo, fv = geometry["face_off"], geometry["face_vi"]
-    nrm, area = facet_normals_areas(V, fo, fv)
+def ext_diffraction_outbeams(V, face_off, face_vi, lam=LAMBDA):
+    """The external-diffraction outbeams the tracer emits for an incident beam
+    along (0,0,-1): one per lit facet, prop_out = prop_in = the incidence
+    direction, vk7 = normalise(n x prop), and ampl = the incident field
+    (identity, e-perp (1,0,0); src/input_mod.f90:2241-2258) times the path
+    phase exp(i k dist), dist = the incident plane's z minus the facet
+    centroid's z (src/beam_loop_mod.f90:2602, :530), rotated from the incident
+    e-perp into vk7 by the normalised rotation of get_rot_matrix
+    (src/beam_loop_mod.f90:525-533, :2611-2638).  The incident plane is put at
+    the highest vertex; another choice changes every outbeam by one common
+    phase.  Returns (ext outbeams, lit facet indices, cos of incidence)."""
+    nrm, area = facet_normals_areas(V, face_off, face_vi)
     inc = np.array([0.0, 0.0, -1.0])
     cosi = -(nrm @ inc)
     lit = np.nonzero(cosi > 1e-6)[0]
     ext = np.zeros(len(lit), dtype=OUTBEAM_DTYPE)
     ext["fi"] = lit + 1
     ext["prop_out"] = inc
-    ext["vk7"] = np.array([0.0, 1.0, 0.0])
-    # external diffraction amplitude: the unit incident field
-    ext["ampl"] = np.array([1.0, 0, 0, 0, 0, 0, 1.0, 0])
+    vk7 = np.cross(nrm[lit], inc)
+    vn = np.linalg.norm(vk7, axis=1)
+    e1 = np.array([1.0, 0.0, 0.0])
+    # a facet facing the incidence head-on has no scattering plane of its own
+    vk7 = np.where(vn[:, None] > 1e-12, vk7 / np.maximum(vn, 1e-300)[:, None], e1)
+    ext["vk7"] = vk7
+    evo2 = np.cross(inc, e1)
+    c = vk7 @ e1
+    s = vk7 @ evo2
+    nrm_rot = np.sqrt(np.abs(c * c + s * s))
+    r11, r12, r21, r22 = c / nrm_rot, -s / nrm_rot, s / nrm_rot, c / nrm_rot
+    mid_z = V[face_vi - 1].reshape(-1, 3, 3)[lit, :, 2].mean(axis=1)
+    k = 2.0 * float(np.float32(np.pi)) / lam
+    ph = np.exp(1j * k * (V[:, 2].max() - mid_z))
+    amp = np.stack([r11 * ph, r21 * ph, r12 * ph, r22 * ph], axis=1)  # (1,1),(2,1),(1,2),(2,2)
+    ext["ampl"][:, 0::2] = amp.real
+    ext["ampl"][:, 1::2] = amp.imag
     ext["fov"] = np.pi / 2
+    return ext, lit, cosi
+
+
+def standin_orientation(geometry, R, rng, lam=LAMBDA, n_internal=(0, 6), rbi=1.31):
+    """A beam list standing in for one orientation of the tracer: the particle
+    rotated by R, lit from +z along (0,0,-1).  External diffraction: one
+    outbeam per lit facet along the incidence direction, built as the tracer
+    builds them (ext_diffraction_outbeams).  Beam outbeams: every facet
+    emits 0..n reflected/refracted outgoing beams with Fresnel-like scalar
+    amplitudes (uneven counts per orientation, like the tracer's output).
+    Returns (rotated vertices, beam, ext, params_in record)."""
+    V = geometry["verts"] @ R.T
+    fo, fv = geometry["face_off"], geometry["face_vi"]
+    nrm, area = facet_normals_areas(V, fo, fv)
+    ext, lit, cosi = ext_diffraction_outbeams(V, fo, fv, lam)
     # outgoing beams: per facet a random number of outgoing directions
     nf = len(area)
     counts = rng.integers(n_internal[0], n_internal[1] + 1, size=nf)

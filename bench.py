@@ -183,11 +183,16 @@ def orientation_average(ctx, args):
     # FP32 batched, all orientations (host API: H2D, one persistent launch per chunk, D2H)
     ctx.diff_batch(beams[:2], exts[:2], Vs[:2], geo, th, ph, LAM, pin[:2], precision="fp32")
     ctx.set_kernel_timing(True)
-    ctx.kernel_time_ms()
-    t0 = time.perf_counter()
-    ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp32")
-    t32 = time.perf_counter() - t0
-    k32_ms, k32_n = ctx.kernel_time_ms()
+    # best of two calls: the host side (gather, copies) shares the box's cores
+    t32 = k32_ms = None
+    for _ in range(2):
+        ctx.kernel_time_ms()
+        t0 = time.perf_counter()
+        ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp32")
+        dt = time.perf_counter() - t0
+        kms, k32_n = ctx.kernel_time_ms()
+        if t32 is None or dt < t32:
+            t32, k32_ms = dt, kms
     # FP32 and FP64 on the first k orientations
     f32 = ctx.diff_batch(beams[:k], exts[:k], Vs[:k], geo, th, ph, LAM, pin[:k], precision="fp32")
     # one untimed FP64 orientation first: the steady state of a per-orientation loop
@@ -226,7 +231,8 @@ def large_case(ctx, args):
     10-30 outgoing beams per facet (~460,000 outbeams per orientation), 1441
     theta x 720 phi (1,037,520 bins).  --large-orient orientations are averaged
     by one FP32 batch; the FP64 drop-in rate is sampled on 4,000 facets and
-    the error taken on a 10 % facet sample of the first orientation."""
+    the error is taken on the whole first orientation (FP64 drop-in over all
+    of its outbeams, ~40 s)."""
     import abt_b200
     from abt_b200 import workloads as W
     from tests.helpers import mueller_rel_err
@@ -260,12 +266,10 @@ def large_case(ctx, args):
     k64_ms, _ = ctx.kernel_time_ms()
     ctx.set_kernel_timing(False)
     r64 = len(sub) * nb / (k64_ms / 1e3)
-    # error on a 10 % sample of the first orientation's outbeams
-    sb = beams[0][::10]
-    se = exts[0][::10]
+    # error on the whole first orientation
     g0 = dict(geo, verts=Vs[0])
-    a32 = ctx.diff_main(sb, se, g0, th, ph, LAM, precision="fp32")
-    a64 = ctx.diff_main(sb, se, g0, th, ph, LAM, precision="fp64")
+    a32 = ctx.diff_main(beams[0], exts[0], g0, th, ph, LAM, precision="fp32")
+    a64 = ctx.diff_main(beams[0], exts[0], g0, th, ph, LAM, precision="fp64")
     m32, _, p32 = ctx.finalise(a32[0], a32[1], th, ph, LAM, pin[0])
     m64, _, p64 = ctx.finalise(a64[0], a64[1], th, ph, LAM, pin[0])
     work = float(F.sum()) * nb
@@ -279,8 +283,8 @@ def large_case(ctx, args):
             "fp64_dropin_facet_bin_per_s": r64,
             "fp64_dropin_orientations_per_s_extrapolated": r64 / (float(F.mean()) * nb),
             "speedup_fp32_batched_vs_fp64_dropin": (work / t32) / r64,
-            "max_rel_mueller_err_vs_fp64_10pct_sample": mueller_rel_err(m32, m64, 1e-6),
-            "max_rel_param_err_vs_fp64_10pct_sample": max(
+            "max_rel_mueller_err_vs_fp64_first_orientation": mueller_rel_err(m32, m64, 1e-6),
+            "max_rel_param_err_vs_fp64_first_orientation": max(
                 abs(float(p32[n]) - float(p64[n])) / abs(float(p64[n]))
                 for n in ("scatt", "ext", "asymmetry"))}
 
