@@ -24,7 +24,18 @@ int validate_outbeams(const pbt_outbeam *obs, int64_t n, int64_t nfaces, const c
         set_error("%s: outbeam array is NULL", what);
         return PBT_EINVAL;
     }
-    for (int64_t j = 0; j < n; j++) {
+    // find the first bad record with all host threads, then report it in order
+    auto good = [nfaces](const pbt_outbeam &ob) {
+        bool ok = ob.fi >= 1 && ob.fi <= nfaces && isfinite(ob.fov);
+        for (int q = 0; q < 8; q++) ok = ok && isfinite(ob.ampl[q]);
+        for (int q = 0; q < 3; q++) ok = ok && isfinite(ob.vk7[q]) && isfinite(ob.prop_out[q]);
+        return ok;
+    };
+    int64_t first_bad = n;
+#pragma omp parallel for reduction(min : first_bad) schedule(static) if (n > 65536)
+    for (int64_t j = 0; j < n; j++)
+        if (!good(obs[j])) first_bad = std::min(first_bad, j);
+    for (int64_t j = first_bad; j < n; j++) {
         const pbt_outbeam &ob = obs[j];
         if (ob.fi < 1 || ob.fi > nfaces) {
             set_error("%s outbeam %lld: face index fi=%lld out of range 1..%lld", what,

@@ -69,13 +69,21 @@ int validate_geometry(const double *verts, int64_t nverts, const int64_t *face_o
         }
     }
     int64_t nvi = face_off[nfaces];
+    // the first bad index and coordinate, found with all host threads
+    int64_t bad_vi = nvi, bad_v = 3 * nverts;
+#pragma omp parallel for reduction(min : bad_vi) schedule(static) if (nvi > 65536)
     for (int64_t q = 0; q < nvi; q++)
+        if (face_vi[q] < 1 || face_vi[q] > nverts) bad_vi = std::min(bad_vi, q);
+#pragma omp parallel for reduction(min : bad_v) schedule(static) if (nverts > 20000)
+    for (int64_t q = 0; q < 3 * nverts; q++)
+        if (!isfinite(verts[q])) bad_v = std::min(bad_v, q);
+    for (int64_t q = bad_vi; q < nvi; q++)
         if (face_vi[q] < 1 || face_vi[q] > nverts) {
             set_error("face_vi[%lld] = %lld out of range 1..%lld", (long long)q,
                       (long long)face_vi[q], (long long)nverts);
             return PBT_EINVAL;
         }
-    for (int64_t q = 0; q < 3 * nverts; q++)
+    for (int64_t q = bad_v; q < 3 * nverts; q++)
         if (!isfinite(verts[q])) {
             set_error("vertex coordinate %lld is not finite", (long long)q);
             return PBT_EINVAL;

@@ -246,12 +246,15 @@ class Context:
 
     # ------------------------------------------------------------ batched
     def diff_batch(self, beams, exts, verts_per_orient, geometry, theta, phi, lam,
-                   params_in, is_fast_diff=False, scaling=False, precision="fp32"):
+                   params_in, is_fast_diff=False, scaling=False, precision="fp32", out=None):
         """Orientation average of norient orientations in one call.
 
         beams / exts: lists (one per orientation) of outbeam arrays.
         verts_per_orient: list of (nverts,3) rotated vertex arrays (topology from geometry).
         params_in: PARAMS_DTYPE array of length norient.
+        out: optional (mueller_avg, mueller_1d_avg) arrays to write into, float64
+        of shapes (nphi, ntheta, 16) and (ntheta, 16) in Fortran order (e.g. views
+        of pinned host memory, which the device writes at full speed).
         Returns (mueller_avg, mueller_1d_avg, params_avg, params_per_orient)."""
         norient = len(beams)
         if len(exts) != norient or len(verts_per_orient) != norient:
@@ -268,8 +271,16 @@ class Context:
         theta = np.ascontiguousarray(theta, dtype=np.float64)
         phi = np.ascontiguousarray(phi, dtype=np.float64)
         pin = np.ascontiguousarray(params_in, dtype=PARAMS_DTYPE)
-        mu = np.empty((len(phi), len(theta), 16), order="F")
-        mu1 = np.empty((len(theta), 16), order="F")
+        if out is None:
+            mu = np.empty((len(phi), len(theta), 16), order="F")
+            mu1 = np.empty((len(theta), 16), order="F")
+        else:
+            mu, mu1 = out
+            for a, shape in ((mu, (len(phi), len(theta), 16)), (mu1, (len(theta), 16))):
+                if (not isinstance(a, np.ndarray) or a.dtype != np.float64 or a.shape != shape
+                        or not a.flags.f_contiguous or not a.flags.writeable):
+                    raise ValueError("out arrays must be writeable Fortran-ordered float64 of "
+                                     "shapes (nphi, ntheta, 16) and (ntheta, 16)")
         pav = np.zeros((), dtype=PARAMS_DTYPE)
         pper = np.zeros(norient, dtype=PARAMS_DTYPE)
         VP = ctypes.c_void_p * norient

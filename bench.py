@@ -529,19 +529,31 @@ def main():
     pb = pinned_beam.numpy().view(abt_b200.OUTBEAM_DTYPE)
     pverts = torch.from_numpy(np.asfortranarray(geo["verts"]).copy()).pin_memory().numpy()
     pverts = np.asfortranarray(pverts.reshape(geo["verts"].shape))
-    geo_p = dict(geo, verts=pverts)
+    def pinned_like(a, order="C"):
+        t = torch.empty(a.size, dtype=torch.float64 if a.dtype == np.float64 else torch.int64,
+                        pin_memory=True).numpy()
+        return t.reshape(a.shape, order=order)
+
+    pfo = pinned_like(np.asarray(geo["face_off"], dtype=np.int64))
+    pfo[...] = geo["face_off"]
+    pfv = pinned_like(np.asarray(geo["face_vi"], dtype=np.int64))
+    pfv[...] = geo["face_vi"]
+    geo_p = dict(geo, verts=pverts, face_off=pfo, face_vi=pfv)
+    # the Mueller outputs go to pinned host arrays owned by the caller
+    pmu = pinned_like(np.empty((len(ph), len(th), 16)), order="F")
+    pmu1 = pinned_like(np.empty((len(th), 16)), order="F")
     out = ctx.diff_batch([pb], [np.zeros(0, abt_b200.OUTBEAM_DTYPE)], [pverts], geo_p, th, ph, LAM,
-                         pin, precision="fp32")
+                         pin, precision="fp32", out=(pmu, pmu1))
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         out = ctx.diff_batch([pb], [np.zeros(0, abt_b200.OUTBEAM_DTYPE)], [pverts], geo_p, th, ph,
-                             LAM, pin, precision="fp32")
+                             LAM, pin, precision="fp32", out=(pmu, pmu1))
     e2e_s = (time.perf_counter() - t0) / args.e2e_steps
     h2d = beam.nbytes + geo["verts"].nbytes + geo["face_off"].nbytes + geo["face_vi"].nbytes + pin.nbytes
     d2h = 16 * nb * 8 + 16 * len(th) * 8 + 2 * pin.nbytes
     e2e = {"value": world * work / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3,
-           "api": "pbt_diff_batch_list_c (host pointers, pinned)"}
+           "api": "pbt_diff_batch_list_c (host pointers; inputs and Mueller outputs pinned)"}
 
     # reference-exact FP64 drop-in rate on a facet sample
     if args.fp64_facets > 0:

@@ -148,3 +148,26 @@ def test_contiguous_batch_entry_matches_list_entry(ctx):
         pin.ctypes.data, mu.ctypes.data, m1.ctypes.data, pav.ctypes.data, None))
     assert mueller_rel_err(mu, mu_l) <= 1e-5
     assert abs(float(pav["scatt"]) - float(pav_l["scatt"])) <= 1e-6 * abs(float(pav_l["scatt"]))
+
+
+@pytest.mark.gpu
+def test_batch_writes_into_caller_arrays(ctx):
+    """diff_batch(out=...) writes the Mueller averages into the caller's
+    (here pinned) arrays, with the same values as freshly allocated ones, and
+    refuses arrays of the wrong layout."""
+    import torch
+    geo, Vs, beams, exts, pin = W.rough_column_orientations(3, seed=62, n_side=2, n_len=3,
+                                                            m_range=(0, 3))
+    th, ph = abt_b200.make_angles([0, 180], [5]), abt_b200.make_angles([0, 350], [10])
+    ref = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp32")
+    mu = torch.empty(len(ph) * len(th) * 16, dtype=torch.float64, pin_memory=True).numpy()
+    mu = mu.reshape((len(ph), len(th), 16), order="F")
+    m1 = np.empty((len(th), 16), order="F")
+    got = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp32", out=(mu, m1))
+    assert got[0] is mu and got[1] is m1
+    # same inputs; only the order of the float atomics may differ
+    assert mueller_rel_err(mu, ref[0]) <= 1e-6
+    assert np.allclose(m1, ref[1], rtol=1e-6, atol=0)
+    with pytest.raises(ValueError):
+        ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp32",
+                       out=(np.empty((len(ph), len(th), 16)), m1))
