@@ -126,3 +126,20 @@ def test_ragged_batch_with_empty_orientations(ctx):
     r32 = ctx.diff_batch(beams, exts, Vs, geo, th, ph, 0.532, pin, precision="fp32")
     r64 = ctx.diff_batch(beams, exts, Vs, geo, th, ph, 0.532, pin, precision="fp64")
     assert mueller_rel_err(r32[0], r64[0]) <= 1e-4
+
+
+def test_first_bad_record_of_a_long_list_is_reported(ctx):
+    """Long lists (above 65,536 records) are checked by all host threads; the
+    record reported is still the first bad one, and nothing runs."""
+    th, ph, geo, ob = _inputs()
+    rng = np.random.default_rng(5)
+    many = outbeams(70000, rng, 1)
+    many["fi"][50000] = 9
+    many["ampl"][60000, 3] = np.nan
+    with pytest.raises(PbtError) as e:
+        ctx.diff_main(many, None, geo, th, ph, LAM, precision="fp32")
+    assert e.value.status == PBT_EINVAL and "outbeam 50001" in str(e.value) and "fi=9" in str(e.value)
+    many["fi"][50000] = 1
+    with pytest.raises(PbtError) as e:
+        ctx.diff_main(many, None, geo, th, ph, LAM, precision="fp32")
+    assert "outbeam 60001" in str(e.value) and "not finite" in str(e.value)
