@@ -12,6 +12,7 @@
 #include <float.h>
 #include <math.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "frame.h"
@@ -45,10 +46,13 @@ __device__ __forceinline__ double dot_3(const double a[3], const double b[3]) {
     return s;
 }
 
-__global__ void __launch_bounds__(128) k1_kernel(
-    const K1Facet *__restrict__ fac, int64_t nf, const K1Edge *__restrict__ edges,
-    const double *__restrict__ xyz, const double *__restrict__ phitab, int64_t nphi, int64_t nb,
-    int64_t theta_i, double waveno, double lambda, int fast_diff, double *__restrict__ out) {
+// The bin of this thread, summed over facets [f0, f1) in order, written to out
+// (8 doubles per bin, the grid's layout).
+__device__ __forceinline__ void k1_bin(const K1Facet *__restrict__ fac, int64_t f0, int64_t f1,
+                                       const K1Edge *__restrict__ edges, const double *__restrict__ xyz,
+                                       const double *__restrict__ phitab, int64_t nphi, int64_t nb,
+                                       int64_t theta_i, double waveno, double lambda, int fast_diff,
+                                       double *__restrict__ out) {
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= nb) return;
     const int64_t i = o % nphi;
@@ -75,7 +79,7 @@ __global__ void __launch_bounds__(128) k1_kernel(
     }
 
     Z acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-    for (int64_t f = 0; f < nf; ++f) {
+    for (int64_t f = f0; f < f1; ++f) {
         const K1Facet *F = fac + f;
         const double c0 = F->com[0], c1 = F->com[1], c2 = F->com[2];
         const double x1 = X - c0, y1 = Y - c1, z1 = Zc - c2;
@@ -230,6 +234,34 @@ __global__ void __launch_bounds__(128) k1_kernel(
     }
 }
 
+// One thread per bin, all facets in order.
+__global__ void __launch_bounds__(128) k1_kernel(
+    const K1Facet *__restrict__ fac, int64_t nf, const K1Edge *__restrict__ edges,
+    const double *__restrict__ xyz, const double *__restrict__ phitab, int64_t nphi, int64_t nb,
+    int64_t theta_i, double waveno, double lambda, int fast_diff, double *__restrict__ out) {
+    k1_bin(fac, 0, nf, edges, xyz, phitab, nphi, nb, theta_i, waveno, lambda, fast_diff, out);
+}
+
+// Small grids: blockIdx.y selects facets [y fchunk, (y + 1) fchunk); each split
+// writes its own partial grid part[y], summed in split order by k1_sum_kernel.
+__global__ void __launch_bounds__(128) k1_split_kernel(
+    const K1Facet *__restrict__ fac, int64_t nf, int64_t fchunk, const K1Edge *__restrict__ edges,
+    const double *__restrict__ xyz, const double *__restrict__ phitab, int64_t nphi, int64_t nb,
+    int64_t theta_i, double waveno, double lambda, int fast_diff, double *__restrict__ part) {
+    const int64_t f0 = (int64_t)blockIdx.y * fchunk, f1 = min(nf, f0 + fchunk);
+    k1_bin(fac, f0, f1, edges, xyz, phitab, nphi, nb, theta_i, waveno, lambda, fast_diff,
+           part + (int64_t)blockIdx.y * 8 * nb);
+}
+
+__global__ void k1_sum_kernel(const double *__restrict__ part, int64_t nsplit, int64_t n,
+                              double *__restrict__ out) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    double s = part[t];
+    for (int64_t k = 1; k < nsplit; k++) s = s + part[k * n + t];
+    out[t] = s;
+}
+
 }  // namespace
 
 int k1_launch(pbt_ctx *ctx, cudaStream_t st, const K1Facet *d_fac, int64_t nf,
@@ -238,12 +270,32 @@ int k1_launch(pbt_ctx *ctx, cudaStream_t st, const K1Facet *d_fac, int64_t nf,
     const double waveno = 2.0 * kPiRef / lambda;
     const int threads = 128;
     const int64_t blocks = (g.nb + threads - 1) / threads;
+    // A grid with fewer bins than about four waves of threads leaves SMs idle:
+    // split the facets over blockIdx.y (at least 16 facets a split, at most 64
+    // splits).  The splits' partial grids are summed in split order, so the
+    // result is deterministic; it differs from the one-split order by rounding.
+    const int64_t want = (int64_t)ctx->sm_count * 4 * threads * 4;
+    int64_t nsplit = std::min<int64_t>(std::min<int64_t>(want / std::max<int64_t>(g.nb, 1), nf / 16), 64);
+    nsplit = std::max<int64_t>(nsplit, 1);
+    const int64_t fchunk = (nf + nsplit - 1) / std::max<int64_t>(nsplit, 1);
+    if (nsplit > 1) nsplit = (nf + fchunk - 1) / fchunk;
     timing_begin(ctx, st);
-    k1_kernel<<<(unsigned)blocks, threads, 0, st>>>(
-        d_fac, nf, d_edges, g.xyz.as<double>(), g.phitab.as<double>(), (int64_t)g.phi.size(), g.nb,
-        g.theta_i, waveno, lambda, fast_diff, d_grid);
+    if (nsplit <= 1) {
+        k1_kernel<<<(unsigned)blocks, threads, 0, st>>>(
+            d_fac, nf, d_edges, g.xyz.as<double>(), g.phitab.as<double>(), (int64_t)g.phi.size(),
+            g.nb, g.theta_i, waveno, lambda, fast_diff, d_grid);
+        ctx->launches++;
+    } else {
+        PBT_TRY(ctx->d_k1part.ensure((size_t)nsplit * 8 * g.nb * sizeof(double)));
+        double *part = ctx->d_k1part.as<double>();
+        k1_split_kernel<<<dim3((unsigned)blocks, (unsigned)nsplit), threads, 0, st>>>(
+            d_fac, nf, fchunk, d_edges, g.xyz.as<double>(), g.phitab.as<double>(),
+            (int64_t)g.phi.size(), g.nb, g.theta_i, waveno, lambda, fast_diff, part);
+        const int64_t n = 8 * g.nb;
+        k1_sum_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(part, nsplit, n, d_grid);
+        ctx->launches += 2;
+    }
     timing_end(ctx, st);
-    ctx->launches++;
     PBT_CUDA_TRY(cudaGetLastError());
     return PBT_OK;
 }

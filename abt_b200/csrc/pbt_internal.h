@@ -117,6 +117,7 @@ struct pbt_ctx {
     pbt::GridCache grid;
     // scratch (grow-only)
     pbt::DevBuf d_fac, d_edge, d_out, d_mu, d_m1, d_misc, d_in, d_rec, d_ws, d_scan, d_items;
+    pbt::DevBuf d_k1part;  // FP64 drop-in: partial grids of the facet splits (small grids)
     pbt::HostBuf h_stage;
     cudaEvent_t stage_ev = nullptr;  // last copy out of h_stage (wait before reuse)
     bool stage_pending = false;
