@@ -1030,9 +1030,22 @@ __global__ void __launch_bounds__(K2_THREADS, (BPT == 1 && FAST) ? 4 : 0) k2_mai
                                   hi_ok && valid[q], P.xyz, P.nb);
             };
             if (FAST) {
-                // two pairs per iteration: with most pairs culled, the loop overhead shows
-#pragma unroll 2
-                for (int j = 0; j < n; j++) pair_step(j);
+                // visit only the pairs with a record the tile cull kept: bit j of pm
+                // is set when record 2j or 2j+1 is (the two ballot words compacted)
+                auto pairs_of = [](unsigned x) {
+                    x = (x | (x >> 1)) & 0x55555555u;
+                    x = (x | (x >> 1)) & 0x33333333u;
+                    x = (x | (x >> 2)) & 0x0F0F0F0Fu;
+                    x = (x | (x >> 4)) & 0x00FF00FFu;
+                    x = (x | (x >> 8)) & 0x0000FFFFu;
+                    return x;
+                };
+                unsigned pm = pairs_of(s_keep[0]) | (pairs_of(s_keep[1]) << 16);
+                while (pm) {
+                    const int j = __ffs(pm) - 1;
+                    pm &= pm - 1u;
+                    pair_step(j);
+                }
             } else {
                 for (int j = 0; j < n; j++) pair_step(j);
             }
