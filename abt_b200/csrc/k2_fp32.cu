@@ -1435,12 +1435,14 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
 
 template <int BPT, bool FAST>
 int k2_launch_main(pbt_ctx *ctx, cudaStream_t st, const K2MainArgs &A) {
-    static int occ = -1;
-    if (occ < 0) {
+    // resident CTAs per SM, computed once (thread-safe static initialisation)
+    static const int occ = [] {
         int n = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k2_main_kernel<BPT, FAST>, K2_THREADS, 0);
-        occ = n > 0 ? n : 1;
-    }
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k2_main_kernel<BPT, FAST>, K2_THREADS, 0) !=
+            cudaSuccess)
+            (void)cudaGetLastError();
+        return n > 0 ? n : 1;
+    }();
     const int grid = ctx->sm_count * occ;
     timing_begin(ctx, st);
     k2_main_kernel<BPT, FAST><<<grid, K2_THREADS, 0, st>>>(A);
@@ -1452,12 +1454,13 @@ int k2_launch_main(pbt_ctx *ctx, cudaStream_t st, const K2MainArgs &A) {
 
 template <int BPT, bool FAST>
 int k2_launch_pk(pbt_ctx *ctx, cudaStream_t st, const K2PkArgs &A) {
-    static int occ = -1;
-    if (occ < 0) {
+    static const int occ = [] {
         int n = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k2_main_pk_kernel<BPT, FAST>, K2_THREADS, 0);
-        occ = n > 0 ? n : 1;
-    }
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k2_main_pk_kernel<BPT, FAST>, K2_THREADS,
+                                                          0) != cudaSuccess)
+            (void)cudaGetLastError();
+        return n > 0 ? n : 1;
+    }();
     const int grid = ctx->sm_count * occ;
     timing_begin(ctx, st);
     k2_main_pk_kernel<BPT, FAST><<<grid, K2_THREADS, 0, st>>>(A);
