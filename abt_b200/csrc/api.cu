@@ -177,6 +177,7 @@ int check_offsets(const int64_t *off, int64_t norient, const char *what) {
 
 #define API_ENTER(ctx)                              \
     clear_error();                                  \
+    pbt::DeviceRestore dev_restore_;                \
     PBT_TRY(check_ctx(ctx));                        \
     std::lock_guard<std::mutex> lock_((ctx)->mu);   \
     (ctx)->launches = 0;                            \
@@ -739,6 +740,7 @@ extern "C" int pbt_diff_batch_dev_graph_c(pbt_ctx *ctx, void *stream, int64_t no
                                           pbt_output_params *params_avg,
                                           pbt_output_params *params_per_orient, pbt_graph **out) {
     clear_error();
+    pbt::DeviceRestore dev_restore_;
     PBT_TRY(check_ctx(ctx));
     if (!out) {
         set_error("graph: out must not be NULL");
@@ -821,6 +823,7 @@ extern "C" int pbt_graph_launch_c(pbt_graph *G, void *stream) {
         set_error("graph: NULL or destroyed graph");
         return PBT_EINVAL;
     }
+    pbt::DeviceRestore dev_restore_;
     PBT_CUDA_TRY(cudaSetDevice(G->device));
     PBT_CUDA_TRY(cudaGraphLaunch(G->exec, (cudaStream_t)stream));
     return PBT_OK;
@@ -831,6 +834,7 @@ extern "C" int64_t pbt_graph_kernel_count(const pbt_graph *G) { return G ? G->la
 extern "C" int pbt_graph_destroy_c(pbt_graph *G) {
     clear_error();
     if (!G) return PBT_OK;
+    pbt::DeviceRestore dev_restore_;
     cudaSetDevice(G->device);
     if (G->exec) cudaGraphExecDestroy(G->exec);
     if (G->graph) cudaGraphDestroy(G->graph);

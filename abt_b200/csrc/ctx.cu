@@ -128,6 +128,7 @@ extern "C" int pbt_kernel_time_ms(pbt_ctx *ctx, double *total_ms, int64_t *nlaun
         set_error("NULL argument");
         return PBT_EINVAL;
     }
+    DeviceRestore dev_restore;
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
     double t = 0.0;
@@ -172,6 +173,7 @@ extern "C" int pbt_ctx_create(int device, pbt_ctx **out) {
                   prop.minor);
         return PBT_ENODEV;
     }
+    DeviceRestore dev_restore;
     PBT_CUDA_TRY(cudaSetDevice(device));
     pbt_ctx *c = new pbt_ctx();
     c->device = device;
@@ -190,6 +192,7 @@ extern "C" int pbt_ctx_destroy(pbt_ctx *ctx) {
     clear_error();
     if (!ctx) return PBT_OK;
     {
+        DeviceRestore dev_restore;
         std::lock_guard<std::mutex> lk(ctx->mu);
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);

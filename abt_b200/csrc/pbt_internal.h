@@ -34,6 +34,23 @@ const char *last_error();
 
 // ------------------------------------------------------------ device memory
 // Grow-only device buffer owned by a context.
+// Restores the calling thread's current device when an entry point returns
+// (entry points make their context's device current while they run).
+struct DeviceRestore {
+    int prev = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            prev = -1;
+            (void)cudaGetLastError();
+        }
+    }
+    ~DeviceRestore() {
+        if (prev >= 0) (void)cudaSetDevice(prev);
+    }
+    DeviceRestore(const DeviceRestore &) = delete;
+    DeviceRestore &operator=(const DeviceRestore &) = delete;
+};
+
 struct DevBuf {
     void *p = nullptr;
     size_t cap = 0;
