@@ -604,12 +604,17 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
     std::vector<Host4> H(nrec);
     for (int64_t q = 0; q < nrec; q++) {
         const pbt_outbeam &ob = q < nbeam ? beam[q] : ext[q - nbeam];
-        const int64_t fb = face_off[ob.fi - 1];
-        if (face_off[ob.fi] - fb != 3) {
+        if (face_off[ob.fi] - face_off[ob.fi - 1] != 3) {
             set_error("the adjoint supports triangular facets only (outbeam %lld, face %lld)",
                       (long long)(q + 1), (long long)ob.fi);
             return PBT_EINVAL;
         }
+    }
+    // per-record set-up in FP64 (independent records: all host threads)
+#pragma omp parallel for schedule(static) if (nrec > 1024)
+    for (int64_t q = 0; q < nrec; q++) {
+        const pbt_outbeam &ob = q < nbeam ? beam[q] : ext[q - nbeam];
+        const int64_t fb = face_off[ob.fi - 1];
         double vx[3], vy[3], vz[3], rx[3], ry[3], rz[3];
         for (int i = 0; i < 3; i++) {
             const int64_t vi = face_vi[fb + i] - 1;
@@ -752,9 +757,12 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
     if (nrec > 0)
         PBT_CUDA_TRY(cudaMemcpyAsync(acc.data(), base + o_out, acc.size() * 8, cudaMemcpyDeviceToHost, st));
     PBT_CUDA_TRY(cudaStreamSynchronize(st));
-    // FP64 mapping of the per-record sums to the vertices and amplitudes
-    for (int64_t q = 0; q < 3 * nverts; q++) gverts[q] = 0.0;
+    // FP64 mapping of the per-record sums to the vertices and amplitudes: each
+    // record's three vertex cotangents are formed in parallel, then added to the
+    // shared vertices in record order (the same sum whatever the thread count)
+    std::vector<double> vc(9 * nrec);
     const double inc[3] = {0, 0, -1};
+#pragma omp parallel for schedule(static) if (nrec > 1024)
     for (int64_t q = 0; q < nrec; q++) {
         const double *A = &acc[q * K4_NACC];
         const Host4 &h = H[q];
@@ -844,9 +852,12 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
         for (int j = 0; j < 3; j++)
             for (int b = 0; b < 3; b++) esum[b] += eb[j][b];
         for (int j = 0; j < 3; j++)
-            for (int b = 0; b < 3; b++)
-                gverts[h.vi[j] + nverts * b] += eb[j][b] + (cb[b] - esum[b]) / 3.0;
+            for (int b = 0; b < 3; b++) vc[9 * q + 3 * j + b] = eb[j][b] + (cb[b] - esum[b]) / 3.0;
     }
+    for (int64_t q = 0; q < 3 * nverts; q++) gverts[q] = 0.0;
+    for (int64_t q = 0; q < nrec; q++)
+        for (int j = 0; j < 3; j++)
+            for (int b = 0; b < 3; b++) gverts[H[q].vi[j] + nverts * b] += vc[9 * q + 3 * j + b];
     return PBT_OK;
 }
 
