@@ -143,3 +143,17 @@ def test_first_bad_record_of_a_long_list_is_reported(ctx):
     with pytest.raises(PbtError) as e:
         ctx.diff_main(many, None, geo, th, ph, LAM, precision="fp32")
     assert "outbeam 60001" in str(e.value) and "not finite" in str(e.value)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_no_outbeams_at_all(ctx, precision):
+    """A call with no outbeams in either list is legal and gives zero grids, and
+    a batch whose orientations are all empty gives a zero Mueller average."""
+    th, ph, geo, ob = _inputs()
+    afb, afe = ctx.diff_main(ob[:0], ob[:0], geo, th, ph, LAM, precision=precision)
+    assert afb.shape == (len(ph), len(th), 2, 2) and not afb.any() and not afe.any()
+    pin = np.zeros(3, dtype=abt_b200.PARAMS_DTYPE)
+    pin["geo_cross_sec"] = 1.0
+    mu, mu1, _, _ = ctx.diff_batch([ob[:0]] * 3, [ob[:0]] * 3, [geo["verts"]] * 3, geo, th, ph,
+                                   LAM, pin, precision=precision)
+    assert not mu.any() and not mu1.any()
