@@ -50,7 +50,7 @@ module pbt_b200_diff_mod
         integer(c_int) function pbt_diff_main_c(ctx, beam, nbeam, ext, next, verts, nverts, &
                 face_off, face_vi, nfaces, theta, ntheta, phi, nphi, lambda, is_fast_diff, &
                 precision, ampl_far_beam, ampl_far_ext_diff) bind(C, name="pbt_diff_main_c")
-            import :: c_int, c_int32_t, c_int64_t, c_double, c_ptr, pbt_outbeam
+            import :: c_int, c_int32_t, c_int64_t, c_double, c_double_complex, c_ptr, pbt_outbeam
             type(c_ptr), value :: ctx
             type(pbt_outbeam), intent(in) :: beam(*), ext(*)
             integer(c_int64_t), value :: nbeam, next, nverts, nfaces, ntheta, nphi
@@ -63,7 +63,7 @@ module pbt_b200_diff_mod
         integer(c_int) function pbt_diffraction_c(ctx, outbeam, verts, nverts, face_off, face_vi, &
                 nfaces, theta, ntheta, phi, nphi, lambda, is_fast_diff, amplC) &
                 bind(C, name="pbt_diffraction_c")
-            import :: c_int, c_int32_t, c_int64_t, c_double, c_ptr, pbt_outbeam
+            import :: c_int, c_int32_t, c_int64_t, c_double, c_double_complex, c_ptr, pbt_outbeam
             type(c_ptr), value :: ctx
             type(pbt_outbeam), intent(in) :: outbeam
             integer(c_int64_t), value :: nverts, nfaces, ntheta, nphi
@@ -76,7 +76,7 @@ module pbt_b200_diff_mod
         integer(c_int) function pbt_finalise_c(ctx, ampl_far_beam, ampl_far_ext_diff, theta, &
                 ntheta, phi, nphi, lambda, scaling, params, mueller, mueller_1d, accumulate) &
                 bind(C, name="pbt_finalise_c")
-            import :: c_int, c_int32_t, c_int64_t, c_double, c_ptr, pbt_output_params
+            import :: c_int, c_int32_t, c_int64_t, c_double, c_double_complex, c_ptr, pbt_output_params
             type(c_ptr), value :: ctx
             complex(c_double_complex), intent(in) :: ampl_far_beam(*), ampl_far_ext_diff(*)
             real(c_double), intent(in) :: theta(*), phi(*)
