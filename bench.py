@@ -11,10 +11,13 @@ epilogue (Mueller matrix, phi/theta integrals, cross sections), inputs
 resident in HBM.  Metric: facet x bin evaluations per second (whole job).
 
 Also reported: the same metric end to end through the host C ABI
-(pbt_diff_batch_c, pinned host buffers, copies inside the timed region), the
+(pbt_diff_batch_list_c, pinned host buffers, copies inside the timed region)
+and the roofline of the dominant kernel; in single-GPU runs also the
 reference-exact FP64 drop-in's rate, the FP32-vs-FP64 Mueller error on the
-full workload, the roofline of the dominant kernel and a CPU baseline (the
-C FP64 restatement of the reference, all host cores, bounded sample).
+full workload, the further workloads (orientation average, differentiation,
+large column, -fast_diff, adjoint) and a CPU baseline (the C FP64
+restatement of the reference, all host cores, bounded sample).  N-GPU runs
+(replicas) time the step, e2e and roofline only.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -524,6 +527,10 @@ def main():
     value = replicas_value(world, work, ms_step)
 
     extra = {}
+    # Beyond the timed step, e2e and the roofline, the sections are single-GPU
+    # measurements: they run in the N = 1 run only, so that an N-GPU run holds
+    # its GPUs for the step alone.
+    solo = world == 1
     # end to end through the host C ABI with pinned host buffers
     pinned_beam = torch.from_numpy(beam.view(np.uint8).copy()).pin_memory()
     pb = pinned_beam.numpy().view(abt_b200.OUTBEAM_DTYPE)
@@ -548,7 +555,7 @@ def main():
     for _ in range(args.e2e_steps):
         out = ctx.diff_batch([pb], [np.zeros(0, abt_b200.OUTBEAM_DTYPE)], [pverts], geo_p, th, ph,
                              LAM, pin, precision="fp32", out=(pmu, pmu1))
-    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    e2e_s = max_over_ranks(dist, (time.perf_counter() - t0) / args.e2e_steps, dev)
     h2d = beam.nbytes + geo["verts"].nbytes + geo["face_off"].nbytes + geo["face_vi"].nbytes + pin.nbytes
     d2h = 16 * nb * 8 + 16 * len(th) * 8 + 2 * pin.nbytes
     e2e = {"value": world * work / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -556,7 +563,7 @@ def main():
            "api": "pbt_diff_batch_list_c (host pointers; inputs and Mueller outputs pinned)"}
 
     # reference-exact FP64 drop-in rate on a facet sample
-    if args.fp64_facets > 0:
+    if args.fp64_facets > 0 and solo:
         sub = beam[:args.fp64_facets]
         ctx.diff_main(sub[:64], None, geo, th, ph, LAM, precision="fp64")
         ctx.set_kernel_timing(True)
@@ -573,7 +580,7 @@ def main():
         extra["fp32_vs_fp64_kernel_speedup"] = (work / (kern_ms / max(kern_n, 1) / 1e3)) / r64
 
     # adjoint (vector-Jacobian product) against the forward, same facets and grid
-    if args.adjoint_facets > 0:
+    if args.adjoint_facets > 0 and solo:
         sub = beam[:args.adjoint_facets]
         rng = np.random.default_rng(1)
         shape = (len(ph), len(th), 2, 2)
@@ -595,17 +602,17 @@ def main():
                             "adjoint_call_ms": adj_call * 1e3,
                             "value": len(sub) * nb / (adj_ms / 1e3), "unit": UNIT}
 
-    if args.orient > 0 and rank == 0:
+    if args.orient > 0 and solo:
         extra["orientation_average"] = orientation_average(ctx, args)
 
-    if args.diff_orient > 0 and rank == 0:
+    if args.diff_orient > 0 and solo:
         extra["differentiation"] = differentiation(ctx, args)
-    if args.large_orient > 0 and rank == 0:
+    if args.large_orient > 0 and solo:
         extra["large_column"] = large_case(ctx, args)
 
     # -fast_diff: the same workload with the field-of-view test (fov = 8 lambda / d);
     # error against the FP64 drop-in with is_fast_diff on the first 20,000 facets
-    if args.fast_diff and rank == 0:
+    if args.fast_diff and solo:
         ctx.diff_main(beam[:64], None, geo, th, ph, LAM, is_fast_diff=True, precision="fp32")
         ctx.set_kernel_timing(True)
         ctx.kernel_time_ms()
@@ -627,7 +634,7 @@ def main():
                                       "bin tile are skipped for that tile"}
 
     # FP32 error against the FP64 drop-in on the full workload
-    if not args.no_error_check:
+    if not args.no_error_check and solo:
         from tests.helpers import mueller_rel_err
         f64 = ctx.diff_batch([beam], [np.zeros(0, abt_b200.OUTBEAM_DTYPE)], [geo["verts"]], geo,
                              th, ph, LAM, pin, precision="fp64")
@@ -668,7 +675,7 @@ def main():
                           "FP32/MUFU/FP64 figure" % (sms, mhz)}
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if solo and not args.no_cpu_baseline:
         cpu = cpu_baseline(geo, beam, th, ph, args.cpu_seconds, os.cpu_count() or 1)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
