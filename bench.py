@@ -156,6 +156,9 @@ def dist_setup(args):
 
         import torch.distributed as dist
         backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)  # each rank's GPU current before NCCL starts
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
@@ -518,6 +521,8 @@ def main():
         launches += step_kernels if graph is not None else ctx.last_launch_count()
     e1.record(stream)
     torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
     clk = clocks.stop()
     ms_total = e0.elapsed_time(e1)
     if graph is not None:
