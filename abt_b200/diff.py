@@ -149,15 +149,27 @@ class Context:
 
     # ------------------------------------------------------------ diff_mod
     def diff_main(self, beam, ext, geometry, theta, phi, lam, is_fast_diff=False,
-                  precision="fp64"):
-        """diff_main (src/diff_mod.f90:674-825) -> (ampl_far_beam, ampl_far_ext_diff)."""
+                  precision="fp64", out=None):
+        """diff_main (src/diff_mod.f90:674-825) -> (ampl_far_beam, ampl_far_ext_diff).
+
+        out: optional (ampl_far_beam, ampl_far_ext_diff) arrays to write into,
+        complex128 of shape (nphi, ntheta, 2, 2) in Fortran order (e.g. views
+        of pinned host memory, reused call after call)."""
         beam, ext = _ob(beam), _ob(ext)
         v, fo, fv = _geo(geometry)
         theta = np.ascontiguousarray(theta, dtype=np.float64)
         phi = np.ascontiguousarray(phi, dtype=np.float64)
         shape = (len(phi), len(theta), 2, 2)
-        afb = np.zeros(shape, dtype=np.complex128, order="F")
-        afe = np.zeros(shape, dtype=np.complex128, order="F")
+        if out is None:
+            afb = np.empty(shape, dtype=np.complex128, order="F")
+            afe = np.empty(shape, dtype=np.complex128, order="F")
+        else:
+            afb, afe = out
+            for a in (afb, afe):
+                if (not isinstance(a, np.ndarray) or a.dtype != np.complex128 or a.shape != shape
+                        or not a.flags.f_contiguous or not a.flags.writeable):
+                    raise ValueError("out arrays must be writeable Fortran-ordered complex128 of "
+                                     "shape (nphi, ntheta, 2, 2)")
         check(_lib.lib().pbt_diff_main_c(self._h, ptr(beam), len(beam), ptr(ext), len(ext),
                                          ptr(v), v.shape[0], ptr(fo), ptr(fv), len(fo) - 1,
                                          ptr(theta), len(theta), ptr(phi), len(phi), float(lam),

@@ -171,3 +171,28 @@ def test_batch_writes_into_caller_arrays(ctx):
     with pytest.raises(ValueError):
         ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp32",
                        out=(np.empty((len(ph), len(th), 16)), m1))
+
+
+@pytest.mark.gpu
+def test_diff_main_writes_into_caller_arrays(ctx):
+    """diff_main(out=...) fills the caller's (here pinned) grids with the values
+    of freshly allocated ones, in both precisions, and refuses a wrong layout."""
+    import torch
+    rng = np.random.default_rng(8)
+    th, ph = abt_b200.make_angles([0, 180], [5]), abt_b200.make_angles([0, 350], [10])
+    geo = one_triangle(scale=2.0)
+    beam = outbeams(3, rng, 1)
+    ext = outbeams(1, rng, 1, prop=(0, 0, -1))
+    shape = (len(ph), len(th), 2, 2)
+    n = int(np.prod(shape)) * 16
+    for prec in ("fp64", "fp32"):
+        ref = ctx.diff_main(beam, ext, geo, th, ph, LAM, precision=prec)
+        grids = [torch.empty(n, dtype=torch.uint8, pin_memory=True).numpy().view(np.complex128)
+                 .reshape(shape, order="F") for _ in range(2)]
+        got = ctx.diff_main(beam, ext, geo, th, ph, LAM, precision=prec, out=tuple(grids))
+        assert got[0] is grids[0] and got[1] is grids[1]
+        tol = 1e-12 if prec == "fp64" else 1e-6
+        assert rel_err(got[0], ref[0]) <= tol and rel_err(got[1], ref[1]) <= tol
+    with pytest.raises(ValueError):
+        ctx.diff_main(beam, ext, geo, th, ph, LAM, precision="fp32",
+                      out=(np.empty(shape, np.complex128), np.empty(shape, np.complex128)))
