@@ -580,39 +580,26 @@ __global__ void k4_prep_kernel(const double *__restrict__ gafb, const double *__
     }
 }
 
-}  // namespace
+// Per-record data of the FP64 mapping: centre, vertex offsets, frame,
+// propagation direction, signed area, anti-parallel sign, vertex indices.
+struct Host4 {
+    double c[3], e[3][3], R[3][3], p[3], As, sign;
+    int64_t vi[3];
+};
 
-// Host side: set-up per triangle (FP64, libm), the kernel, and the FP64
-// mapping of the per-record sums to vertex and amplitude gradients.
-int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t nbeam,
-               const pbt_outbeam *ext, int64_t next, const double *verts, int64_t nverts,
-               const int64_t *face_off, const int64_t *face_vi, int64_t nfaces, double lambda,
-               int fast_diff, const double *gafb, const double *gafe, double *gverts,
-               double *gbeam, double *gext) {
-    (void)nfaces;  // face indices were validated by the caller
-    const GridCache &g = ctx->grid;
-    const int64_t nb = g.nb, nphi = (int64_t)g.phi.size();
-    const double k = 2.0 * kPiRef / lambda, Rf = kFarR;
-    const int64_t nrec = nbeam + next;
-    struct Host4 {
-        double c[3], e[3][3], R[3][3], p[3], As, sign;
-        int64_t vi[3];
-    };
-    std::vector<K4Rec> recs(nrec);
-    std::vector<int> kinds(nrec);
-    std::vector<float> fovd(4 * nrec);
-    std::vector<Host4> H(nrec);
-    for (int64_t q = 0; q < nrec; q++) {
-        const pbt_outbeam &ob = q < nbeam ? beam[q] : ext[q - nbeam];
-        if (face_off[ob.fi] - face_off[ob.fi - 1] != 3) {
-            set_error("the adjoint supports triangular facets only (outbeam %lld, face %lld)",
-                      (long long)(q + 1), (long long)ob.fi);
-            return PBT_EINVAL;
-        }
-    }
-    // per-record set-up in FP64 (independent records: all host threads)
-#pragma omp parallel for schedule(static) if (nrec > 1024)
-    for (int64_t q = 0; q < nrec; q++) {
+// Thread per record (beam outbeams, then external diffraction): the FP64
+// set-up of the kernel record K4Rec (frame, aperture-frame vertices, the
+// constants of the bin loop, the circular-basis amplitudes), of the
+// field-of-view data and of the mapping data Host4.
+__global__ void k4_setup_kernel(const pbt_outbeam *__restrict__ beam, int64_t nbeam,
+                                const pbt_outbeam *__restrict__ ext, int64_t nrec,
+                                const double *__restrict__ verts, int64_t nverts,
+                                const int64_t *__restrict__ face_off, const int64_t *__restrict__ face_vi,
+                                double k, double lambda, K4Rec *__restrict__ recs, int *__restrict__ kinds,
+                                float *__restrict__ fovd, Host4 *__restrict__ H) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nrec) return;
+    const double Rf = kFarR;
         const pbt_outbeam &ob = q < nbeam ? beam[q] : ext[q - nbeam];
         const int64_t fb = face_off[ob.fi - 1];
         double vx[3], vy[3], vz[3], rx[3], ry[3], rz[3];
@@ -691,79 +678,20 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
         fovd[4 * q + 2] = (float)ob.prop_out[2];
         fovd[4 * q + 3] = (float)cos(fov);
     }
-    // device buffers: recs | kinds | fov | gafb | gafe | ud | uh | gbin | out
-    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t o_rec = 0, o_kind = al(nrec * sizeof(K4Rec)), o_fov = al(o_kind + nrec * 4),
-                 o_ga = al(o_fov + 16 * nrec), o_gb = al(o_ga + 8 * nb * 8),
-                 o_bin = al(o_gb + 8 * nb * 8), o_gbin = al(o_bin + nb * sizeof(K4Bin)),
-                 o_out = al(o_gbin + 16 * nb * 4),
-                 o_end = al(o_out + nrec * K4_NACC * 8);
-    PBT_TRY(ctx->d_ws.ensure(o_end));
-    char *base = ctx->d_ws.as<char>();
-    if (nrec > 0) {
-        PBT_CUDA_TRY(cudaMemcpyAsync(base + o_rec, recs.data(), nrec * sizeof(K4Rec), cudaMemcpyHostToDevice, st));
-        PBT_CUDA_TRY(cudaMemcpyAsync(base + o_kind, kinds.data(), nrec * 4, cudaMemcpyHostToDevice, st));
-        PBT_CUDA_TRY(cudaMemcpyAsync(base + o_fov, fovd.data(), 16 * nrec, cudaMemcpyHostToDevice, st));
-        PBT_CUDA_TRY(cudaMemsetAsync(base + o_out, 0, nrec * K4_NACC * 8, st));
-    }
-    PBT_CUDA_TRY(cudaMemcpyAsync(base + o_ga, gafb, 8 * nb * 8, cudaMemcpyHostToDevice, st));
-    PBT_CUDA_TRY(cudaMemcpyAsync(base + o_gb, gafe, 8 * nb * 8, cudaMemcpyHostToDevice, st));
-    k4_prep_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, st>>>(
-        (const double *)(base + o_ga), (const double *)(base + o_gb), g.xyz.as<double>(),
-        g.phitab.as<double>(), nb, nphi, k, (K4Bin *)(base + o_bin),
-        (float4 *)(base + o_gbin));
-    // bin ranges: at most K4_MAX_LANE_BINS terms per lane, and enough CTAs
-    // for a few waves when there are few records
-    const int64_t ncta_rec = (nrec + K4_WARPS - 1) / K4_WARPS;
-    int64_t nsplit = (nb + 32 * K4_MAX_LANE_BINS - 1) / (32 * K4_MAX_LANE_BINS);
-    if (ncta_rec > 0) nsplit = std::max(nsplit, (int64_t)(8 * ctx->sm_count + ncta_rec - 1) / ncta_rec);
-    nsplit = std::min(nsplit, std::max<int64_t>(1, nb / 256));
-    nsplit = std::min<int64_t>(nsplit, 65535);
-    const int64_t chunk = (((nb + nsplit - 1) / nsplit) + 31) / 32 * 32;
-    nsplit = (nb + chunk - 1) / chunk;
-    const dim3 grid((unsigned)ncta_rec, (unsigned)nsplit);
-    timing_begin(ctx, st);
-    // Minimum CTAs per SM for the register budget: 3 (168 registers, a few
-    // bytes of spill) by default; PBT_K4_MINB=1|2|4 selects another build.
-    static const int minb = [] {
-        const char *e = getenv("PBT_K4_MINB");
-        const int v = e ? atoi(e) : 3;
-        return (v == 1 || v == 2 || v == 4) ? v : 3;
-    }();
-    if (nrec > 0) {
-        auto launch = [&](auto kern) {
-            kern<<<grid, K4_WARPS * 32, 0, st>>>(
-                (const K4Rec *)(base + o_rec), (const int *)(base + o_kind), (const float *)(base + o_fov),
-                nrec, (const K4Bin *)(base + o_bin), (const float4 *)(base + o_gbin), nb, nphi,
-                g.theta_i, chunk, (float)k,
-                (float)(0.5 * k * Rf), (float)(1.0 / Rf), (double *)(base + o_out));
-        };
-        if (fast_diff) {
-            if (minb == 1) launch(k4_adjoint_kernel<true, 1>);
-            else if (minb == 2) launch(k4_adjoint_kernel<true, 2>);
-            else if (minb == 4) launch(k4_adjoint_kernel<true, 4>);
-            else launch(k4_adjoint_kernel<true, 3>);
-        } else {
-            if (minb == 1) launch(k4_adjoint_kernel<false, 1>);
-            else if (minb == 2) launch(k4_adjoint_kernel<false, 2>);
-            else if (minb == 4) launch(k4_adjoint_kernel<false, 4>);
-            else launch(k4_adjoint_kernel<false, 3>);
-        }
-    }
-    timing_end(ctx, st);
-    ctx->launches += nrec > 0 ? 2 : 1;
-    PBT_CUDA_TRY(cudaGetLastError());
-    std::vector<double> acc(nrec * K4_NACC);
-    if (nrec > 0)
-        PBT_CUDA_TRY(cudaMemcpyAsync(acc.data(), base + o_out, acc.size() * 8, cudaMemcpyDeviceToHost, st));
-    PBT_CUDA_TRY(cudaStreamSynchronize(st));
-    // FP64 mapping of the per-record sums to the vertices and amplitudes: each
-    // record's three vertex cotangents are formed in parallel, then added to the
-    // shared vertices in record order (the same sum whatever the thread count)
-    std::vector<double> vc(9 * nrec);
+
+// Thread per record: the record's 36 sums mapped through the frame
+// construction (z = -n, x = unit(p - (p.n) n), y = z x x, n = unit(e0 x e1),
+// c = mean(v)) to its three vertices (added with FP64 atomics) and to its
+// amplitude (gamp: 8 doubles, the outbeam's ampl order).
+__global__ void k4_map_kernel(const double *__restrict__ acc, const Host4 *__restrict__ H,
+                              const pbt_outbeam *__restrict__ beam, int64_t nbeam,
+                              const pbt_outbeam *__restrict__ ext, int64_t nrec, double lambda,
+                              int64_t nverts, double *__restrict__ gbeam, double *__restrict__ gext,
+                              double *__restrict__ gverts) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nrec) return;
+    const double Rf = kFarR;
     const double inc[3] = {0, 0, -1};
-#pragma omp parallel for schedule(static) if (nrec > 1024)
-    for (int64_t q = 0; q < nrec; q++) {
         const double *A = &acc[q * K4_NACC];
         const Host4 &h = H[q];
         const pbt_outbeam &ob = q < nbeam ? beam[q] : ext[q - nbeam];
@@ -852,12 +780,124 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
         for (int j = 0; j < 3; j++)
             for (int b = 0; b < 3; b++) esum[b] += eb[j][b];
         for (int j = 0; j < 3; j++)
-            for (int b = 0; b < 3; b++) vc[9 * q + 3 * j + b] = eb[j][b] + (cb[b] - esum[b]) / 3.0;
+            for (int b = 0; b < 3; b++)
+                atomicAdd(&gverts[h.vi[j] + nverts * b], eb[j][b] + (cb[b] - esum[b]) / 3.0);
     }
-    for (int64_t q = 0; q < 3 * nverts; q++) gverts[q] = 0.0;
-    for (int64_t q = 0; q < nrec; q++)
-        for (int j = 0; j < 3; j++)
-            for (int b = 0; b < 3; b++) gverts[H[q].vi[j] + nverts * b] += vc[9 * q + 3 * j + b];
+
+}  // namespace
+
+// Host side: the triangle check, the device set-up, the kernels, and the
+// gradient copies.
+int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t nbeam,
+               const pbt_outbeam *ext, int64_t next, const double *verts, int64_t nverts,
+               const int64_t *face_off, const int64_t *face_vi, int64_t nfaces, double lambda,
+               int fast_diff, const double *gafb, const double *gafe, double *gverts,
+               double *gbeam, double *gext) {
+    const GridCache &g = ctx->grid;
+    const int64_t nb = g.nb, nphi = (int64_t)g.phi.size();
+    const double k = 2.0 * kPiRef / lambda, Rf = kFarR;
+    const int64_t nrec = nbeam + next;
+    for (int64_t q = 0; q < nrec; q++) {
+        const pbt_outbeam &ob = q < nbeam ? beam[q] : ext[q - nbeam];
+        if (face_off[ob.fi] - face_off[ob.fi - 1] != 3) {
+            set_error("the adjoint supports triangular facets only (outbeam %lld, face %lld)",
+                      (long long)(q + 1), (long long)ob.fi);
+            return PBT_EINVAL;
+        }
+    }
+    // device buffers: recs | kinds | fov | gafb | gafe | bins | gbin | out | outbeams |
+    // verts | face_off | face_vi | mapping data | vertex gradients | amplitude gradients
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const int64_t nvi = face_off[nfaces];
+    const size_t ob = sizeof(pbt_outbeam);
+    const size_t o_rec = 0, o_kind = al(nrec * sizeof(K4Rec)), o_fov = al(o_kind + nrec * 4),
+                 o_ga = al(o_fov + 16 * nrec), o_gb = al(o_ga + 8 * nb * 8),
+                 o_bin = al(o_gb + 8 * nb * 8), o_gbin = al(o_bin + nb * sizeof(K4Bin)),
+                 o_out = al(o_gbin + 16 * nb * 4), o_ob = al(o_out + nrec * K4_NACC * 8),
+                 o_vert = al(o_ob + nrec * ob), o_fo = al(o_vert + 3 * nverts * 8),
+                 o_fv = al(o_fo + (nfaces + 1) * 8), o_h = al(o_fv + nvi * 8),
+                 o_gv = al(o_h + nrec * sizeof(Host4)), o_gamp = al(o_gv + 3 * nverts * 8),
+                 o_end = al(o_gamp + nrec * 8 * 8);
+    PBT_TRY(ctx->d_ws.ensure(o_end));
+    char *base = ctx->d_ws.as<char>();
+    pbt_outbeam *d_ob = (pbt_outbeam *)(base + o_ob);
+    Host4 *d_h = (Host4 *)(base + o_h);
+    double *d_gv = (double *)(base + o_gv), *d_gamp = (double *)(base + o_gamp);
+    PBT_CUDA_TRY(cudaMemsetAsync(d_gv, 0, 3 * nverts * 8, st));
+    if (nrec > 0) {
+        // the FP64 set-up of each record on the device (the same frame code as the
+        // forward's set-up), one thread per record
+        if (nbeam) PBT_CUDA_TRY(cudaMemcpyAsync(d_ob, beam, nbeam * ob, cudaMemcpyHostToDevice, st));
+        if (next) PBT_CUDA_TRY(cudaMemcpyAsync(d_ob + nbeam, ext, next * ob, cudaMemcpyHostToDevice, st));
+        PBT_CUDA_TRY(cudaMemcpyAsync(base + o_vert, verts, 3 * nverts * 8, cudaMemcpyHostToDevice, st));
+        PBT_CUDA_TRY(cudaMemcpyAsync(base + o_fo, face_off, (nfaces + 1) * 8, cudaMemcpyHostToDevice, st));
+        PBT_CUDA_TRY(cudaMemcpyAsync(base + o_fv, face_vi, nvi * 8, cudaMemcpyHostToDevice, st));
+        k4_setup_kernel<<<(unsigned)((nrec + 127) / 128), 128, 0, st>>>(
+            d_ob, nbeam, d_ob + nbeam, nrec, (const double *)(base + o_vert), nverts,
+            (const int64_t *)(base + o_fo), (const int64_t *)(base + o_fv), k, lambda,
+            (K4Rec *)(base + o_rec), (int *)(base + o_kind), (float *)(base + o_fov), d_h);
+        PBT_CUDA_TRY(cudaMemsetAsync(base + o_out, 0, nrec * K4_NACC * 8, st));
+    }
+    PBT_CUDA_TRY(cudaMemcpyAsync(base + o_ga, gafb, 8 * nb * 8, cudaMemcpyHostToDevice, st));
+    PBT_CUDA_TRY(cudaMemcpyAsync(base + o_gb, gafe, 8 * nb * 8, cudaMemcpyHostToDevice, st));
+    k4_prep_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, st>>>(
+        (const double *)(base + o_ga), (const double *)(base + o_gb), g.xyz.as<double>(),
+        g.phitab.as<double>(), nb, nphi, k, (K4Bin *)(base + o_bin),
+        (float4 *)(base + o_gbin));
+    // bin ranges: at most K4_MAX_LANE_BINS terms per lane, and enough CTAs
+    // for a few waves when there are few records
+    const int64_t ncta_rec = (nrec + K4_WARPS - 1) / K4_WARPS;
+    int64_t nsplit = (nb + 32 * K4_MAX_LANE_BINS - 1) / (32 * K4_MAX_LANE_BINS);
+    if (ncta_rec > 0) nsplit = std::max(nsplit, (int64_t)(8 * ctx->sm_count + ncta_rec - 1) / ncta_rec);
+    nsplit = std::min(nsplit, std::max<int64_t>(1, nb / 256));
+    nsplit = std::min<int64_t>(nsplit, 65535);
+    const int64_t chunk = (((nb + nsplit - 1) / nsplit) + 31) / 32 * 32;
+    nsplit = (nb + chunk - 1) / chunk;
+    const dim3 grid((unsigned)ncta_rec, (unsigned)nsplit);
+    timing_begin(ctx, st);
+    // Minimum CTAs per SM for the register budget: 3 (168 registers, a few
+    // bytes of spill) by default; PBT_K4_MINB=1|2|4 selects another build.
+    static const int minb = [] {
+        const char *e = getenv("PBT_K4_MINB");
+        const int v = e ? atoi(e) : 3;
+        return (v == 1 || v == 2 || v == 4) ? v : 3;
+    }();
+    if (nrec > 0) {
+        auto launch = [&](auto kern) {
+            kern<<<grid, K4_WARPS * 32, 0, st>>>(
+                (const K4Rec *)(base + o_rec), (const int *)(base + o_kind), (const float *)(base + o_fov),
+                nrec, (const K4Bin *)(base + o_bin), (const float4 *)(base + o_gbin), nb, nphi,
+                g.theta_i, chunk, (float)k,
+                (float)(0.5 * k * Rf), (float)(1.0 / Rf), (double *)(base + o_out));
+        };
+        if (fast_diff) {
+            if (minb == 1) launch(k4_adjoint_kernel<true, 1>);
+            else if (minb == 2) launch(k4_adjoint_kernel<true, 2>);
+            else if (minb == 4) launch(k4_adjoint_kernel<true, 4>);
+            else launch(k4_adjoint_kernel<true, 3>);
+        } else {
+            if (minb == 1) launch(k4_adjoint_kernel<false, 1>);
+            else if (minb == 2) launch(k4_adjoint_kernel<false, 2>);
+            else if (minb == 4) launch(k4_adjoint_kernel<false, 4>);
+            else launch(k4_adjoint_kernel<false, 3>);
+        }
+    }
+    timing_end(ctx, st);
+    ctx->launches += nrec > 0 ? 2 : 1;
+    PBT_CUDA_TRY(cudaGetLastError());
+    // FP64 mapping of the per-record sums to the vertices and amplitudes, one
+    // thread per record; the vertex cotangents are added with FP64 atomics
+    if (nrec > 0)
+        k4_map_kernel<<<(unsigned)((nrec + 127) / 128), 128, 0, st>>>(
+            (const double *)(base + o_out), d_h, d_ob, nbeam, d_ob + nbeam, nrec, lambda, nverts,
+            d_gamp, d_gamp + 8 * nbeam, d_gv);
+    ctx->launches += nrec > 0 ? 2 : 0;
+    PBT_CUDA_TRY(cudaGetLastError());
+    PBT_CUDA_TRY(cudaMemcpyAsync(gverts, d_gv, 3 * nverts * 8, cudaMemcpyDeviceToHost, st));
+    if (nbeam) PBT_CUDA_TRY(cudaMemcpyAsync(gbeam, d_gamp, nbeam * 8 * 8, cudaMemcpyDeviceToHost, st));
+    if (next)
+        PBT_CUDA_TRY(cudaMemcpyAsync(gext, d_gamp + 8 * nbeam, next * 8 * 8, cudaMemcpyDeviceToHost, st));
+    PBT_CUDA_TRY(cudaStreamSynchronize(st));
     return PBT_OK;
 }
 
