@@ -40,7 +40,18 @@ EXPORTS = ("pbt_ctx_create", "pbt_ctx_destroy", "pbt_last_error_string", "pbt_ve
            "pbt_graph_kernel_count", "pbt_graph_destroy_c", "pbt_beamlist_writer_open",
            "pbt_beamlist_writer_add", "pbt_beamlist_writer_close", "pbt_beamlist_read",
            "pbt_beamlist_info", "pbt_beamlist_arrays", "pbt_beamlist_free",
-           "pbt_make_far_field_bins_c", "pbt_selftest_bounded_wait_c", "pbt_diff_batch_list_c")
+           "pbt_make_far_field_bins_c", "pbt_selftest_bounded_wait_c", "pbt_diff_batch_list_c",
+           "pbt_particle_create", "pbt_particle_info", "pbt_particle_verts",
+           "pbt_particle_destroy", "pbt_trace_orientation_c", "pbt_trace_sizes", "pbt_trace_copy",
+           "pbt_trace_destroy")
+
+# pbt_trace_params / pbt_trace_energy
+TRACE_PARAMS_DTYPE = np.dtype([("lambda", "<f8"), ("rbi", "<f8"), ("ibi", "<f8"), ("rec", "<i8"),
+                               ("refl", "<i8"), ("thresh_area", "<f8"),
+                               ("thresh_energy", "<f8")])
+TRACE_ENERGY_DTYPE = np.dtype([("abs", "<f8"), ("geo_cross_sec", "<f8"),
+                               ("beam_energy_out", "<f8"), ("ext_energy_out", "<f8"),
+                               ("nbeams", "<i8")])
 
 
 class PbtError(RuntimeError):
@@ -101,6 +112,14 @@ def lib():
         "pbt_set_plan": (C, [P, I32, I32, I64]),
         "pbt_diff_adjoint_c": (C, [P, P, I64, P, I64, P, I64, P, P, I64, P, I64, P, I64, D, I32,
                                    P, P, P, P, P]),
+        "pbt_particle_create": (C, [P, I64, P, P, I64, P, ctypes.POINTER(P)]),
+        "pbt_particle_info": (C, [P, P, P, P, P]),
+        "pbt_particle_verts": (C, [P, P]),
+        "pbt_particle_destroy": (C, [P]),
+        "pbt_trace_orientation_c": (C, [P, P, P, ctypes.POINTER(P)]),
+        "pbt_trace_sizes": (C, [P, P, P]),
+        "pbt_trace_copy": (C, [P, P, P, P, P]),
+        "pbt_trace_destroy": (C, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -33,7 +33,10 @@ HOST_UNITS = {"host_setup.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math", "
                                  "-fPIC", "-std=c++17", "-I" + CSRC, "-I" + INCLUDE,
                                  "-I" + os.path.join(CUDA_HOME, "include")],
               "beamlist.cpp": ["-O2", "-fPIC", "-std=c++17", "-I" + CSRC, "-I" + INCLUDE,
-                               "-I" + os.path.join(CUDA_HOME, "include")]}
+                               "-I" + os.path.join(CUDA_HOME, "include")],
+              "tracer.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
+                             "-std=c++17", "-I" + CSRC, "-I" + INCLUDE,
+                             "-I" + os.path.join(CUDA_HOME, "include")]}
 
 
 def _headers():

@@ -125,12 +125,15 @@ def hex_prism(radius, length, n_side=4, n_len=8, roughness=0.0, seed=0):
     triangles, each basal face a fan of 6 x n_side^2 triangles.  Optional
     Gaussian vertex roughness (standard deviation `roughness`) perturbs the
     interior vertices of every face along the face normal.  Faces are
-    counter-clockwise seen from outside.  Returns a geometry dict."""
+    counter-clockwise seen from outside.  Returns a geometry dict whose
+    "apertures" entry gives each triangle's parent face (1-6 the sides, 7 the
+    top, 8 the bottom), the apertures of the reference's tracer."""
     rng = np.random.default_rng(seed)
     ang = np.arange(6) * np.pi / 3
     corners = np.stack([radius * np.cos(ang), radius * np.sin(ang)], 1)
     verts = []
     faces = []
+    parent = []
 
     def add(p):
         verts.append(p)
@@ -155,6 +158,7 @@ def hex_prism(radius, length, n_side=4, n_len=8, roughness=0.0, seed=0):
                 v00, v10, v01, v11 = idx[i, j], idx[i + 1, j], idx[i, j + 1], idx[i + 1, j + 1]
                 faces.append([v00, v10, v11])
                 faces.append([v00, v11, v01])
+                parent += [k + 1, k + 1]
     # basal faces (fan of triangles subdivided per sector)
     for zsgn in (1.0, -1.0):
         z = zsgn * length / 2
@@ -183,12 +187,16 @@ def hex_prism(radius, length, n_side=4, n_len=8, roughness=0.0, seed=0):
                     if zsgn < 0:
                         t1 = t1[::-1]
                     faces.append(t1)
+                    parent.append(7 if zsgn > 0 else 8)
                     if c < r:
                         t2 = [rows[r][c], rows[r + 1][c + 1], rows[r][c + 1]]
                         if zsgn < 0:
                             t2 = t2[::-1]
                         faces.append(t2)
-    return make_geometry(np.array(verts), faces)
+                        parent.append(7 if zsgn > 0 else 8)
+    geo = make_geometry(np.array(verts), faces)
+    geo["apertures"] = np.array(parent, dtype=np.int64)
+    return geo
 
 
 def facet_normals_areas(verts, face_off, face_vi):

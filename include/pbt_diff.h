@@ -308,6 +308,65 @@ int pbt_beamlist_arrays(const pbt_beamlist *bl, const double **theta, const doub
                         const pbt_output_params **params_in);
 int pbt_beamlist_free(pbt_beamlist *bl);
 
+/* ---------------------------------------------------------------------------
+ * Near-field tracer (host, FP64): the producer of the outbeam lists, for one
+ * orientation at a time.  Replaces the reference's orientation step ahead of
+ * diff_main (src/pbt_seq_mod.f90:165-201): PROT_MPI (src/input_mod.f90:
+ * 1705-1908), make_incident_beam (:2112-2264) and beam_loop_for_speed
+ * (src/beam_loop_mod.f90:1626-1806).  No device memory, no CUDA calls.
+ *
+ * pbt_particle_create prepares a particle as the reference does after reading
+ * it (src/input_mod.f90:2663-2680): vertices v(nverts,3) column-major, faces
+ * as a 0-based offset array plus 1-based vertex indices (triangles only: the
+ * visibility test reads three vertices per face), face_ap the 1-based
+ * aperture of each face (NULL: every face its own aperture, as without an
+ * apertures file).  The centre of mass is moved to the origin.
+ *
+ * pbt_trace_orientation_c rotates the particle by the Euler angles euler[3]
+ * (alpha, beta, gamma in radians; the reference's 'euler' method converts its
+ * degrees and lifts |beta| < 1e-4 degree to 1e-4 first, 'multi' draws
+ * alpha = 2 pi u1, beta = acos(1 - 2 u2), gamma = 2 pi u3), traces it and
+ * keeps the result: the beam outbeams (beam_outbeam_tree), the external-
+ * diffraction outbeams (ext_diff_outbeam_tree, fov = pi/2), the rotated
+ * vertices (the geometry diff_main reads) and the energy record.  Outbeams
+ * are listed in the order a single-threaded run of the reference appends
+ * them, on any number of host threads.  A NaN outbeam amplitude (the
+ * reference stops there, src/beam_loop_mod.f90:1570-1573) gives PBT_ESTATE. */
+typedef struct pbt_particle pbt_particle;
+typedef struct pbt_trace pbt_trace;
+typedef struct pbt_trace_params {
+    double lambda;        /* wavelength (job_params%la) */
+    double rbi, ibi;      /* refractive index, real part > 1 and imaginary part >= 0 */
+    int64_t rec;          /* max recursions (reference default 8) */
+    int64_t refl;         /* max total internal reflections (default 10) */
+    double thresh_area;   /* aperture area threshold for a new beam (default 0.1) */
+    double thresh_energy; /* aperture energy threshold for a new beam (default 1e-4) */
+} pbt_trace_params;
+typedef struct pbt_trace_energy {
+    double abs;             /* absorption cross section (output_parameters%abs) */
+    double geo_cross_sec;   /* illuminated geometric cross section */
+    double beam_energy_out; /* energy of the beam outbeams */
+    double ext_energy_out;  /* energy of the external-diffraction outbeams */
+    int64_t nbeams;         /* beams traced (beam-tree size) */
+} pbt_trace_energy;
+int pbt_particle_create(const double *verts, int64_t nverts, const int64_t *face_off,
+                        const int64_t *face_vi, int64_t nfaces, const int64_t *face_ap,
+                        pbt_particle **out);
+/* counts of the prepared particle and the centre of mass it was moved by */
+int pbt_particle_info(const pbt_particle *p, int64_t *nverts, int64_t *nfaces,
+                      int64_t *napertures, double *com);
+/* the centred vertices, (nverts,3) column-major */
+int pbt_particle_verts(const pbt_particle *p, double *verts);
+int pbt_particle_destroy(pbt_particle *p);
+int pbt_trace_orientation_c(const pbt_particle *p, const double *euler,
+                            const pbt_trace_params *params, pbt_trace **out);
+int pbt_trace_sizes(const pbt_trace *t, int64_t *nbeam, int64_t *next);
+/* copies the outbeams (nbeam, next records), the rotated vertices
+ * ((nverts,3) column-major) and the energy record; NULL skips an output */
+int pbt_trace_copy(const pbt_trace *t, pbt_outbeam *beam, pbt_outbeam *ext, double *verts,
+                   pbt_trace_energy *energy);
+int pbt_trace_destroy(pbt_trace *t);
+
 /* Failure-detection self-test (no counterpart in the reference): launches a
  * device wait on an mbarrier that nothing completes, bounded like every wait of
  * the far-field kernels; it gives up after limit_ms (1..5000) and the call

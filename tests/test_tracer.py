@@ -1,0 +1,194 @@
+"""The near-field tracer (host, FP64; no GPU needed).
+
+The reference's tracer cannot be built here (Fortran), so these checks use
+what the physics and the reference's own energy bookkeeping fix:
+  * on a convex particle with no recursion beyond the first interaction, the
+    outbeams are the Fresnel-reflected incident field and the external-
+    diffraction records are the incident field on the lit faces -- both
+    restated independently below in numpy and compared to 1e-12;
+  * the external-diffraction energy equals the illuminated geometric cross
+    section, and the beam energy (plus absorption) conserves the incident
+    energy to the few per cent the reference's energy checks report;
+  * the lists do not depend on the number of host threads.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from abt_b200 import PbtError, _lib, workloads as W
+from abt_b200 import tracer as T
+from abt_b200.diff import PI_REF
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LAM, RBI = 0.532, 1.31
+
+
+@pytest.fixture(scope="module")
+def smooth():
+    geo = W.hex_prism(5.0, 10.0, n_side=2, n_len=3, roughness=0.0)
+    return geo, T.Particle(geo, geo["apertures"])
+
+
+@pytest.fixture(scope="module")
+def rough():
+    geo = W.hex_prism(10.0, 20.0, n_side=6, n_len=12, roughness=0.1, seed=3)
+    return geo, T.Particle(geo, geo["apertures"])
+
+
+def _faces(V, geo):
+    tri = V[geo["face_vi"] - 1].reshape(-1, 3, 3)
+    n = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 1])
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    mid = tri.mean(axis=1)
+    c = tri - mid[:, None, :]
+    area = 0.5 * sum(np.linalg.norm(np.cross(c[:, k], c[:, (k + 1) % 3]), axis=1)
+                     for k in range(3))
+    return n, mid, area
+
+
+def _ampl(z):
+    """(n, 2, 2) complex from the records' ampl (column-major re/im)."""
+    a = z[:, 0::2] + 1j * z[:, 1::2]
+    return np.stack([np.stack([a[:, 0], a[:, 2]], 1), np.stack([a[:, 1], a[:, 3]], 1)], 1)
+
+
+def test_particle_is_centred(rough):
+    geo, P = rough
+    assert P.napertures == 8
+    V = P.geometry["verts"]
+    assert np.allclose(V + P.com, geo["verts"], atol=1e-12)
+    _, mid, area = _faces(V, geo)
+    com = (mid * area[:, None]).sum(0) / area.sum()
+    assert np.abs(com).max() < 1e-9
+
+
+@pytest.mark.parametrize("euler", [(0.4, 0.9, 1.3), (2.1, 2.3, 0.2), (5.0, 1.2, 4.1)])
+def test_first_interaction_matches_independent_restatement(smooth, euler):
+    """rec = 0: every outbeam is the first external reflection.  Restated here
+    from the physics: lit faces face the incidence (aperture normal z >= 0.01),
+    path phase from the incident plane z = 1000, e-perp rotation into
+    vk7 = n x prop, Fresnel r_p, r_s with real Snell's law, mirror direction,
+    fov = 8 lambda / d of the lit aperture area."""
+    geo, P = smooth
+    V, beam, ext, pin, en = T.trace(P, np.array(euler), LAM, RBI, rec=0)
+    n, mid, area = _faces(V, geo)
+    ap = geo["apertures"] - 1
+    apn = np.zeros((8, 3))
+    np.add.at(apn, ap, n)
+    apn /= np.linalg.norm(apn, axis=1, keepdims=True)
+    lit = np.nonzero(apn[ap, 2] >= np.float32(0.01))[0]
+    inc = np.array([0.0, 0.0, -1.0])
+    k = 2 * PI_REF / LAM
+    vk7 = np.cross(n[lit], inc)
+    vk7 /= np.linalg.norm(vk7, axis=1, keepdims=True)
+    evo2 = np.cross(inc, [1.0, 0.0, 0.0])
+    c, s = vk7[:, 0], vk7 @ evo2
+    rot = np.stack([np.stack([c, -s], 1), np.stack([s, c], 1)], 1) / np.sqrt(np.abs(c * c + s * s))[:, None, None]
+    A = rot * np.exp(1j * k * (1000.0 - mid[lit, 2]))[:, None, None]
+    # external diffraction: the incident field on every lit face, in face order
+    assert np.array_equal(ext["fi"], lit + 1)
+    assert np.allclose(_ampl(ext["ampl"]), A, rtol=0, atol=1e-12)
+    assert np.allclose(ext["vk7"], vk7, atol=1e-12)
+    assert np.all(ext["prop_out"] == inc)
+    # first reflections, aperture by aperture
+    ti = np.arccos(apn[ap[lit], 2])
+    tt = np.arcsin(np.sin(ti) / RBI)
+    rs = (np.cos(ti) - RBI * np.cos(tt)) / (np.cos(ti) + RBI * np.cos(tt))
+    rp = (RBI * np.cos(ti) - np.cos(tt)) / (np.cos(tt) + RBI * np.cos(ti))
+    R = np.stack([rp, rs], 1)[:, :, None] * A
+    a3 = apn[ap[lit]]
+    mirror = np.stack([2 * a3[:, 2] * a3[:, 0], 2 * a3[:, 2] * a3[:, 1],
+                       -1 + 2 * a3[:, 2] * a3[:, 2]], 1)
+    order, fov = [], []
+    for a in range(8):
+        sel = np.nonzero(ap[lit] == a)[0]
+        if area[lit[sel]].sum() > 0.1:
+            order.extend(sel)
+            fov += [8 * LAM / (2 * np.sqrt(area[lit[sel]].sum() / PI_REF))] * len(sel)
+    order = np.array(order)
+    assert len(beam) == len(order) > 0
+    assert np.array_equal(beam["fi"], lit[order] + 1)
+    assert np.allclose(_ampl(beam["ampl"]), R[order], rtol=0, atol=1e-12)
+    assert np.allclose(beam["prop_out"], mirror[order], atol=1e-12)
+    assert np.allclose(beam["vk7"], vk7[order], atol=1e-12)
+    assert np.allclose(beam["fov"], fov, rtol=1e-12)
+    # cross sections of this orientation
+    geo_cs = (area[lit] * n[lit, 2]).sum()
+    assert pin["geo_cross_sec"] == pytest.approx(geo_cs, rel=1e-12)
+    assert en["ext_energy_out"] == pytest.approx(geo_cs, rel=1e-12)
+
+
+@pytest.mark.parametrize("euler", [(0.3, 0.7, 0.2), (1.0, 2.0, 0.5), (4.4, 1.57, 2.9)])
+def test_energy_is_conserved(rough, euler):
+    geo, P = rough
+    V, beam, ext, pin, en = T.trace(P, np.array(euler), LAM, RBI)
+    gcs = en["geo_cross_sec"]
+    assert en["ext_energy_out"] == pytest.approx(gcs, rel=1e-12)
+    assert 0.97 < en["beam_energy_out"] / gcs < 1.03
+    assert en["abs"] == 0.0 and len(beam) > len(ext) > 0
+    assert np.all((beam["fi"] >= 1) & (beam["fi"] <= len(geo["face_off"]) - 1))
+    assert np.allclose(np.linalg.norm(beam["prop_out"], axis=1), 1.0, atol=1e-12)
+    # outgoing beams leave through the face they are emitted from
+    n, _, _ = _faces(V, geo)
+    assert np.all((beam["prop_out"] * n[beam["fi"] - 1]).sum(1) > -0.2)
+    # absorbing: what is not absorbed leaves
+    _, beam2, _, pin2, en2 = T.trace(P, np.array(euler), LAM, RBI, ibi=1e-3)
+    assert en2["abs"] > 0 and pin2["abs"] == en2["abs"]
+    assert 0.97 < (en2["beam_energy_out"] + en2["abs"]) / gcs < 1.03
+    assert en2["beam_energy_out"] < en["beam_energy_out"]
+
+
+def test_recursion_limit_and_thresholds(rough):
+    geo, P = rough
+    e = np.array([0.5, 1.1, 0.3])
+    counts = [T.trace(P, e, LAM, RBI, rec=r)[4]["nbeams"] for r in (0, 2, 4, 8)]
+    assert counts[0] < counts[1] < counts[2] < counts[3]
+    _, beam, ext, _, en = T.trace(P, e, LAM, RBI, thresh_area=1e9)
+    assert len(beam) == 0 and en["nbeams"] == 0 and len(ext) > 0
+
+
+def test_same_lists_on_one_thread(rough):
+    """The lists are built in beam order whatever the number of host threads."""
+    geo, P = rough
+    e = np.array([1.7, 0.8, 2.2])
+    V, beam, ext, pin, en = T.trace(P, e, LAM, RBI, ibi=1e-3)
+    code = ("import numpy as np, sys; sys.path.insert(0, %r)\n"
+            "from abt_b200 import workloads as W, tracer as T\n"
+            "g = W.hex_prism(10.0, 20.0, n_side=6, n_len=12, roughness=0.1, seed=3)\n"
+            "P = T.Particle(g, g['apertures'])\n"
+            "V, b, x, p, e = T.trace(P, np.array([1.7, 0.8, 2.2]), 0.532, 1.31, ibi=1e-3)\n"
+            "sys.stdout.buffer.write(b.tobytes() + x.tobytes() + V.tobytes() + e.tobytes())\n"
+            % ROOT)
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True,
+                         check=True).stdout
+    assert out == beam.tobytes() + ext.tobytes() + V.tobytes() + en.tobytes()
+
+
+def test_euler_helpers():
+    e = T.euler_from_degrees(30, 0, 10)
+    assert e[1] == 1e-4 * PI_REF / 180.0 and e[0] == 30 * PI_REF / 180.0
+    m = T.multi_euler(0.25, 0.5, 0.75)
+    assert m[0] == 2 * PI_REF * 0.25 and m[1] == np.arccos(0.0)
+
+
+def test_bad_input_is_rejected(rough):
+    geo, P = rough
+    quad = dict(verts=np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0.]]),
+                face_off=np.array([0, 4]), face_vi=np.array([1, 2, 3, 4]))
+    with pytest.raises(PbtError, match="triangles"):
+        T.Particle(quad)
+    with pytest.raises(PbtError, match="aperture"):
+        T.Particle(geo, np.zeros(len(geo["face_off"]) - 1, dtype=np.int64))
+    bad = dict(geo, verts=geo["verts"].copy())
+    bad["verts"][3, 1] = np.nan
+    with pytest.raises(PbtError, match="not finite"):
+        T.Particle(bad)
+    with pytest.raises(PbtError) as e:
+        T.trace(P, np.array([0.1, 0.2, 0.3]), LAM, 0.9)
+    assert e.value.status == _lib.PBT_EINVAL
+    with pytest.raises(PbtError):
+        T.trace(P, np.array([0.1, np.inf, 0.3]), LAM, RBI)
