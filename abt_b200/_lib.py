@@ -42,8 +42,8 @@ EXPORTS = ("pbt_ctx_create", "pbt_ctx_destroy", "pbt_last_error_string", "pbt_ve
            "pbt_beamlist_info", "pbt_beamlist_arrays", "pbt_beamlist_free",
            "pbt_make_far_field_bins_c", "pbt_selftest_bounded_wait_c", "pbt_diff_batch_list_c",
            "pbt_particle_create", "pbt_particle_info", "pbt_particle_verts",
-           "pbt_particle_destroy", "pbt_trace_orientation_c", "pbt_trace_sizes", "pbt_trace_copy",
-           "pbt_trace_destroy")
+           "pbt_particle_destroy", "pbt_trace_orientation_c", "pbt_trace_batch_c", "pbt_trace_sizes",
+           "pbt_trace_copy", "pbt_trace_destroy")
 
 # pbt_trace_params / pbt_trace_energy
 TRACE_PARAMS_DTYPE = np.dtype([("lambda", "<f8"), ("rbi", "<f8"), ("ibi", "<f8"), ("rec", "<i8"),
@@ -117,6 +117,7 @@ def lib():
         "pbt_particle_verts": (C, [P, P]),
         "pbt_particle_destroy": (C, [P]),
         "pbt_trace_orientation_c": (C, [P, P, P, ctypes.POINTER(P)]),
+        "pbt_trace_batch_c": (C, [P, I64, P, P, P]),
         "pbt_trace_sizes": (C, [P, P, P]),
         "pbt_trace_copy": (C, [P, P, P, P, P]),
         "pbt_trace_destroy": (C, [P]),

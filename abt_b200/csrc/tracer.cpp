@@ -40,6 +40,7 @@
 #include <algorithm>
 #include <memory>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "frame.h"
@@ -352,7 +353,8 @@ enum VisKind { VIS_INC, VIS_INT, VIS_EXT };
 // the beam (closest such j); another aperture's face in front of it blocks it.
 // Candidate blockers are the faces with a vertex nearest to the 4 x 4 bucket
 // nearest to m's centroid, visited in face order as the reference does.
-void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, Vis &out) {
+void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, bool par,
+              Vis &out) {
     const int64_t nf = g.nf;
     // buckets (beam_aligned_bounding_boxes, :2668-2743), midpoints of 4 corners
     double mnx = R.v[0], mxx = R.v[0], mny = R.v[1], mxy = R.v[1];
@@ -391,7 +393,7 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
     std::vector<std::vector<int64_t>> members(kBB * kBB);
     {
         std::vector<unsigned> f5(nf);
-#pragma omp parallel for schedule(static) if (nf > 4096)
+#pragma omp parallel for schedule(static) if (par && nf > 4096)
         for (int64_t f = 0; f < nf; f++) {
             f3[f] = nearest(R.mid[3 * f], R.mid[3 * f + 1]);
             unsigned m = 0;
@@ -434,7 +436,7 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
         if (kind == VIS_INT ? nz >= 0 : nz <= 0) out.is_shad[f] = 1;
     }
     const double esign = kind == VIS_EXT ? -1.0 : 1.0;
-#pragma omp parallel for schedule(dynamic, 64) if (nf > 256)
+#pragma omp parallel for schedule(dynamic, 64) if (par && nf > 256)
     for (int64_t m = 0; m < nf; m++) {
         if (!is_vis[m]) continue;
         const double apz = R.apn[3 * g.ap[m] + 2];
@@ -574,6 +576,7 @@ void fresnel_outside(double ti, double tt, Z m, Z fr[2][2], Z ft[2][2]) {
 struct Params {
     double lambda, rbi, ibi, thresh_area, thresh_energy;
     int64_t rec, refl;
+    bool par;  // spread one orientation's work over the host threads
 };
 
 // recursion_inc (src/beam_loop_mod.f90:424-612): the incident beam on the
@@ -592,7 +595,7 @@ void propagate_inc(const Shape &g, const Params &P, std::vector<FieldOut> &fo,
     inc.prop[1] = 0.0;
     inc.prop[2] = -1.0;
     Vis vis;
-    find_vis(g, R, inc, VIS_INC, vis);
+    find_vis(g, R, inc, VIS_INC, P.par, vis);
     const double prop[3] = {0.0, 0.0, -1.0}, e_perp_inc[3] = {1.0, 0.0, 0.0};
     for (int64_t i = 0; i < g.nf; i++) {
         if (!vis.in_beam[i]) continue;
@@ -651,7 +654,7 @@ void propagate_int(const Shape &g, const Params &P, Beam &beam, std::vector<Fiel
     Rotated R;
     rotate_shape(g, rot, R);
     Vis vis;
-    find_vis(g, R, beam, VIS_INT, vis);
+    find_vis(g, R, beam, VIS_INT, P.par, vis);
     double prop_ext_prev[3] = {0.0, 0.0, 0.0};  // left over from the previous face on TIR
     for (int64_t i = 0; i < g.nf; i++) {
         if (!vis.in_beam[i]) continue;
@@ -718,7 +721,7 @@ void propagate_ext(const Shape &g, const Params &P, Beam &beam, std::vector<Fiel
     Rotated R;
     rotate_shape(g, rot, R);
     Vis vis;
-    find_vis(g, R, beam, VIS_EXT, vis);
+    find_vis(g, R, beam, VIS_EXT, P.par, vis);
     for (int64_t j = 0; j < g.nf; j++)
         if (vis.in_beam[j]) beam.in[vis.id_beam[j]].is_outgoing = false;
     for (int64_t i = 0; i < g.nf; i++) {
@@ -995,29 +998,32 @@ extern "C" int pbt_particle_destroy(pbt_particle *p) {
     return PBT_OK;
 }
 
-extern "C" int pbt_trace_orientation_c(const pbt_particle *p, const double *euler,
-                                       const pbt_trace_params *prm, pbt_trace **out) {
-    if (!out) {
-        set_error("pbt_trace_orientation_c: NULL output handle");
-        return PBT_EINVAL;
-    }
-    *out = nullptr;
-    if (!p || !euler || !prm) {
-        set_error("pbt_trace_orientation_c: NULL argument");
+namespace {
+
+int check_trace_args(const pbt_particle *p, const double *euler, int64_t n,
+                     const pbt_trace_params *prm, const char *who) {
+    if (!p || (n > 0 && !euler) || !prm) {
+        set_error("%s: NULL argument", who);
         return PBT_EINVAL;
     }
     if (!(prm->lambda > 0) || !isfinite(prm->lambda) || !(prm->rbi > 1.0) ||
         !isfinite(prm->rbi) || !(prm->ibi >= 0) || !isfinite(prm->ibi) || prm->rec < 0 ||
         prm->refl < 0 || !isfinite(prm->thresh_area) || !isfinite(prm->thresh_energy)) {
-        set_error("pbt_trace_orientation_c: bad parameters (need lambda > 0, rbi > 1, ibi >= 0, "
-                  "rec >= 0, refl >= 0, finite thresholds)");
+        set_error("%s: bad parameters (need lambda > 0, rbi > 1, ibi >= 0, rec >= 0, "
+                  "refl >= 0, finite thresholds)",
+                  who);
         return PBT_EINVAL;
     }
-    for (int k = 0; k < 3; k++)
+    for (int64_t k = 0; k < 3 * n; k++)
         if (!isfinite(euler[k])) {
-            set_error("pbt_trace_orientation_c: Euler angle %d is not finite", k + 1);
+            set_error("%s: Euler angle %lld of orientation %lld is not finite", who,
+                      (long long)(k % 3 + 1), (long long)(k / 3 + 1));
             return PBT_EINVAL;
         }
+    return PBT_OK;
+}
+
+Params make_params(const pbt_trace_params *prm, bool par) {
     Params P;
     P.lambda = prm->lambda;
     P.rbi = prm->rbi;
@@ -1026,11 +1032,13 @@ extern "C" int pbt_trace_orientation_c(const pbt_particle *p, const double *eule
     P.refl = prm->refl;
     P.thresh_area = prm->thresh_area;
     P.thresh_energy = prm->thresh_energy;
-    std::unique_ptr<pbt_trace> tr(new (std::nothrow) pbt_trace);
-    if (!tr) {
-        set_error("pbt_trace_orientation_c: out of host memory");
-        return PBT_ENOMEM;
-    }
+    P.par = par;
+    return P;
+}
+
+// One orientation: PROT_MPI, make_incident_beam, beam_loop_for_speed and
+// energy_checks into tr.
+int trace_one(const pbt_particle *p, const double *euler, const Params &P, pbt_trace *tr) {
     try {
         // PROT_MPI: rotate the vertices, recompute midpoints, normals, apertures
         Shape g = p->g;
@@ -1062,7 +1070,7 @@ extern "C" int pbt_trace_orientation_c(const pbt_particle *p, const double *eule
             std::vector<std::vector<FieldOut>> fo(hi - lo);
             // many beams: one per thread; few: one at a time, each with
             // the visibility test spread over the threads
-            const bool outer = hi - lo >= (size_t)omp_get_max_threads();
+            const bool outer = P.par && hi - lo >= (size_t)omp_get_max_threads();
 #pragma omp parallel for schedule(dynamic, 1) if (outer)
             for (size_t j = lo; j < hi; j++) {
                 if (tree[j].is_int)
@@ -1082,8 +1090,7 @@ extern "C" int pbt_trace_orientation_c(const pbt_particle *p, const double *eule
                     emit(g, P, b, tr->beam);
                 }
                 if ((int64_t)tree.size() > kMaxBeams) {
-                    set_error("pbt_trace_orientation_c: beam tree exceeds %lld beams",
-                              (long long)kMaxBeams);
+                    set_error("tracer: beam tree exceeds %lld beams", (long long)kMaxBeams);
                     return PBT_ESTATE;
                 }
             }
@@ -1095,8 +1102,7 @@ extern "C" int pbt_trace_orientation_c(const pbt_particle *p, const double *eule
             const pbt_outbeam &o = tr->beam[i];
             const double oi = outbeam_intensity(o);
             if (isnan(oi)) {
-                set_error("pbt_trace_orientation_c: outbeam %lld has a NaN amplitude",
-                          (long long)(i + 1));
+                set_error("tracer: outbeam %lld has a NaN amplitude", (long long)(i + 1));
                 return PBT_ESTATE;
             }
             const int64_t f = o.fi - 1;
@@ -1115,10 +1121,72 @@ extern "C" int pbt_trace_orientation_c(const pbt_particle *p, const double *eule
         for (int64_t i = 0; i < g.nv; i++)
             for (int c = 0; c < 3; c++) tr->verts[i + g.nv * c] = g.v[3 * i + c];
     } catch (const std::bad_alloc &) {
+        set_error("tracer: out of host memory");
+        return PBT_ENOMEM;
+    }
+    return PBT_OK;
+}
+
+}  // namespace
+
+extern "C" int pbt_trace_orientation_c(const pbt_particle *p, const double *euler,
+                                       const pbt_trace_params *prm, pbt_trace **out) {
+    if (!out) {
+        set_error("pbt_trace_orientation_c: NULL output handle");
+        return PBT_EINVAL;
+    }
+    *out = nullptr;
+    int st = check_trace_args(p, euler, 1, prm, "pbt_trace_orientation_c");
+    if (st != PBT_OK) return st;
+    std::unique_ptr<pbt_trace> tr(new (std::nothrow) pbt_trace);
+    if (!tr) {
         set_error("pbt_trace_orientation_c: out of host memory");
         return PBT_ENOMEM;
     }
+    st = trace_one(p, euler, make_params(prm, true), tr.get());
+    if (st != PBT_OK) return st;
     *out = tr.release();
+    return PBT_OK;
+}
+
+extern "C" int pbt_trace_batch_c(const pbt_particle *p, int64_t n, const double *euler,
+                                 const pbt_trace_params *prm, pbt_trace **out) {
+    if (!out || n < 0) {
+        set_error("pbt_trace_batch_c: NULL output array or negative count");
+        return PBT_EINVAL;
+    }
+    for (int64_t i = 0; i < n; i++) out[i] = nullptr;
+    int st = check_trace_args(p, euler, n, prm, "pbt_trace_batch_c");
+    if (st != PBT_OK) return st;
+    const Params P = make_params(prm, false);
+    std::vector<int> status(n, PBT_OK);
+    std::vector<std::string> msg(n);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t i = 0; i < n; i++) {
+        pbt_trace *tr = new (std::nothrow) pbt_trace;
+        if (!tr) {
+            status[i] = PBT_ENOMEM;
+            msg[i] = "out of host memory";
+            continue;
+        }
+        status[i] = trace_one(p, euler + 3 * i, P, tr);
+        if (status[i] != PBT_OK) {
+            msg[i] = pbt::last_error();
+            delete tr;
+        } else {
+            out[i] = tr;
+        }
+    }
+    for (int64_t i = 0; i < n; i++)
+        if (status[i] != PBT_OK) {
+            for (int64_t j = 0; j < n; j++) {
+                delete out[j];
+                out[j] = nullptr;
+            }
+            set_error("pbt_trace_batch_c: orientation %lld: %s", (long long)(i + 1),
+                      msg[i].c_str());
+            return status[i];
+        }
     return PBT_OK;
 }
 

@@ -11,6 +11,8 @@ reference's orientation step ahead of diff_main (src/pbt_seq_mod.f90:165-201):
                                   rotated vertices, beam outbeams, external-
                                   diffraction outbeams and the params record
                                   finalise reads (abs, geo_cross_sec, energies)
+  trace_batch(particle, eulers)   the same for many orientations, one per host
+                                  thread
   euler_from_degrees(a, b, g)     the 'euler' rotation method's angles
   multi_euler(u1, u2, u3)         the 'multi' method's angles
 
@@ -89,6 +91,20 @@ class Particle:
         self.close()
 
 
+def _collect(L, h, nverts):
+    nb, ne = np.zeros(1, np.int64), np.zeros(1, np.int64)
+    check(L.pbt_trace_sizes(h, ptr(nb), ptr(ne)))
+    beam = np.zeros(int(nb[0]), dtype=OUTBEAM_DTYPE)
+    ext = np.zeros(int(ne[0]), dtype=OUTBEAM_DTYPE)
+    V = np.zeros((nverts, 3), order="F")
+    en = np.zeros((), dtype=TRACE_ENERGY_DTYPE)
+    check(L.pbt_trace_copy(h, ptr(beam), ptr(ext), ptr(V), en.ctypes.data))
+    pin = _params(abs=float(en["abs"]), geo_cross_sec=float(en["geo_cross_sec"]),
+                  beam_energy_out=float(en["beam_energy_out"]),
+                  ext_energy_out=float(en["ext_energy_out"]))
+    return V, beam, ext, pin, en
+
+
 def trace(particle, euler, lam, rbi, ibi=0.0, rec=8, refl=10, thresh_area=0.1,
           thresh_energy=1e-4):
     """One orientation: rotate by euler (radians), trace, and return
@@ -104,16 +120,34 @@ def trace(particle, euler, lam, rbi, ibi=0.0, rec=8, refl=10, thresh_area=0.1,
     h = ctypes.c_void_p()
     check(L.pbt_trace_orientation_c(particle._h, ptr(e), prm.ctypes.data, ctypes.byref(h)))
     try:
-        nb, ne = np.zeros(1, np.int64), np.zeros(1, np.int64)
-        check(L.pbt_trace_sizes(h, ptr(nb), ptr(ne)))
-        beam = np.zeros(int(nb[0]), dtype=OUTBEAM_DTYPE)
-        ext = np.zeros(int(ne[0]), dtype=OUTBEAM_DTYPE)
-        V = np.zeros(particle.geometry["verts"].shape, order="F")
-        en = np.zeros((), dtype=TRACE_ENERGY_DTYPE)
-        check(L.pbt_trace_copy(h, ptr(beam), ptr(ext), ptr(V), en.ctypes.data))
+        return _collect(L, h, particle.geometry["verts"].shape[0])
     finally:
         L.pbt_trace_destroy(h)
-    pin = _params(abs=float(en["abs"]), geo_cross_sec=float(en["geo_cross_sec"]),
-                  beam_energy_out=float(en["beam_energy_out"]),
-                  ext_energy_out=float(en["ext_energy_out"]))
-    return V, beam, ext, pin, en
+
+
+def trace_batch(particle, eulers, lam, rbi, ibi=0.0, rec=8, refl=10, thresh_area=0.1,
+                thresh_energy=1e-4):
+    """Many orientations (eulers: (n,3) radians), one per host thread.  Returns
+    lists (Vs, beams, exts), the params records (n,) and the energy records (n,),
+    each orientation exactly as trace() gives it."""
+    L = _lib.lib()
+    e = np.ascontiguousarray(eulers, dtype=np.float64).reshape(-1, 3)
+    n = e.shape[0]
+    prm = trace_params(lam, rbi, ibi, rec, refl, thresh_area, thresh_energy)
+    hs = (ctypes.c_void_p * max(n, 1))()
+    check(L.pbt_trace_batch_c(particle._h, n, ptr(e), prm.ctypes.data, hs))
+    Vs, beams, exts = [], [], []
+    pins = np.zeros(n, dtype=_params().dtype)
+    ens = np.zeros(n, dtype=TRACE_ENERGY_DTYPE)
+    try:
+        for i in range(n):
+            V, beam, ext, pin, en = _collect(L, hs[i], particle.geometry["verts"].shape[0])
+            Vs.append(V)
+            beams.append(beam)
+            exts.append(ext)
+            pins[i] = pin
+            ens[i] = en
+    finally:
+        for i in range(n):
+            L.pbt_trace_destroy(hs[i])
+    return Vs, beams, exts, pins, ens

@@ -360,6 +360,12 @@ int pbt_particle_verts(const pbt_particle *p, double *verts);
 int pbt_particle_destroy(pbt_particle *p);
 int pbt_trace_orientation_c(const pbt_particle *p, const double *euler,
                             const pbt_trace_params *params, pbt_trace **out);
+/* n orientations (euler: n x 3, alpha beta gamma per orientation) traced in
+ * parallel, one orientation per host thread; out receives n handles, each as
+ * pbt_trace_orientation_c would give it.  On failure none is kept and the
+ * message names the first failing orientation. */
+int pbt_trace_batch_c(const pbt_particle *p, int64_t n, const double *euler,
+                      const pbt_trace_params *params, pbt_trace **out);
 int pbt_trace_sizes(const pbt_trace *t, int64_t *nbeam, int64_t *next);
 /* copies the outbeams (nbeam, next records), the rotated vertices
  * ((nverts,3) column-major) and the energy record; NULL skips an output */

@@ -192,3 +192,19 @@ def test_bad_input_is_rejected(rough):
     assert e.value.status == _lib.PBT_EINVAL
     with pytest.raises(PbtError):
         T.trace(P, np.array([0.1, np.inf, 0.3]), LAM, RBI)
+
+
+def test_batch_equals_single_orientation_traces(rough):
+    geo, P = rough
+    eul = np.array([T.multi_euler(*u) for u in np.random.default_rng(5).uniform(size=(6, 3))])
+    Vs, beams, exts, pins, ens = T.trace_batch(P, eul, LAM, RBI, ibi=1e-4)
+    for i, e in enumerate(eul):
+        V, beam, ext, pin, en = T.trace(P, e, LAM, RBI, ibi=1e-4)
+        assert Vs[i].tobytes() == V.tobytes()
+        assert beams[i].tobytes() == beam.tobytes() and exts[i].tobytes() == ext.tobytes()
+        assert pins[i].tobytes() == pin.tobytes() and ens[i].tobytes() == en.tobytes()
+    bad = eul.copy()
+    bad[4, 2] = np.nan
+    with pytest.raises(PbtError, match="orientation 5"):
+        T.trace_batch(P, bad, LAM, RBI)
+    assert T.trace_batch(P, np.zeros((0, 3)), LAM, RBI)[0] == []
