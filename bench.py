@@ -68,6 +68,8 @@ def parse():
                     help="enqueue each step through the C ABI instead of replaying a CUDA graph")
     ap.add_argument("--orient", type=int, default=1024,
                     help="orientations of the rough-column orientation average (0: skip)")
+    ap.add_argument("--traced-orient", type=int, default=1024,
+                    help="orientations traced on the host and averaged (0: skip)")
     ap.add_argument("--orient-fp64", type=int, default=16,
                     help="orientations timed with the FP64 drop-in and used for the error")
     ap.add_argument("--fast-diff", type=int, default=1,
@@ -178,14 +180,53 @@ def orientation_average(ctx, args):
     timed on the first --orient-fp64 orientations and extrapolated by facet·bin
     count; the error of the averaged Mueller matrix and cross sections is taken
     on those orientations."""
-    import abt_b200
     from abt_b200 import workloads as W
-    from tests.helpers import mueller_rel_err
     geo, Vs, beams, exts, pin = W.rough_column_orientations(args.orient, seed=3)
     th, ph = W.grid_orientation_average()
+    out = {"workload": "rough hexagonal column r 10 um, L 20 um, sigma 0.1 um (1296 triangles), "
+                       "stand-in beam lists, %d orientations uniform on SO(3), 361 theta x 180 phi"
+                       % args.orient}
+    out.update(_average(ctx, args, geo, Vs, beams, exts, pin, th, ph))
+    return out
+
+
+def traced_orientation_average(ctx, args):
+    """The same orientation average on beam lists from the host tracer: the
+    rough column (apertures = its 8 parent faces) traced at --traced-orient
+    orientations uniform on SO(3) with pbt_trace_batch_c (n = 1.31, 8
+    recursions, the reference's thresholds), one orientation per host thread;
+    the tracing is timed on the host cores, then the FP32 batch and the FP64
+    drop-in sample are timed as in orientation_average."""
+    from abt_b200 import tracer as T
+    from abt_b200 import workloads as W
+    g = W.hex_prism(10.0, 20.0, n_side=6, n_len=12, roughness=0.1, seed=3)
+    P = T.Particle(g, g["apertures"])
+    eul = W.uniform_euler(np.random.default_rng(3), args.traced_orient)
+    T.trace_batch(P, eul[:8], LAM, 1.31)
+    t0 = time.perf_counter()
+    Vs, beams, exts, pin, en = T.trace_batch(P, eul, LAM, 1.31)
+    t_trace = time.perf_counter() - t0
+    th, ph = W.grid_orientation_average()
+    ratio = en["beam_energy_out"] / en["geo_cross_sec"]
+    out = {"workload": "rough hexagonal column r 10 um, L 20 um, sigma 0.1 um (1296 triangles, "
+                       "8 apertures), beam lists traced on the host (n = 1.31, rec 8), "
+                       "%d orientations uniform on SO(3), 361 theta x 180 phi" % args.traced_orient,
+           "trace_s": t_trace, "trace_orientations_per_s": args.traced_orient / t_trace,
+           "trace_threads": int(os.cpu_count() or 1),
+           "beams_traced_per_orientation": [int(en["nbeams"].min()), int(en["nbeams"].mean()),
+                                            int(en["nbeams"].max())],
+           "beam_energy_over_geo_cross_section": [float(ratio.min()), float(ratio.mean()),
+                                                  float(ratio.max())]}
+    out.update(_average(ctx, args, P.geometry, Vs, beams, exts, pin, th, ph))
+    return out
+
+
+def _average(ctx, args, geo, Vs, beams, exts, pin, th, ph):
+    from tests.helpers import mueller_rel_err
+    norient = len(beams)
     nb = len(th) * len(ph)
     F = np.array([len(b) + len(e) for b, e in zip(beams, exts)])
-    k = max(1, min(args.orient_fp64, args.orient))
+    k = max(1, min(args.orient_fp64, norient))
     # FP32 batched, all orientations (host API: H2D, one persistent launch per chunk, D2H)
     ctx.diff_batch(beams[:2], exts[:2], Vs[:2], geo, th, ph, LAM, pin[:2], precision="fp32")
     ctx.set_kernel_timing(True)
@@ -214,17 +255,14 @@ def orientation_average(ctx, args):
     t64 = t64k * work / work_k
     perr = max(abs(float(f32[2][n]) - float(f64[2][n])) / abs(float(f64[2][n]))
                for n in ("scatt", "ext", "asymmetry", "back_scatt"))
-    return {"workload": "rough hexagonal column r 10 um, L 20 um, sigma 0.1 um (1296 triangles), "
-                        "stand-in beam lists, %d orientations uniform on SO(3), 361 theta x 180 phi"
-                        % args.orient,
-            "orientations": int(args.orient), "facets_total": int(F.sum()),
+    return {"orientations": int(norient), "facets_total": int(F.sum()),
             "facets_per_orientation": [int(F.min()), int(F.mean()), int(F.max())], "bins": nb,
-            "fp32_batched_s": t32, "fp32_orientations_per_s": args.orient / t32,
+            "fp32_batched_s": t32, "fp32_orientations_per_s": norient / t32,
             "fp32_facet_bin_per_s": work / t32, "fp32_kernel_ms": k32_ms,
             "fp32_main_launches": int(k32_n),
             "fp64_dropin_sample_orientations": k, "fp64_dropin_sample_s": t64k,
             "fp64_dropin_kernel_ms": k64_ms,
-            "fp64_dropin_orientations_per_s": args.orient / t64,
+            "fp64_dropin_orientations_per_s": norient / t64,
             "speedup_fp32_batched_vs_fp64_dropin": t64 / t32,
             "max_rel_mueller_err_vs_fp64": mueller_rel_err(f32[0], f64[0], 1e-6),
             "max_rel_param_err_vs_fp64": perr,
@@ -609,6 +647,8 @@ def main():
 
     if args.orient > 0 and solo:
         extra["orientation_average"] = orientation_average(ctx, args)
+    if args.traced_orient > 0 and solo:
+        extra["orientation_average_traced"] = traced_orientation_average(ctx, args)
 
     if args.diff_orient > 0 and solo:
         extra["differentiation"] = differentiation(ctx, args)

@@ -4,15 +4,18 @@ kernels -> finalise, the reference's per-orientation sequence
 
 Checks the consistency the reference's documentation asks of a result: the
 external-diffraction and beam scattering efficiencies close to 1 for a
-non-absorbing particle on a fine enough grid (README, "far-field bins"), the
-FP32 batch within its error bars of the FP64 drop-in on these lists, and a
-physically sized asymmetry parameter for a hexagonal column."""
+non-absorbing particle with large facets on a fine enough grid (README,
+"far-field bins"; facets a few wavelengths across lose some energy in the
+aperture diffraction itself, about 9 % per facet for 1.3 um^2 triangles at
+0.532 um); the FP64 drop-in on traced lists against the C oracle; the FP32
+batch within its error bars of the FP64 drop-in on a rough column's traced
+lists; a physically sized asymmetry parameter for a hexagonal column."""
 import numpy as np
 import pytest
 
 from abt_b200 import Context, make_angles, workloads as W
 from abt_b200 import tracer as T
-from abt_b200.diff import PI_REF
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -39,17 +42,28 @@ def ctx():
     return Context(0)
 
 
-def test_one_orientation_efficiencies(ctx, traced):
-    geo, Vs, beams, exts, pins = traced
+def test_one_orientation_conserves_energy(ctx):
+    """Smooth column, 144 triangles: 302 beam and 72 external-diffraction
+    outbeams in the orientation below (the C oracle gives beam and external
+    efficiencies 0.974 and 0.997, asymmetry 0.908 on this grid)."""
+    geo = W.hex_prism(10.0, 20.0, n_side=2, n_len=4, roughness=0.0)
+    P = T.Particle(geo, geo["apertures"])
+    V, beam, ext, pin, en = T.trace(P, T.multi_euler(0.2, 0.4, 0.6), LAM, RBI)
     theta = make_angles([0, 180], [0.25])
-    phi = make_angles([0, 358], [2])
-    g = dict(geo, verts=Vs[0])
-    afb, afe = ctx.diff_main(beams[0], exts[0], g, theta, phi, LAM, precision="fp64")
-    mu, mu1, p = ctx.finalise(afb, afe, theta, phi, LAM, pins[0])
-    assert abs(p["scatt_eff_ext_diff"] - 1.0) < 0.03
-    assert abs(p["scatt_eff_beam"] - 1.0) < 0.05
-    assert 0.6 < p["asymmetry"] < 0.95
-    assert p["geo_cross_sec"] == pins[0]["geo_cross_sec"]
+    phi = make_angles([0, 359], [1])
+    g = dict(P.geometry, verts=V)
+    afb, afe = ctx.diff_main(beam, ext, g, theta, phi, LAM, precision="fp64")
+    mu, mu1, p = ctx.finalise(afb, afe, theta, phi, LAM, pin)
+    assert abs(p["scatt_eff_ext_diff"] - 1.0) < 0.02
+    assert abs(p["scatt_eff_beam"] - 1.0) < 0.04
+    assert 0.75 < p["asymmetry"] < 0.95
+    assert p["geo_cross_sec"] == pin["geo_cross_sec"]
+    # the drop-in on traced lists against the C oracle, on a coarser grid
+    th2, ph2 = make_angles([0, 180], [2]), make_angles([0, 356], [4])
+    g64 = ctx.diff_main(beam, ext, g, th2, ph2, LAM, precision="fp64")
+    ref = O.diff_main(th2, ph2, LAM, g, beam, ext, nthreads=8)
+    for a, b in zip(g64, ref):
+        assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max()
 
 
 def test_fp32_batch_on_traced_lists(ctx, traced):
