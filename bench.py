@@ -14,8 +14,9 @@ Also reported: the same metric end to end through the host C ABI
 (pbt_diff_batch_list_c, pinned host buffers, copies inside the timed region)
 and the roofline of the dominant kernel; in single-GPU runs also the
 reference-exact FP64 drop-in's rate, the FP32-vs-FP64 Mueller error on the
-full workload, the further workloads (orientation average, differentiation,
-large column, -fast_diff, adjoint) and a CPU baseline (the C FP64
+full workload, the further workloads (orientation average on stand-in and on
+host-traced beam lists, differentiation, large column, -fast_diff, adjoint)
+and a CPU baseline (the C FP64
 restatement of the reference, all host cores, bounded sample).  N-GPU runs
 (replicas) time the step, e2e and roofline only.
 
@@ -242,13 +243,19 @@ def _average(ctx, args, geo, Vs, beams, exts, pin, th, ph):
             t32, k32_ms = dt, kms
     # FP32 and FP64 on the first k orientations
     f32 = ctx.diff_batch(beams[:k], exts[:k], Vs[:k], geo, th, ph, LAM, pin[:k], precision="fp32")
-    # one untimed FP64 orientation first: the steady state of a per-orientation loop
-    ctx.diff_batch(beams[:1], exts[:1], Vs[:1], geo, th, ph, LAM, pin[:1], precision="fp64")
-    ctx.kernel_time_ms()
-    t0 = time.perf_counter()
-    f64 = ctx.diff_batch(beams[:k], exts[:k], Vs[:k], geo, th, ph, LAM, pin[:k], precision="fp64")
-    t64k = time.perf_counter() - t0
-    k64_ms, _ = ctx.kernel_time_ms()
+    # the FP64 drop-in in its steady state: best of two calls after an untimed
+    # one of the same size (host buffers already allocated and touched)
+    ctx.diff_batch(beams[:k], exts[:k], Vs[:k], geo, th, ph, LAM, pin[:k], precision="fp64")
+    t64k = k64_ms = None
+    for _ in range(2):
+        ctx.kernel_time_ms()
+        t0 = time.perf_counter()
+        f64 = ctx.diff_batch(beams[:k], exts[:k], Vs[:k], geo, th, ph, LAM, pin[:k],
+                             precision="fp64")
+        dt = time.perf_counter() - t0
+        kms, _ = ctx.kernel_time_ms()
+        if t64k is None or dt < t64k:
+            t64k, k64_ms = dt, kms
     ctx.set_kernel_timing(False)
     work = float(F.sum()) * nb
     work_k = float(F[:k].sum()) * nb
