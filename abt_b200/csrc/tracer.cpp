@@ -333,20 +333,43 @@ Mat3 beam_rotation(const double *prop) {
     return r;
 }
 
+// component i of matmul(r, x), summed as the full product does
+inline double row_dot(const Mat3 &r, int i, const double *x) {
+    double s = 0.0;
+    s = s + r.m[i][0] * x[0];
+    s = s + r.m[i][1] * x[1];
+    s = s + r.m[i][2] * x[2];
+    return s;
+}
+
+// The particle in a beam's frame.  The visibility test reads the vertices' x
+// and y, the normals' z, and the midpoints and aperture normals whole; only
+// those components are formed (each exactly as the full rotation forms it).
 void rotate_shape(const Shape &g, const Mat3 &r, Rotated &o) {
     o.v.resize(3 * g.nv);
     o.mid.resize(3 * g.nf);
     o.n.resize(3 * g.nf);
     o.apn.resize(3 * g.na);
-    for (int64_t i = 0; i < g.nv; i++) pbt::mv33(r, &g.v[3 * i], &o.v[3 * i]);
+    for (int64_t i = 0; i < g.nv; i++) {
+        o.v[3 * i] = row_dot(r, 0, &g.v[3 * i]);
+        o.v[3 * i + 1] = row_dot(r, 1, &g.v[3 * i]);
+    }
     for (int64_t f = 0; f < g.nf; f++) {
-        pbt::mv33(r, &g.n[3 * f], &o.n[3 * f]);
+        o.n[3 * f + 2] = row_dot(r, 2, &g.n[3 * f]);
         pbt::mv33(r, &g.mid[3 * f], &o.mid[3 * f]);
     }
     for (int64_t a = 0; a < g.na; a++) pbt::mv33(r, &g.apn[3 * a], &o.apn[3 * a]);
 }
 
 enum VisKind { VIS_INC, VIS_INT, VIS_EXT };
+
+// A triangle seen along -z as a possible blocker: corners, the edge normals of
+// the reference's inside test (edge k from corner k to k+1), centroid height,
+// and whether it faces the incidence (n_z >= 0.01, tested for incidence only)
+struct Blocker {
+    double x[3], y[3], en1[3], en2[3], z;
+    bool up;
+};
 
 // find_vis_inc / find_vis_int / find_vis_ext (src/beam_loop_mod.f90:2037-2609).
 // A face m is lit when its centroid, seen along -z, lies inside a face j of
@@ -369,50 +392,93 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
         xs[i] = kLit1_1 * (mnx + (mxx - mnx) / kBB * (double)i);
         ys[i] = kLit1_1 * (mny + (mxy - mny) / kBB * (double)i);  // the reference divides by the x count
     }
-    double bx[kBB * kBB], by[kBB * kBB];
-    for (int i = 0; i < kBB; i++)
-        for (int j = 0; j < kBB; j++) {
-            // corners (i,j), (i,j+1), (i+1,j+1), (i+1,j)
-            bx[i * kBB + j] = (((xs[i] + xs[i]) + xs[i + 1]) + xs[i + 1]) / 4.0;
-            by[i * kBB + j] = (((ys[j] + ys[j + 1]) + ys[j + 1]) + ys[j]) / 4.0;
-        }
+    // bucket (i,j), corners (i,j), (i,j+1), (i+1,j+1), (i+1,j): its centre's x
+    // depends on i only and its y on j only
+    double cx[kBB], cy[kBB];
+    for (int i = 0; i < kBB; i++) {
+        cx[i] = (((xs[i] + xs[i]) + xs[i + 1]) + xs[i + 1]) / 4.0;
+        cy[i] = (((ys[i] + ys[i + 1]) + ys[i + 1]) + ys[i]) / 4.0;
+    }
+    // minloc over b = 4 i + j of sqrt((cx_i - x)^2 + (cy_j - y)^2), the
+    // reference's distances.  Rounded addition is monotone in each term, so
+    // the smallest sum pairs the smallest x and y terms; only sums within
+    // rounding of it can tie after the (monotone) square root, and then the
+    // first b with the smallest root wins, as minloc picks it.
     auto nearest = [&](double x, double y) {
-        int best = 0;
-        double bd = 0.0;
+        double dx2[kBB], dy2[kBB];
+        for (int i = 0; i < kBB; i++) {
+            const double dx = cx[i] - x, dy = cy[i] - y;
+            dx2[i] = dx * dx;
+            dy2[i] = dy * dy;
+        }
+        int im = 0, jm = 0;
+        for (int i = 1; i < kBB; i++) {
+            if (dx2[i] < dx2[im]) im = i;
+            if (dy2[i] < dy2[jm]) jm = i;
+        }
+        const double smin = dx2[im] + dy2[jm], win = smin * (1.0 + 1e-14);
+        bool alone = true;
+        for (int i = 0; i < kBB; i++) {
+            if (i != im && dx2[i] + dy2[jm] <= win) alone = false;
+            if (i != jm && dx2[im] + dy2[i] <= win) alone = false;
+        }
+        if (alone) return im * kBB + jm;
+        const double rmin = sqrt(smin);
         for (int b = 0; b < kBB * kBB; b++) {
-            const double dx = bx[b] - x, dy = by[b] - y;
-            const double d = sqrt(dx * dx + dy * dy);
-            if (b == 0 || d < bd) {
-                bd = d;
-                best = b;
-            }
+            const double sb = dx2[b / kBB] + dy2[b % kBB];
+            if (sb <= win && (sb == smin || sqrt(sb) == rmin)) return b;
         }
-        return best;
+        return 0;  // not reached for finite coordinates
     };
-    std::vector<int> f3(nf);
-    std::vector<std::vector<int64_t>> members(kBB * kBB);
-    {
-        std::vector<unsigned> f5(nf);
+    // scratch of the calling thread, reused from beam to beam (bound by
+    // reference so that the threads of the loops below share this instance)
+    thread_local std::vector<int> f3_tl, vb_tl;
+    thread_local std::vector<Blocker> bl_tl;
+    thread_local std::vector<int64_t> members_tl[kBB * kBB];
+    thread_local std::vector<char> is_vis_tl;
+    thread_local std::vector<int64_t> map_tl;
+    std::vector<int> &f3 = f3_tl, &vb = vb_tl;
+    std::vector<Blocker> &bl = bl_tl;
+    std::vector<int64_t>(&members)[kBB * kBB] = members_tl;
+    std::vector<char> &is_vis = is_vis_tl;
+    std::vector<int64_t> &map = map_tl;  // face -> index in the beam's field list
+    f3.resize(nf);
+    vb.resize(g.nv);
+    bl.resize(nf);
+    // bucket of every vertex (a face's vertices are tested one by one in the
+    // reference; the answer depends on the coordinates only)
+#pragma omp parallel for schedule(static) if (par && g.nv > 4096)
+    for (int64_t q = 0; q < g.nv; q++) vb[q] = nearest(R.v[3 * q], R.v[3 * q + 1]);
 #pragma omp parallel for schedule(static) if (par && nf > 4096)
-        for (int64_t f = 0; f < nf; f++) {
-            f3[f] = nearest(R.mid[3 * f], R.mid[3 * f + 1]);
-            unsigned m = 0;
-            for (int k = 0; k < 3; k++) {
-                const int64_t q = g.vi[g.off[f] + k];
-                m |= 1u << nearest(R.v[3 * q], R.v[3 * q + 1]);
-            }
-            f5[f] = m;
+    for (int64_t f = 0; f < nf; f++) {
+        f3[f] = nearest(R.mid[3 * f], R.mid[3 * f + 1]);
+        // the face as a blocker: its corners and edge normals in x, y
+        Blocker &B = bl[f];
+        for (int k = 0; k < 3; k++) {
+            const double *v = &R.v[3 * g.vi[g.off[f] + k]];
+            B.x[k] = v[0];
+            B.y[k] = v[1];
         }
-        for (int64_t f = 0; f < nf; f++)
-            for (int b = 0; b < kBB * kBB; b++)
-                if (f5[f] >> b & 1u) members[b].push_back(f);
+        for (int k = 0; k < 3; k++) {
+            const int kn = k == 2 ? 0 : k + 1;
+            B.en2[k] = -B.x[kn] + B.x[k];
+            B.en1[k] = B.y[kn] - B.y[k];
+        }
+        B.z = R.mid[3 * f + 2];
+        B.up = R.n[3 * f + 2] >= kLit0_01;
+    }
+    for (int b = 0; b < kBB * kBB; b++) members[b].clear();
+    for (int64_t f = 0; f < nf; f++) {
+        unsigned m = 0;
+        for (int k = 0; k < 3; k++) m |= 1u << vb[g.vi[g.off[f] + k]];
+        for (; m; m &= m - 1) members[__builtin_ctz(m)].push_back(f);
     }
     out.in_beam.assign(nf, kind == VIS_INC ? 1 : 0);
     out.is_shad.assign(nf, 0);
     out.id_beam.assign(nf, -1);
     out.dist.assign(nf, 0.0);
-    std::vector<char> is_vis(nf, 1);
-    std::vector<int64_t> map(nf, -1);  // face -> index in the beam's field list
+    is_vis.assign(nf, 1);
+    map.assign(nf, -1);
     if (kind != VIS_INC) {
         for (size_t i = 0; i < beam.in.size(); i++) map[beam.in[i].fi] = (int64_t)i;
         // beam extent in x, y (:2126-2160)
@@ -449,19 +515,15 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
         const double mx = R.mid[3 * m], my = R.mid[3 * m + 1], mz = R.mid[3 * m + 2];
         for (const int64_t j : members[f3[m]]) {
             if (j == m) continue;
-            if (kind == VIS_INC && R.n[3 * j + 2] < kLit0_01) continue;  // down-facing blocker
-            const double jz = R.mid[3 * j + 2];
+            const Blocker &B = bl[j];
+            if (kind == VIS_INC && !B.up) continue;  // down-facing blocker
+            const double jz = B.z;
             if (mz > jz) continue;  // j behind m
+            // m's centroid inside j's outline, edge by edge
             bool inside = true;
-            const int64_t b = g.off[j], e = g.off[j + 1];
-            for (int64_t q = b; q < e; q++) {
-                const int64_t qn = (q + 1 < e) ? q + 1 : b;
-                const double *vk = &R.v[3 * g.vi[q]], *vn = &R.v[3 * g.vi[qn]];
-                const double en2 = -vn[0] + vk[0];
-                const double en1 = vn[1] - vk[1];
-                const double b1 = mx - vk[0], b2 = my - vk[1];
-                const double chk = esign * (b1 * en1 + b2 * en2);
-                if (chk > 0) inside = false;
+            for (int k = 0; k < 3 && inside; k++) {
+                const double b1 = mx - B.x[k], b2 = my - B.y[k];
+                if (esign * (b1 * B.en1[k] + b2 * B.en2[k]) > 0) inside = false;
             }
             if (!inside) continue;
             if (kind == VIS_INC) {
@@ -651,7 +713,8 @@ void propagate_int(const Shape &g, const Params &P, Beam &beam, std::vector<Fiel
     const double waveno = 2 * kPiRef / P.lambda;
     const Z m_int = {P.rbi, P.ibi}, m_ext = {1.0, 0.0};
     const Mat3 rot = beam_rotation(beam.prop);
-    Rotated R;
+    thread_local Rotated R_tl;  // reused from beam to beam
+    Rotated &R = R_tl;
     rotate_shape(g, rot, R);
     Vis vis;
     find_vis(g, R, beam, VIS_INT, P.par, vis);
@@ -718,7 +781,8 @@ void propagate_ext(const Shape &g, const Params &P, Beam &beam, std::vector<Fiel
     const double waveno = 2 * kPiRef / P.lambda;
     const Z m_int = {P.rbi, P.ibi}, m_ext = {1.0, 0.0};
     const Mat3 rot = beam_rotation(beam.prop);
-    Rotated R;
+    thread_local Rotated R_tl;  // reused from beam to beam
+    Rotated &R = R_tl;
     rotate_shape(g, rot, R);
     Vis vis;
     find_vis(g, R, beam, VIS_EXT, P.par, vis);
