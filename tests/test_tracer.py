@@ -6,6 +6,9 @@ what the physics and the reference's own energy bookkeeping fix:
     outbeams are the Fresnel-reflected incident field and the external-
     diffraction records are the incident field on the lit faces -- both
     restated independently below in numpy and compared to 1e-12;
+  * up to the light refracted in, propagated once inside and refracted out
+    (visibility buckets, internal Fresnel, thresholds and list order
+    included), a second independent numpy restatement gives the same lists;
   * the external-diffraction energy equals the illuminated geometric cross
     section, and the beam energy (plus absorption) conserves the incident
     energy to the few per cent the reference's energy checks report;
@@ -208,3 +211,195 @@ def test_batch_equals_single_orientation_traces(rough):
     with pytest.raises(PbtError, match="orientation 5"):
         T.trace_batch(P, bad, LAM, RBI)
     assert T.trace_batch(P, np.zeros((0, 3)), LAM, RBI)[0] == []
+
+
+# ---------------------------------------------------------------- second order
+# An independent numpy restatement of the tracer on a convex particle up to the
+# light refracted in, propagated once inside and refracted out (rec = 2,
+# refl = 0: no chains of total internal reflection), following the reference's
+# routines: recursion_inc, add_to_beam_tree_external, recursion_int with
+# find_vis_int (its 4 x 4 bucket prefilter included), add_to_beam_tree_internal,
+# recursion_ext and add_to_outbeam_tree (src/beam_loop_mod.f90).  On a convex
+# particle no external beam meets the particle again.
+
+F01 = float(np.float32(0.01))
+F11 = float(np.float32(1.1))
+
+
+def _snell(ti, n1, n2):
+    # get_theta_t_complex for real indices
+    return np.arcsin(np.sin(ti) / np.sqrt(np.sin(ti) ** 2 + (n2 / n1) ** 2 * (1 - np.sin(ti) ** 2 * (n1 / n2) ** 2)))
+
+
+def _trans_prop(ti, tt, prop, norm):
+    if tt < float(np.float32(1e-5)):
+        a, b = 0.25, 0.75
+    else:
+        a, b = np.sin(tt - ti) / np.sin(ti), np.sin(PI_REF - tt) / np.sin(ti)
+    p = b * prop - a * norm
+    return p / np.linalg.norm(p)
+
+
+def _rot2(vk7, ev1, ev3):
+    c = vk7 @ ev1
+    evo2 = np.cross(ev3, ev1)
+    evo2 /= np.linalg.norm(evo2)
+    s = vk7 @ evo2
+    return np.array([[c, -s], [s, c]]) / np.sqrt(abs(c * c + s * s))
+
+
+def _beam_frame(prop):
+    t1 = 2 * PI_REF - np.arctan2(prop[1], prop[0])
+    r1 = np.array([[np.cos(t1), -np.sin(t1), 0], [np.sin(t1), np.cos(t1), 0], [0, 0, 1.0]])
+    t = r1 @ prop
+    t2 = np.arccos(-(t / np.linalg.norm(t))[2])
+    r2 = np.array([[np.cos(t2), 0, np.sin(t2)], [0, 1.0, 0], [-np.sin(t2), 0, np.cos(t2)]])
+    return r2 @ r1
+
+
+def _buckets(vx, vy, px, py):
+    """Index of the nearest of the 4 x 4 bucket centres (first on ties)."""
+    xs = F11 * (vx.min() + (vx.max() - vx.min()) / 4 * np.arange(5))
+    ys = F11 * (vy.min() + (vy.max() - vy.min()) / 4 * np.arange(5))
+    cx = (xs[:4] + xs[:4] + xs[1:] + xs[1:]) / 4
+    cy = (ys[:4] + ys[1:] + ys[1:] + ys[:4]) / 4
+    d = np.sqrt((cx[:, None, None] - px) ** 2 + (cy[None, :, None] - py) ** 2).reshape(16, -1)
+    return np.argmin(d, axis=0)
+
+
+def _second_order(V, geo, lam, rbi):
+    tri_i = geo["face_vi"].reshape(-1, 3) - 1
+    ap = geo["apertures"] - 1
+    n, mid, area = _faces(V, geo)
+    na = ap.max() + 1
+    apn = np.zeros((na, 3))
+    np.add.at(apn, ap, n)
+    apn /= np.linalg.norm(apn, axis=1, keepdims=True)
+    k = 2 * PI_REF / lam
+    inc = np.array([0.0, 0.0, -1.0])
+    ident = np.eye(2, dtype=complex)
+    out = []
+
+    def fresnel_outside(ti, tt):
+        ci, ct = np.cos(ti), np.cos(tt)
+        return np.diag([(rbi * ci - ct) / (ct + rbi * ci), (ci - rbi * ct) / (ci + rbi * ct)]), \
+            np.diag([2 * ci / (ct + rbi * ci), 2 * ci / (ci + rbi * ct)])
+
+    # incidence: lit faces (convex: no blockers), in face order
+    lit = [i for i in range(len(ap)) if apn[ap[i], 2] >= F01]
+    fo = []
+    for i in lit:
+        an = apn[ap[i]]
+        vk7 = np.cross(n[i], inc)
+        vk7 /= np.linalg.norm(vk7)
+        A = _rot2(vk7, np.array([1.0, 0, 0]), inc) @ (ident * np.exp(1j * k * (1000.0 - mid[i, 2])))
+        ti = np.arccos(an[2])
+        fr, ft = fresnel_outside(ti, _snell(ti, 1.0, rbi))
+        tt = _snell(ti, 1.0, rbi)
+        fo.append(dict(fi=i, ap=ap[i], e_perp=vk7, a_ext=fr @ A, a_int=ft @ A,
+                       p_int=_trans_prop(ti, tt, inc, -an),
+                       p_ext=np.array([2 * an[2] * an[0], 2 * an[2] * an[1], -1 + 2 * an[2] ** 2])))
+    # add_to_beam_tree_external: per aperture with enough area, internal then external
+    tree = []
+    for a in range(na):
+        fa = [o for o in fo if o["ap"] == a]
+        if sum(area[o["fi"]] for o in fa) > 0.1:
+            tree.append(dict(int=True, rec=1, fields=[(o["fi"], o["a_int"], o["e_perp"], False) for o in fa],
+                             prop=fa[-1]["p_int"]))
+            tree.append(dict(int=False, rec=1, fields=[(o["fi"], o["a_ext"], o["e_perp"], True) for o in fa],
+                             prop=fa[-1]["p_ext"]))
+
+    def emit(beam):
+        d = 2 * np.sqrt(sum(area[f[0]] for f in beam["fields"]) / PI_REF)
+        for fi, a, e, outgoing in beam["fields"]:
+            if outgoing:
+                out.append((fi, a, e, beam["prop"], lam / d * 8))
+
+    children = []
+    for beam in tree:
+        if not beam["int"]:
+            emit(beam)  # convex: external beams leave the particle
+            continue
+        prop = beam["prop"]
+        R = _beam_frame(prop)
+        Vr, nr, midr, apr = V @ R.T, n @ R.T, mid @ R.T, apn @ R.T
+        src = {f[0]: (j, f) for j, f in enumerate(beam["fields"])}
+        bv = np.concatenate([tri_i[f[0]] for f in beam["fields"]])
+        box = (Vr[bv, 0].min(), Vr[bv, 0].max(), Vr[bv, 1].min(), Vr[bv, 1].max())
+        f3 = _buckets(Vr[:, 0], Vr[:, 1], midr[:, 0], midr[:, 1])
+        vb = _buckets(Vr[:, 0], Vr[:, 1], Vr[:, 0], Vr[:, 1])
+        fo = []
+        for m in range(len(ap)):
+            if not (box[0] <= midr[m, 0] <= box[1] and box[2] <= midr[m, 1] <= box[3]):
+                continue
+            if apr[ap[m], 2] > -F01:
+                continue
+            hit, best = None, None
+            for j in range(len(ap)):
+                if j == m or f3[m] not in vb[tri_i[j]] or midr[m, 2] > midr[j, 2]:
+                    continue
+                x, y = Vr[tri_i[j], 0], Vr[tri_i[j], 1]
+                inside = all((midr[m, 0] - x[q]) * (y[(q + 1) % 3] - y[q])
+                             + (midr[m, 1] - y[q]) * (x[q] - x[(q + 1) % 3]) <= 0 for q in range(3))
+                if not inside:
+                    continue
+                if j in src:
+                    if hit is None or midr[j, 2] < midr[src[hit][1][0], 2]:
+                        hit, best = j, midr[j, 2] - midr[m, 2]
+                elif ap[j] != ap[m]:
+                    if hit is not None and midr[j, 2] > midr[src[hit][1][0], 2]:
+                        continue
+                    hit = None
+                    break
+            if hit is None:
+                continue
+            _, (_, a_src, e_src, _) = src[hit]
+            vk7 = np.cross(-n[m], prop)
+            vk7 /= np.linalg.norm(vk7)
+            A = _rot2(vk7, e_src, prop) @ a_src * np.exp(1j * k * rbi * best)
+            ti = np.arccos(-apr[ap[m], 2])
+            ti_f = np.arccos(-nr[m, 2])
+            tir = ti >= np.arcsin(1 / rbi)
+            if tir:
+                fr, ft, tt = -np.eye(2), np.zeros((2, 2)), 0.0
+            else:
+                tt = _snell(ti, rbi, 1.0)
+                ci, ct = np.cos(ti), np.cos(tt)
+                fr = np.diag([(ci - rbi * ct) / (rbi * ct + ci), (rbi * ci - ct) / (rbi * ci + ct)])
+                ft = np.diag([2 * rbi * ci / (rbi * ct + ci), 2 * rbi * ci / (rbi * ci + ct)])
+            refl = fr @ A
+            pr = 0.5 * np.sum(np.abs(refl) ** 2) * area[m] * np.cos(ti_f) * rbi
+            ra = apr[ap[m]]
+            p_int = R.T @ np.array([2 * ra[2] * ra[0], 2 * ra[2] * ra[1], -1 + 2 * ra[2] ** 2])
+            p_ext = None if tir else _trans_prop(ti, tt, prop, n[m])
+            fo.append(dict(fi=m, ap=ap[m], e_perp=vk7, a_int=refl, a_ext=ft @ A, tir=tir,
+                           p_int=p_int, p_ext=p_ext, pr=pr))
+        # add_to_beam_tree_internal (rec 1 < 2): area and energy thresholds
+        for a in range(na):
+            fa = [o for o in fo if o["ap"] == a]
+            if not (sum(area[o["fi"]] for o in fa) > 0.1 and sum(o["pr"] for o in fa) > 1e-4):
+                continue
+            if not any(o["tir"] for o in fa):
+                children.append(dict(int=False, fields=[(o["fi"], o["a_ext"], o["e_perp"], True) for o in fa],
+                                     prop=fa[-1]["p_ext"]))
+    for beam in children:
+        emit(beam)  # convex: the refracted-out light leaves
+    return out
+
+
+@pytest.mark.parametrize("mesh,euler", [((2, 3), (0.4, 0.9, 1.3)), ((2, 3), (2.1, 2.3, 0.2)),
+                                        ((4, 6), (1.1, 1.9, 2.6)), ((4, 6), (5.5, 0.6, 0.9))])
+def test_second_order_matches_independent_restatement(mesh, euler):
+    geo = W.hex_prism(5.0, 10.0, n_side=mesh[0], n_len=mesh[1], roughness=0.0)
+    P = T.Particle(geo, geo["apertures"])
+    V, beam, ext, pin, en = T.trace(P, np.array(euler), LAM, RBI, rec=2, refl=0)
+    n0 = len(T.trace(P, np.array(euler), LAM, RBI, rec=0)[1])
+    assert len(beam) > n0  # refracted-out beams beyond the first reflections
+    g = dict(P.geometry, apertures=geo["apertures"])
+    ref = _second_order(V, g, LAM, RBI)
+    assert len(beam) == len(ref) > 0
+    assert np.array_equal(beam["fi"], [r[0] + 1 for r in ref])
+    assert np.allclose(_ampl(beam["ampl"]), np.array([r[1] for r in ref]), rtol=0, atol=1e-11)
+    assert np.allclose(beam["vk7"], [r[2] for r in ref], atol=1e-12)
+    assert np.allclose(beam["prop_out"], [r[3] for r in ref], atol=1e-12)
+    assert np.allclose(beam["fov"], [r[4] for r in ref], rtol=1e-12)
