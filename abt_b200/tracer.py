@@ -13,6 +13,8 @@ reference's orientation step ahead of diff_main (src/pbt_seq_mod.f90:165-201):
                                   finalise reads (abs, geo_cross_sec, energies)
   trace_batch(particle, eulers)   the same for many orientations, one per host
                                   thread
+  traced_orientation_average(...) trace on the host and average on the GPU,
+                                  overlapped chunk by chunk
   euler_from_degrees(a, b, g)     the 'euler' rotation method's angles
   multi_euler(u1, u2, u3)         the 'multi' method's angles
 
@@ -151,3 +153,51 @@ def trace_batch(particle, eulers, lam, rbi, ibi=0.0, rec=8, refl=10, thresh_area
         for i in range(n):
             L.pbt_trace_destroy(hs[i])
     return Vs, beams, exts, pins, ens
+
+
+def traced_orientation_average(ctx, particle, eulers, theta, phi, lam, rbi, ibi=0.0, rec=8,
+                               refl=10, thresh_area=0.1, thresh_energy=1e-4, chunk=256,
+                               precision="fp32", is_fast_diff=False, scaling=False):
+    """The reference's orientation loop (src/pbt_seq_mod.f90:146-274) with the
+    tracer on the host cores and the far field on the GPU, overlapped: while
+    the GPU averages one chunk of orientations (Context.diff_batch), the host
+    traces the next.  Returns (mueller_avg, mueller_1d_avg, params_avg,
+    params_per_orientation) as Context.diff_batch does for all orientations at
+    once; the chunk averages are combined weighted by their orientation counts
+    in FP64, which differs from one call by rounding only."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    e = np.ascontiguousarray(eulers, dtype=np.float64).reshape(-1, 3)
+    n = e.shape[0]
+    if n == 0:
+        raise ValueError("no orientations")
+    chunk = max(1, int(chunk))
+    starts = list(range(0, n, chunk))
+    geo = particle.geometry
+    mu = mu1 = pavg = None
+    per = []
+
+    def run(s):
+        return trace_batch(particle, e[s:s + chunk], lam, rbi, ibi, rec, refl, thresh_area,
+                           thresh_energy)
+
+    with ThreadPoolExecutor(max_workers=1) as ex:
+        fut = ex.submit(run, starts[0])
+        for c, s in enumerate(starts):
+            Vs, beams, exts, pins, _ = fut.result()
+            if c + 1 < len(starts):
+                fut = ex.submit(run, starts[c + 1])
+            m, m1, pa, pp = ctx.diff_batch(beams, exts, Vs, geo, theta, phi, lam, pins,
+                                           is_fast_diff=is_fast_diff, scaling=scaling,
+                                           precision=precision)
+            w = len(beams) / n
+            if mu is None:
+                mu, mu1 = m * w, m1 * w
+                pavg = np.zeros((), dtype=pa.dtype)
+            else:
+                mu += m * w
+                mu1 += m1 * w
+            for name in pa.dtype.names:
+                pavg[name] = pavg[name] + w * pa[name]
+            per.append(np.atleast_1d(pp))
+    return mu, mu1, pavg, np.concatenate(per)

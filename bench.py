@@ -197,7 +197,10 @@ def traced_orientation_average(ctx, args):
     orientations uniform on SO(3) with pbt_trace_batch_c (n = 1.31, 8
     recursions, the reference's thresholds), one orientation per host thread;
     the tracing is timed on the host cores, then the FP32 batch and the FP64
-    drop-in sample are timed as in orientation_average."""
+    drop-in sample are timed as in orientation_average; last, the whole loop
+    with tracing (host) and averaging (GPU) overlapped chunk by chunk
+    (abt_b200.tracer.traced_orientation_average, FP32, 128 orientations per
+    chunk)."""
     from abt_b200 import tracer as T
     from abt_b200 import workloads as W
     g = W.hex_prism(10.0, 20.0, n_side=6, n_len=12, roughness=0.1, seed=3)
@@ -208,11 +211,18 @@ def traced_orientation_average(ctx, args):
     Vs, beams, exts, pin, en = T.trace_batch(P, eul, LAM, 1.31)
     t_trace = time.perf_counter() - t0
     th, ph = W.grid_orientation_average()
+    # the whole loop with tracing and the GPU average overlapped chunk by chunk
+    T.traced_orientation_average(ctx, P, eul[:64], th, ph, LAM, 1.31, chunk=32)
+    t0 = time.perf_counter()
+    T.traced_orientation_average(ctx, P, eul, th, ph, LAM, 1.31, chunk=128)
+    t_pipe = time.perf_counter() - t0
     ratio = en["beam_energy_out"] / en["geo_cross_sec"]
     out = {"workload": "rough hexagonal column r 10 um, L 20 um, sigma 0.1 um (1296 triangles, "
                        "8 apertures), beam lists traced on the host (n = 1.31, rec 8), "
                        "%d orientations uniform on SO(3), 361 theta x 180 phi" % args.traced_orient,
            "trace_s": t_trace, "trace_orientations_per_s": args.traced_orient / t_trace,
+           "trace_and_average_overlapped_s": t_pipe,
+           "trace_and_average_orientations_per_s": args.traced_orient / t_pipe,
            "trace_threads": int(os.cpu_count() or 1),
            "beams_traced_per_orientation": [int(en["nbeams"].min()), int(en["nbeams"].mean()),
                                             int(en["nbeams"].max())],

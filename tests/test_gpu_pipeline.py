@@ -80,3 +80,23 @@ def test_fp32_batch_on_traced_lists(ctx, traced):
         assert abs(p32[name] - p64[name]) <= 1e-5 * abs(p64[name]), name
     assert 0.6 < p64["asymmetry"] < 0.95
     assert 0.9 < p64["scatt_eff"] / 2.0 < 1.1  # extinction paradox: Q_sca ~ 2
+
+
+def test_overlapped_trace_and_average(ctx):
+    """Tracing chunk c+1 on the host while the GPU averages chunk c gives the
+    single-call average of all orientations (up to the rounding of combining
+    the chunk averages)."""
+    geo = W.hex_prism(10.0, 20.0, n_side=6, n_len=12, roughness=0.1, seed=3)
+    P = T.Particle(geo, geo["apertures"])
+    eul = W.uniform_euler(np.random.default_rng(7), 40)
+    theta = make_angles([0, 180], [1])
+    phi = make_angles([0, 356], [4])
+    Vs, beams, exts, pins, _ = T.trace_batch(P, eul, LAM, RBI)
+    ref = ctx.diff_batch(beams, exts, Vs, P.geometry, theta, phi, LAM, pins, precision="fp64")
+    got = T.traced_orientation_average(ctx, P, eul, theta, phi, LAM, RBI, chunk=16,
+                                       precision="fp64")
+    assert np.allclose(got[0], ref[0], rtol=1e-12, atol=1e-12 * np.abs(ref[0]).max())
+    assert np.allclose(got[1], ref[1], rtol=1e-12, atol=1e-12 * np.abs(ref[1]).max())
+    for name in ("scatt", "ext", "asymmetry", "geo_cross_sec", "beam_energy_out"):
+        assert got[2][name] == pytest.approx(float(ref[2][name]), rel=1e-12)
+    assert got[3].tobytes() == np.atleast_1d(ref[3]).tobytes()
