@@ -1166,7 +1166,11 @@ int trace_one(const pbt_particle *p, const double *euler, const Params &P, pbt_t
             const pbt_outbeam &o = tr->beam[i];
             const double oi = outbeam_intensity(o);
             if (isnan(oi)) {
-                set_error("tracer: outbeam %lld has a NaN amplitude", (long long)(i + 1));
+                set_error("tracer: outbeam %lld has a NaN amplitude (a face normal parallel to "
+                          "a beam direction leaves its e-perp undefined, e.g. an axis-aligned "
+                          "orientation; the reference's 'euler' method lifts beta to 1e-4 "
+                          "degree against this)",
+                          (long long)(i + 1));
                 return PBT_ESTATE;
             }
             const int64_t f = o.fi - 1;

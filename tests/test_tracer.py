@@ -178,6 +178,18 @@ def test_euler_helpers():
     assert m[0] == 2 * PI_REF * 0.25 and m[1] == np.arccos(0.0)
 
 
+def test_axis_aligned_orientation(smooth):
+    """A face normal along the incidence leaves e-perp = n x prop undefined:
+    NaN amplitudes, on which the reference stops (src/beam_loop_mod.f90:1570);
+    the 'euler' method's lift of beta to 1e-4 degree avoids it."""
+    geo, P = smooth
+    with pytest.raises(PbtError, match="NaN amplitude") as e:
+        T.trace(P, np.zeros(3), LAM, RBI)
+    assert e.value.status == _lib.PBT_ESTATE
+    V, beam, ext, pin, en = T.trace(P, T.euler_from_degrees(0, 0, 0), LAM, RBI)
+    assert np.isfinite(beam["ampl"]).all() and np.isfinite(ext["ampl"]).all() and len(beam) > 0
+
+
 def test_bad_input_is_rejected(rough):
     geo, P = rough
     quad = dict(verts=np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0.]]),
