@@ -795,16 +795,18 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     const float2 t3 = fma2(kyy, P.vy[2], fma2(kxx, P.vx[2], ph));
     float2 gx, gy;
     tri_dd_pk(t1, t2, t3, gx, gy);
-    // polarisation matrix [[d, e], [-e, d]] (see k2_record for the forms)
+    // polarisation matrix [[d, e], [-e, d]] (see k2_record for the forms) and
+    // the rotation into the scattering plane, with their normalisations folded
+    // into one factor: with s = sqrt(tt) and hc = h / |h|,
+    //   d = d1 / s, e = e1 / s, p = P1 / (|h| s), rr = R1 / (|h| s),
+    // so A = p d + rr e = sc (P1 d1 + R1 e1) and B = sc (P1 e1 - R1 d1) with
+    // sc = 1 / (|h| tt) = rsqrt(|h|^2 tt^2).
     const float2 kyc = make_float2(fminf(fmaxf(ky.x, -0.999999f), 0.999999f),
                                    fminf(fmaxf(ky.y, -0.999999f), 0.999999f));
     const float2 tr = fma2(kx, kx, mul2(kz, kz));
     const float2 tt = make_float2(fmaxf(tr.x, kOneMinusClampSq), fmaxf(tr.y, kOneMinusClampSq));
-    const float2 rs = make_float2(rsqrtf(tt.x), rsqrtf(tt.y));
-    const float2 s = mul2(tt, rs);
-    const float2 kyrs = mul2(kyc, rs);
-    const float2 d = fma2(P.hkz_cf, s, neg2(mul2(mul2(kz, rs), P.hicf)));
-    const float2 e = fma2(P.hkxky_cf, s, neg2(mul2(mul2(kx, kyrs), P.hicf)));
+    const float2 d1 = fma2(P.hkz_cf, tt, neg2(mul2(kz, P.hicf)));
+    const float2 e1 = fma2(P.hkxky_cf, tt, neg2(mul2(mul2(kx, kyc), P.hicf)));
     float2 qx = kx, qy = kyc, qz = kz;
     const float2 dinc = fma2(P.inc[2], kz, fma2(P.inc[1], kyc, mul2(P.inc[0], kx)));
     const bool bx = !(fabsf(dinc.x) < 0.999f), by = !(fabsf(dinc.y) < 0.999f);
@@ -822,36 +824,34 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
         qy = sel2(bx, by, vy, qy);
         qz = sel2(bx, by, vz, qz);
     }
-    // hc = h / |h| with h = inc x q; p = hc.m, rr = hc.evo2
+    // h = inc x q
     const float2 hx = fma2(P.inc[1], qz, neg2(mul2(P.inc[2], qy)));
     const float2 hy = fma2(P.inc[2], qx, neg2(mul2(P.inc[0], qz)));
     const float2 hz = fma2(P.inc[0], qy, neg2(mul2(P.inc[1], qx)));
     const float2 hn2 = fma2(hz, hz, fma2(hy, hy, mul2(hx, hx)));
-    const float2 hn = make_float2(rsqrtf(hn2.x), rsqrtf(hn2.y));
+    const float2 ht = mul2(mul2(hn2, tt), tt);
+    const float2 sc = make_float2(rsqrtf(ht.x), rsqrtf(ht.y));
+    // P1 = p |h| s = hy tt - ky (hx kx + hz kz), from m = (-kx ky / s, s, -kz ky / s);
+    // inside the clamp evo2 = (-kz, 0, kx) / s, so R1 = rr |h| s = hz kx - hx kz
+    const float2 t = fma2(hx, kx, mul2(hz, kz));
+    const float2 P1 = fma2(hy, tt, neg2(mul2(kyc, t)));
+    float2 R1 = fma2(hz, kx, neg2(mul2(hx, kz)));
     const bool cx = tt.x <= kOneMinusClampSq, cy = tt.y <= kOneMinusClampSq;
-    float2 p, rr;
-    if (!(cx || cy)) {
-        // unit k, |ky| inside the clamp: evo2 = k x m = (-kz, 0, kx) / s, so
-        // p = hy s - (ky/s)(hx kx + hz kz) and rr = (hz kx - hx kz) / s, over |h|
-        const float2 t = fma2(hx, kx, mul2(hz, kz));
-        p = mul2(hn, fma2(hy, s, neg2(mul2(kyrs, t))));
-        rr = mul2(mul2(hn, rs), fma2(hz, kx, neg2(mul2(hx, kz))));
-    } else {
-        // a lane on the clamp: evo2 = normalise(k x m) with the clamped ky
+    if (cx || cy) {
+        // a lane on the clamp: evo2 = normalise(k x m) with the clamped ky, R1 = s (h . evo2)
+        const float2 rs = make_float2(rsqrtf(tt.x), rsqrtf(tt.y));
+        const float2 s = mul2(tt, rs), kyrs = mul2(kyc, rs);
         const float2 m0 = neg2(mul2(kx, kyrs)), m1 = s, m2 = neg2(mul2(kz, kyrs));
         float2 ex = fma2(kyc, m2, neg2(mul2(kz, m1)));
         float2 ey = fma2(kz, m0, neg2(mul2(kx, m2)));
         float2 ez = fma2(kx, m1, neg2(mul2(kyc, m0)));
         const float2 en2 = fma2(ez, ez, fma2(ey, ey, mul2(ex, ex)));
         const float2 ne = make_float2(cx ? rsqrtf(en2.x) : 1.0f, cy ? rsqrtf(en2.y) : 1.0f);
-        ex = mul2(ex, ne);
-        ey = mul2(ey, ne);
-        ez = mul2(ez, ne);
-        p = mul2(hn, fma2(hz, m2, fma2(hy, m1, mul2(hx, m0))));
-        rr = mul2(hn, fma2(hz, ez, fma2(hy, ey, mul2(hx, ex))));
+        const float2 rc = mul2(mul2(s, ne), fma2(hz, ez, fma2(hy, ey, mul2(hx, ex))));
+        R1 = sel2(cx, cy, rc, R1);
     }
-    const float2 A = fma2(p, d, mul2(rr, e));
-    const float2 Bc = fma2(p, e, neg2(mul2(rr, d)));
+    const float2 A = mul2(sc, fma2(P1, d1, mul2(R1, e1)));
+    const float2 Bc = mul2(sc, fma2(P1, e1, neg2(mul2(R1, d1))));
     // [[A, B], [-B, A]] is diagonal in the circular basis: with z = A - iB the
     // columns' u+ take z, their u- take conj(z).  q+ = g z, q- = g conj(z).
     const float2 gyB = mul2(gy, Bc), gxB = mul2(gx, Bc);
