@@ -654,6 +654,23 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
 // three phases and the FP64 phase stay per facet.
 
 __device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+// the special-function unit's approximations with subnormal inputs flushed
+// to zero (the arguments here are phases and squared norms, never subnormal)
+__device__ __forceinline__ float sin_fz(float x) {
+    float r;
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float cos_fz(float x) {
+    float r;
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rsqrt_fz(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
@@ -669,22 +686,14 @@ struct BinPk {
     int64_t bin;           // bin index
 };
 
-// sin(h)/h (h >= 0) with one shared reciprocal: rh = 1/max(h, 0.5)
-// The series is evaluated only when a lane of the warp needs it: small gaps
-// occur near a facet's specular and forward directions, so whole warps of
-// neighbouring bins mostly skip it.  Every lane of the warp calls this.
-__device__ __forceinline__ float2 sinc_pk(float2 h, float2 rh) {
-    float2 q = mul2(make_float2(__sinf(h.x), __sinf(h.y)), rh);
-    const bool sx = h.x < 0.5f, sy = h.y < 0.5f;
-    if (__any_sync(0xffffffffu, sx || sy)) {
-        const float2 h2 = mul2(h, h);
-        const float2 p = fma2(h2, fma2(h2, fma2(h2, fma2(h2, bc2(2.7557319e-6f), bc2(-1.9841270e-4f)),
-                                                bc2(8.3333333e-3f)),
-                                       bc2(-1.6666667e-1f)),
-                              bc2(1.0f));
-        q = sel2(sx, sy, p, q);
-    }
-    return q;
+// Taylor series of sin(h)/h, used below h = 0.5 where the MUFU sine's
+// absolute error would be a large relative one
+__device__ __forceinline__ float2 sinc_series(float2 h) {
+    const float2 hh = mul2(h, h);
+    return fma2(hh, fma2(hh, fma2(hh, fma2(hh, bc2(2.7557319e-6f), bc2(-1.9841270e-4f)),
+                                  bc2(8.3333333e-3f)),
+                         bc2(-1.6666667e-1f)),
+                bc2(1.0f));
 }
 
 // Second divided difference of e^{ix} at the three phases of each lane.
@@ -705,10 +714,10 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
     const float2 h2 = mul2(bc2(0.5f), add2(hi, neg2(mid)));
     const float2 c1 = add2(lo, h1), c2 = add2(mid, h2);
     float2 s1, k1, s2, k2;
-    __sincosf(c1.x, &s1.x, &k1.x);
-    __sincosf(c1.y, &s1.y, &k1.y);
-    __sincosf(c2.x, &s2.x, &k2.x);
-    __sincosf(c2.y, &s2.y, &k2.y);
+    s1 = make_float2(sin_fz(c1.x), sin_fz(c1.y));
+    k1 = make_float2(cos_fz(c1.x), cos_fz(c1.y));
+    s2 = make_float2(sin_fz(c2.x), sin_fz(c2.y));
+    k2 = make_float2(cos_fz(c2.x), cos_fz(c2.y));
     // 1/max(h1,.5), 1/max(h2,.5) and 1/D from one reciprocal of their product
     const float2 a1 = make_float2(fmaxf(h1.x, 0.5f), fmaxf(h1.y, 0.5f));
     const float2 a2 = make_float2(fmaxf(h2.x, 0.5f), fmaxf(h2.y, 0.5f));
@@ -717,8 +726,19 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
     const float2 pr = mul2(p12, Dg);
     const float2 r = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
     const float2 rD = mul2(Dg, r);
-    const float2 sc1 = sinc_pk(h1, mul2(a2, rD));
-    const float2 sc2 = sinc_pk(h2, mul2(a1, rD));
+    // sinc(h1), sinc(h2) with the shared reciprocal (1/max(h, 0.5) = a2 rD,
+    // a1 rD); the series is evaluated only when a lane of the warp needs it
+    // (small gaps occur near a facet's specular and forward directions, so
+    // whole warps of neighbouring bins mostly skip it), one vote for both
+    float2 sc1 = mul2(make_float2(sin_fz(h1.x), sin_fz(h1.y)), mul2(a2, rD));
+    float2 sc2 = mul2(make_float2(sin_fz(h2.x), sin_fz(h2.y)), mul2(a1, rD));
+    {
+        const bool ax = h1.x < 0.5f, ay = h1.y < 0.5f, bx = h2.x < 0.5f, by = h2.y < 0.5f;
+        if (__any_sync(0xffffffffu, ax || ay || bx || by)) {
+            sc1 = sel2(ax, ay, sinc_series(h1), sc1);
+            sc2 = sel2(bx, by, sinc_series(h2), sc2);
+        }
+    }
     const float2 iD = mul2(p12, r);
     gx = mul2(fma2(sc1, s1, neg2(mul2(sc2, s2))), iD);
     gy = mul2(fma2(sc2, k2, neg2(mul2(sc1, k1))), iD);
@@ -739,8 +759,8 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
         const float2 im = fma2(q5, bc2(-1.0f / 5040.0f),
                                fma2(q3, bc2(1.0f / 120.0f), mul2(q1, bc2(-1.0f / 6.0f))));
         float2 sm, cm;
-        __sincosf(mid.x, &sm.x, &cm.x);
-        __sincosf(mid.y, &sm.y, &cm.y);
+        sm = make_float2(sin_fz(mid.x), sin_fz(mid.y));
+        cm = make_float2(cos_fz(mid.x), cos_fz(mid.y));
         const float2 sx = fma2(cm, re, neg2(mul2(sm, im)));
         const float2 sy = fma2(cm, im, mul2(sm, re));
         gx = sel2(D.x < 0.25f, D.y < 0.25f, sx, gx);
@@ -830,7 +850,7 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     const float2 hz = fma2(P.inc[0], qy, neg2(mul2(P.inc[1], qx)));
     const float2 hn2 = fma2(hz, hz, fma2(hy, hy, mul2(hx, hx)));
     const float2 ht = mul2(mul2(hn2, tt), tt);
-    const float2 sc = make_float2(rsqrtf(ht.x), rsqrtf(ht.y));
+    const float2 sc = make_float2(rsqrt_fz(ht.x), rsqrt_fz(ht.y));
     // P1 = p |h| s = hy tt - ky (hx kx + hz kz), from m = (-kx ky / s, s, -kz ky / s);
     // inside the clamp evo2 = (-kz, 0, kx) / s, so R1 = rr |h| s = hz kx - hx kz
     const float2 t = fma2(hx, kx, mul2(hz, kz));
