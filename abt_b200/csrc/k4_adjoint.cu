@@ -96,13 +96,25 @@ __device__ __forceinline__ float rcp4(float x) {
     return r;
 }
 
+// the special-function unit's approximations with subnormal inputs flushed
+// to zero (phases and squared norms here, never subnormal)
+__device__ __forceinline__ void sincos4(float x, float *sn, float *cs) {
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(*sn) : "f"(x));
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(*cs) : "f"(x));
+}
+__device__ __forceinline__ float rsqrt4(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // sinc(h) and sinc'(h) for h >= 0: series below 0.5, else sin(h)/h and
 // (cos h - sinc h)/h with rh = 1/max(h, 0.5).  series (warp-uniform) is false
 // when no lane of the warp has an argument below 0.5; the polynomials are
 // then skipped.
 __device__ __forceinline__ void sinc_d(float h, float rh, bool series, float &sc, float &dsc) {
     float s, c;
-    __sincosf(h, &s, &c);
+    sincos4(h, &s, &c);
     sc = s * rh;
     dsc = (c - sc) * rh;
     if (series) {
@@ -130,8 +142,8 @@ __device__ __forceinline__ void dd_grad(float t0, float t1, float t2, float2 &g,
     {
         const float h1 = 0.5f * (mid - lo), h2 = 0.5f * (hi - mid);
         float s1, c1, s2, c2;
-        __sincosf(lo + h1, &s1, &c1);
-        __sincosf(mid + h2, &s2, &c2);
+        sincos4(lo + h1, &s1, &c1);
+        sincos4(mid + h2, &s2, &c2);
         // 1/max(h1,.5), 1/max(h2,.5), 1/max(D,.25) from one reciprocal
         const float a1 = fmaxf(h1, 0.5f), a2 = fmaxf(h2, 0.5f), Dg = fmaxf(D, 0.25f);
         const float p12 = a1 * a2;
@@ -174,7 +186,7 @@ __device__ __forceinline__ void dd_grad(float t0, float t1, float t2, float2 &g,
             sc.y = fmaf(ci[n], dc, sc.y);
         }
         float sm, cm;
-        __sincosf(mid, &sm, &cm);
+        sincos4(mid, &sm, &cm);
         auto rot = [&](float2 z) { return make_float2(cm * z.x - sm * z.y, cm * z.y + sm * z.x); };
         g = rot(sg);
         dlo = rot(sa);
@@ -247,7 +259,7 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const float traw = fmaf(kx, kx, kz * kz);
     const bool floored = !(traw > kClampSq4);
     const float tt = floored ? kClampSq4 : traw;
-    const float rs = rsqrtf(tt), s = tt * rs;
+    const float rs = rsqrt4(tt), s = tt * rs;
     const float kyrs = kyc * rs;
     const float m[3] = {-kx * kyrs, s, -kz * kyrs};
     // dd = -Kz cf s / 2 - kz icf / (2 s), ee = Kx Ky cf s / 2 - kx ky icf / (2 s)
@@ -272,7 +284,7 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     }
     const float hr[3] = {fmaf(r.inc[1], q[2], -r.inc[2] * q[1]), fmaf(r.inc[2], q[0], -r.inc[0] * q[2]),
                          fmaf(r.inc[0], q[1], -r.inc[1] * q[0])};
-    const float hn = rsqrtf(fmaf(hr[2], hr[2], fmaf(hr[1], hr[1], hr[0] * hr[0])));
+    const float hn = rsqrt4(fmaf(hr[2], hr[2], fmaf(hr[1], hr[1], hr[0] * hr[0])));
     // p = hc.m, rr = hc.evo2 with hc = hr hn.  Inside the clamp k is a unit
     // vector and evo2 = k x m = (-kz, 0, kx) / s, so p = hn (hy s - ky T1 / s),
     // T1 = hx kx + hz kz, and rr = hn (hz kx - hx kz) / s.
@@ -288,7 +300,7 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
         for (int i = 0; i < 3; i++) hc[i] = hr[i] * hn;
         const float vr[3] = {fmaf(kyc, m[2], -kz * m[1]), fmaf(kz, m[0], -kx * m[2]),
                              fmaf(kx, m[1], -kyc * m[0])};
-        vn = rsqrtf(fmaf(vr[2], vr[2], fmaf(vr[1], vr[1], vr[0] * vr[0])));
+        vn = rsqrt4(fmaf(vr[2], vr[2], fmaf(vr[1], vr[1], vr[0] * vr[0])));
         for (int i = 0; i < 3; i++) ev[i] = vr[i] * vn;
         pp = fmaf(hc[2], m[2], fmaf(hc[1], m[1], hc[0] * m[0]));
         rr = fmaf(hc[2], ev[2], fmaf(hc[1], ev[1], hc[0] * ev[0]));
