@@ -415,3 +415,22 @@ def test_second_order_matches_independent_restatement(mesh, euler):
     assert np.allclose(beam["vk7"], [r[2] for r in ref], atol=1e-12)
     assert np.allclose(beam["prop_out"], [r[3] for r in ref], atol=1e-12)
     assert np.allclose(beam["fov"], [r[4] for r in ref], rtol=1e-12)
+
+
+def test_c_caller(tmp_path):
+    """abt_b200/examples/c_trace.c, built with gcc against the library: the
+    tracer through the C ABI gives what the Python face gives for the same
+    prism (24 triangles, 8 apertures)."""
+    exe = str(tmp_path / "c_trace")
+    libdir = os.path.join(ROOT, "abt_b200")
+    subprocess.check_call(["gcc", "-O2", "-std=c99", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(libdir, "examples", "c_trace.c"), "-o", exe,
+                           "-L", libdir, "-lpbt_b200", "-Wl,-rpath," + libdir, "-lm"])
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    tag, nbeam, next_, ratio = r.stdout.split()
+    g = W.hex_prism(5.0, 10.0, n_side=1, n_len=1, roughness=0.0)
+    _, beam, ext, _, en = T.trace(T.Particle(g, g["apertures"]), np.array([0.4, 0.9, 1.3]),
+                                  LAM, RBI)
+    assert tag == "ok" and int(nbeam) == len(beam) and int(next_) == len(ext)
+    assert float(ratio) == pytest.approx(en["beam_energy_out"] / en["geo_cross_sec"], rel=1e-9)
