@@ -100,3 +100,28 @@ def test_overlapped_trace_and_average(ctx):
     for name in ("scatt", "ext", "asymmetry", "geo_cross_sec", "beam_energy_out"):
         assert got[2][name] == pytest.approx(float(ref[2][name]), rel=1e-12)
     assert got[3].tobytes() == np.atleast_1d(ref[3]).tobytes()
+
+
+def test_config1_analogue_traced(ctx):
+    """The reference's first configuration, with the host tracer in place of
+    the Fortran one: a hexagonal column r 5 um, L 10 um triangulated to about
+    0.5 um^2 (900 triangles, its 8 parent faces as apertures), -rot euler
+    30 40 10, lambda 0.532 um, n 1.31, 8 recursions, 181 theta x 180 phi
+    (1,719 beam and 450 external-diffraction outbeams).  The FP64 drop-in
+    matches the C oracle within 1e-10; the FP32 form is within its bars."""
+    geo = W.hex_prism(5.0, 10.0, n_side=5, n_len=10, roughness=0.0)
+    P = T.Particle(geo, geo["apertures"])
+    V, beam, ext, pin, en = T.trace(P, T.euler_from_degrees(30, 40, 10), LAM, RBI)
+    assert 0.97 < en["beam_energy_out"] / en["geo_cross_sec"] < 1.03
+    g = dict(P.geometry, verts=V)
+    theta, phi = make_angles([0, 180], [1]), make_angles([0, 358], [2])
+    a64 = ctx.diff_main(beam, ext, g, theta, phi, LAM, precision="fp64")
+    ref = O.diff_main(theta, phi, LAM, g, beam, ext, nthreads=8)
+    for a, b in zip(a64, ref):
+        assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max()
+    a32 = ctx.diff_main(beam, ext, g, theta, phi, LAM, precision="fp32")
+    m64 = ctx.finalise(a64[0], a64[1], theta, phi, LAM, pin)
+    m32 = ctx.finalise(a32[0], a32[1], theta, phi, LAM, pin)
+    assert mueller_rel_err(m32[0], m64[0], 1e-6) < 1e-4
+    for name in ("scatt", "ext", "asymmetry", "scatt_eff"):
+        assert abs(m32[2][name] - m64[2][name]) <= 1e-5 * abs(m64[2][name]), name
