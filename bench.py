@@ -77,6 +77,8 @@ def parse():
                     help="1: also time the workload with is_fast_diff (field-of-view tile cull)")
     ap.add_argument("--large-orient", type=int, default=2,
                     help="orientations of the large absorbing column timed (0: skip)")
+    ap.add_argument("--large-traced-orient", type=int, default=8,
+                    help="orientations of the large column traced on the host (0: skip)")
     ap.add_argument("--diff-orient", type=int, default=64,
                     help="orientations of the differentiation workload (0: skip)")
     ap.add_argument("--adjoint-facets", type=int, default=20000,
@@ -284,6 +286,63 @@ def _average(ctx, args, geo, Vs, beams, exts, pin, th, ph):
             "max_rel_mueller_err_vs_fp64": mueller_rel_err(f32[0], f64[0], 1e-6),
             "max_rel_param_err_vs_fp64": perr,
             "api": "pbt_diff_batch_list_c (host pointers, one array per orientation), wall clock"}
+
+
+def large_traced(ctx, args):
+    """The large column with beam lists from the host tracer: the same column
+    and grid as large_case, its 8 parent faces as apertures, n = 1.31 + 0.01i,
+    8 recursions, --large-traced-orient orientations uniform on SO(3) traced
+    with pbt_trace_batch_c and averaged by one FP32 batch; the FP64 drop-in and
+    the error on the whole first orientation."""
+    import abt_b200
+    from abt_b200 import tracer as T
+    from abt_b200 import workloads as W
+    from tests.helpers import mueller_rel_err
+    g = W.hex_prism(50.0, 100.0, n_side=25, n_len=50, roughness=0.0, seed=5)
+    P = T.Particle(g, g["apertures"])
+    th = abt_b200.make_angles([0, 180], [0.125])
+    ph = abt_b200.make_angles([0, 359.5], [0.5])
+    nb = len(th) * len(ph)
+    n = args.large_traced_orient
+    eul = W.uniform_euler(np.random.default_rng(5), n)
+    t0 = time.perf_counter()
+    Vs, beams, exts, pin, en = T.trace_batch(P, eul, LAM, 1.31, ibi=0.01)
+    t_trace = time.perf_counter() - t0
+    geo = P.geometry
+    F = np.array([len(b) + len(e) for b, e in zip(beams, exts)])
+    ctx.diff_batch(beams[:1], [exts[0][:64]], Vs[:1], geo, th, ph, LAM, pin[:1], precision="fp32")
+    ctx.set_kernel_timing(True)
+    ctx.kernel_time_ms()
+    t0 = time.perf_counter()
+    ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pin, precision="fp32")
+    t32 = time.perf_counter() - t0
+    k_ms, _ = ctx.kernel_time_ms()
+    g0 = dict(geo, verts=Vs[0])
+    a32 = ctx.diff_main(beams[0], exts[0], g0, th, ph, LAM, precision="fp32")
+    ctx.kernel_time_ms()
+    t0 = time.perf_counter()
+    a64 = ctx.diff_main(beams[0], exts[0], g0, th, ph, LAM, precision="fp64")
+    t64 = time.perf_counter() - t0
+    k64_ms, _ = ctx.kernel_time_ms()
+    ctx.set_kernel_timing(False)
+    m32, _, p32 = ctx.finalise(a32[0], a32[1], th, ph, LAM, pin[0])
+    m64, _, p64 = ctx.finalise(a64[0], a64[1], th, ph, LAM, pin[0])
+    work = float(F.sum()) * nb
+    ratio = (en["beam_energy_out"] + en["abs"]) / en["geo_cross_sec"]
+    return {"workload": "smooth hexagonal column r 50 um, L 100 um, 2 um^2 triangles (22,500, "
+                        "8 apertures), beam lists traced on the host (n = 1.31 + 0.01i, rec 8), "
+                        "%d orientations, 1441 theta x 720 phi" % n,
+            "trace_s": t_trace, "outbeams_per_orientation": [int(F.min()), int(F.mean()),
+                                                             int(F.max())],
+            "energy_out_plus_absorbed_over_geo": [float(ratio.min()), float(ratio.max())],
+            "bins": nb, "fp32_batched_s": t32, "fp32_orientations_per_s": n / t32,
+            "fp32_facet_bin_per_s": work / t32, "fp32_kernel_ms": k_ms,
+            "fp64_dropin_first_orientation_s": t64, "fp64_dropin_kernel_ms": k64_ms,
+            "speedup_fp32_batched_vs_fp64_dropin": t64 * n / t32 * float(F.mean()) / float(F[0]),
+            "max_rel_mueller_err_vs_fp64_first_orientation": mueller_rel_err(m32, m64, 1e-6),
+            "max_rel_param_err_vs_fp64_first_orientation": max(
+                abs(float(p32[k]) - float(p64[k])) / abs(float(p64[k]))
+                for k in ("scatt", "ext", "asymmetry", "back_scatt", "albedo"))}
 
 
 def large_case(ctx, args):
@@ -671,6 +730,8 @@ def main():
         extra["differentiation"] = differentiation(ctx, args)
     if args.large_orient > 0 and solo:
         extra["large_column"] = large_case(ctx, args)
+    if args.large_traced_orient > 0 and solo:
+        extra["large_column_traced"] = large_traced(ctx, args)
 
     # -fast_diff: the same workload with the field-of-view test (fov = 8 lambda / d);
     # error against the FP64 drop-in with is_fast_diff on the first 20,000 facets
