@@ -340,9 +340,22 @@ def large_traced(ctx, args):
             "fp64_dropin_first_orientation_s": t64, "fp64_dropin_kernel_ms": k64_ms,
             "speedup_fp32_batched_vs_fp64_dropin": t64 * n / t32 * float(F.mean()) / float(F[0]),
             "max_rel_mueller_err_vs_fp64_first_orientation": mueller_rel_err(m32, m64, 1e-6),
+            "mueller_err_above_1e-5_and_1e-4_of_peak": [mueller_rel_err(m32, m64, 1e-5),
+                                                        mueller_rel_err(m32, m64, 1e-4)],
+            "worst_bin_theta_deg_m11_over_peak": _worst_bin(m32, m64, th),
             "max_rel_param_err_vs_fp64_first_orientation": max(
                 abs(float(p32[k]) - float(p64[k])) / abs(float(p64[k]))
                 for k in ("scatt", "ext", "asymmetry", "back_scatt", "albedo"))}
+
+
+def _worst_bin(mu, mu_ref, theta, thresh=1e-6):
+    """theta (degrees) of the bin with the largest M11-normalised Mueller error
+    above thresh of the peak M11, and that bin's M11 over the peak."""
+    m11 = mu_ref[..., 0]
+    sel = m11 > thresh * m11.max()
+    e = np.where(sel, np.abs(mu - mu_ref).max(axis=-1) / np.where(sel, m11, 1.0), 0.0)
+    i, j = np.unravel_index(np.argmax(e), e.shape)
+    return [float(np.degrees(theta[j])), float(m11[i, j] / m11.max())]
 
 
 def large_case(ctx, args):
