@@ -238,9 +238,23 @@ F01 = float(np.float32(0.01))
 F11 = float(np.float32(1.1))
 
 
-def _snell(ti, n1, n2):
-    # get_theta_t_complex for real indices
-    return np.arcsin(np.sin(ti) / np.sqrt(np.sin(ti) ** 2 + (n2 / n1) ** 2 * (1 - np.sin(ti) ** 2 * (n1 / n2) ** 2)))
+def _snell(ti, m1, m2):
+    """Angle of refraction from m1 into m2, complex Snell's law as Macke's
+    form states it (src/beam_loop_mod.f90:342-383)."""
+    m1, m2 = complex(m1), complex(m2)
+    k1, k2 = m1.imag / m1.real, m2.imag / m2.real
+    krel = (k2 - k1) / (1 + k1 * k2)
+    nrel = m2.real / m1.real * (1 + k1 * k2) / (1 + k1 * k1)
+    ref1, ref2 = nrel * nrel, krel * krel
+    ref3 = (1 + ref2) ** 2
+    ref6 = ref1 * ref3 / (1 + krel * k2) ** 2
+    st2 = np.sin(ti) ** 2
+    ref4 = 1 - (1 - ref2) / ref1 / ref3 * st2
+    ref5 = 2 * krel / ref1 / ref3 * st2
+    q2 = np.sqrt(ref4 * ref4 + ref5 * ref5)
+    g = np.arccos(ref4 / q2) / 2
+    ref7 = (np.cos(g) - k2 * np.sin(g)) ** 2
+    return np.arcsin(np.sin(ti) / np.sqrt(st2 + ref6 * q2 * ref7))
 
 
 def _trans_prop(ti, tt, prop, norm):
@@ -279,7 +293,7 @@ def _buckets(vx, vy, px, py):
     return np.argmin(d, axis=0)
 
 
-def _second_order(V, geo, lam, rbi):
+def _second_order(V, geo, lam, rbi, ibi=0.0):
     tri_i = geo["face_vi"].reshape(-1, 3) - 1
     ap = geo["apertures"] - 1
     n, mid, area = _faces(V, geo)
@@ -292,10 +306,12 @@ def _second_order(V, geo, lam, rbi):
     ident = np.eye(2, dtype=complex)
     out = []
 
+    mi = complex(rbi, ibi)  # refractive index
+
     def fresnel_outside(ti, tt):
         ci, ct = np.cos(ti), np.cos(tt)
-        return np.diag([(rbi * ci - ct) / (ct + rbi * ci), (ci - rbi * ct) / (ci + rbi * ct)]), \
-            np.diag([2 * ci / (ct + rbi * ci), 2 * ci / (ci + rbi * ct)])
+        return np.diag([(mi * ci - ct) / (ct + mi * ci), (ci - mi * ct) / (ci + mi * ct)]), \
+            np.diag([2 * ci / (ct + mi * ci), 2 * ci / (ci + mi * ct)])
 
     # incidence: lit faces (convex: no blockers), in face order
     lit = [i for i in range(len(ap)) if apn[ap[i], 2] >= F01]
@@ -306,8 +322,8 @@ def _second_order(V, geo, lam, rbi):
         vk7 /= np.linalg.norm(vk7)
         A = _rot2(vk7, np.array([1.0, 0, 0]), inc) @ (ident * np.exp(1j * k * (1000.0 - mid[i, 2])))
         ti = np.arccos(an[2])
-        fr, ft = fresnel_outside(ti, _snell(ti, 1.0, rbi))
-        tt = _snell(ti, 1.0, rbi)
+        fr, ft = fresnel_outside(ti, _snell(ti, 1.0, mi))
+        tt = _snell(ti, 1.0, mi)
         fo.append(dict(fi=i, ap=ap[i], e_perp=vk7, a_ext=fr @ A, a_int=ft @ A,
                        p_int=_trans_prop(ti, tt, inc, -an),
                        p_ext=np.array([2 * an[2] * an[0], 2 * an[2] * an[1], -1 + 2 * an[2] ** 2])))
@@ -369,16 +385,17 @@ def _second_order(V, geo, lam, rbi):
             vk7 = np.cross(-n[m], prop)
             vk7 /= np.linalg.norm(vk7)
             A = _rot2(vk7, e_src, prop) @ a_src * np.exp(1j * k * rbi * best)
+            A = A * np.exp(-2 * k * ibi * np.sqrt(best))  # the reference's attenuation
             ti = np.arccos(-apr[ap[m], 2])
             ti_f = np.arccos(-nr[m, 2])
             tir = ti >= np.arcsin(1 / rbi)
             if tir:
                 fr, ft, tt = -np.eye(2), np.zeros((2, 2)), 0.0
             else:
-                tt = _snell(ti, rbi, 1.0)
+                tt = _snell(ti, mi, 1.0)
                 ci, ct = np.cos(ti), np.cos(tt)
-                fr = np.diag([(ci - rbi * ct) / (rbi * ct + ci), (rbi * ci - ct) / (rbi * ci + ct)])
-                ft = np.diag([2 * rbi * ci / (rbi * ct + ci), 2 * rbi * ci / (rbi * ci + ct)])
+                fr = np.diag([(ci - mi * ct) / (mi * ct + ci), (mi * ci - ct) / (mi * ci + ct)])
+                ft = np.diag([2 * mi * ci / (mi * ct + ci), 2 * mi * ci / (mi * ci + ct)])
             refl = fr @ A
             pr = 0.5 * np.sum(np.abs(refl) ** 2) * area[m] * np.cos(ti_f) * rbi
             ra = apr[ap[m]]
@@ -399,16 +416,20 @@ def _second_order(V, geo, lam, rbi):
     return out
 
 
-@pytest.mark.parametrize("mesh,euler", [((2, 3), (0.4, 0.9, 1.3)), ((2, 3), (2.1, 2.3, 0.2)),
-                                        ((4, 6), (1.1, 1.9, 2.6)), ((4, 6), (5.5, 0.6, 0.9))])
-def test_second_order_matches_independent_restatement(mesh, euler):
+@pytest.mark.parametrize("mesh,euler,ibi", [((2, 3), (0.4, 0.9, 1.3), 0.0),
+                                            ((2, 3), (2.1, 2.3, 0.2), 0.0),
+                                            ((4, 6), (1.1, 1.9, 2.6), 0.0),
+                                            ((4, 6), (5.5, 0.6, 0.9), 0.0),
+                                            ((4, 6), (1.1, 1.9, 2.6), 2e-3),
+                                            ((2, 3), (0.4, 0.9, 1.3), 1e-2)])
+def test_second_order_matches_independent_restatement(mesh, euler, ibi):
     geo = W.hex_prism(5.0, 10.0, n_side=mesh[0], n_len=mesh[1], roughness=0.0)
     P = T.Particle(geo, geo["apertures"])
-    V, beam, ext, pin, en = T.trace(P, np.array(euler), LAM, RBI, rec=2, refl=0)
-    n0 = len(T.trace(P, np.array(euler), LAM, RBI, rec=0)[1])
+    V, beam, ext, pin, en = T.trace(P, np.array(euler), LAM, RBI, ibi=ibi, rec=2, refl=0)
+    n0 = len(T.trace(P, np.array(euler), LAM, RBI, ibi=ibi, rec=0)[1])
     assert len(beam) > n0  # refracted-out beams beyond the first reflections
     g = dict(P.geometry, apertures=geo["apertures"])
-    ref = _second_order(V, g, LAM, RBI)
+    ref = _second_order(V, g, LAM, RBI, ibi)
     assert len(beam) == len(ref) > 0
     assert np.array_equal(beam["fi"], [r[0] + 1 for r in ref])
     assert np.allclose(_ampl(beam["ampl"]), np.array([r[1] for r in ref]), rtol=0, atol=1e-11)
