@@ -56,7 +56,8 @@ constexpr float kOneMinusClampSq = (float)(1.0 - (double)0.999999f * (double)0.9
 struct BinDev {
     double ux, uy, uz;  // unit bin direction, FP64
     float fx, fy, fz;   // same, FP32
-    float hx, hy, hz;   // direction of the (phi_i, theta_i) bin used by the forward bodge
+    float sz, sg;       // s = u + sg z: sz = uz + sg (rounded once from FP64), sg = +-1
+    float hx, hy, hsz;  // the (phi_i, theta_i) bin of the forward bodge in the same form
     int64_t bin;        // bin index
 };
 
@@ -405,6 +406,7 @@ struct K2MainArgs {
     int64_t theta_i;
     float k;      // wavenumber
     float hkR;    // k R / 2
+    float sgh;    // +1 when the bodge row theta_i lies in the hemisphere of (0,0,-1), else -1
     float *ws;    // [seg][8][nb]
     unsigned long long *counter;
     int *err;
@@ -413,7 +415,8 @@ struct K2MainArgs {
 template <int BPT, bool FAST>
 __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const BinDev (&bd)[BPT],
                                           const bool (&valid)[BPT], float (&acc)[BPT][8], float k,
-                                          float hkR, const double *__restrict__ xyz, int64_t nb) {
+                                          float hkR, float sgh, const double *__restrict__ xyz,
+                                          int64_t nb) {
     const double kc0 = r.kc[0], kc1 = r.kc[1], kc2 = r.kc[2];
 #pragma unroll
     for (int q = 0; q < BPT; q++) {
@@ -428,14 +431,20 @@ __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const
         // (u - e)/|u - e| = u (1 + a + 3a^2/2 - b/2) - e (1 + a) + O(|e|^3), e = c/R.
         // The second-order terms matter: near k ~ +-y the polarisation matrix
         // depends on 1 - ky^2 and amplifies direction errors by 1/(1 - ky^2).
+        // With s = u + sg z and inc = -R z: k = ks + sg opa2 inc, ks = R s opa2 - ea opa,
+        // and h = inc x k = inc x ks is formed from small vectors near the poles.
         const float opa = 1.0f + a;
         const float opa2 = fmaf(a, fmaf(1.5f, a, 1.0f), fmaf(-0.5f, r.b, 1.0f));
-        const float w0 = fmaf(r.R[2], B.fz, fmaf(r.R[1], B.fy, r.R[0] * B.fx));
-        const float w1 = fmaf(r.R[5], B.fz, fmaf(r.R[4], B.fy, r.R[3] * B.fx));
-        const float w2 = fmaf(r.R[8], B.fz, fmaf(r.R[7], B.fy, r.R[6] * B.fx));
-        const float kx = fmaf(w0, opa2, -r.ea[0] * opa);
-        const float ky = fmaf(w1, opa2, -r.ea[1] * opa);
-        const float kz = fmaf(w2, opa2, -r.ea[2] * opa);
+        const float w0 = fmaf(r.R[2], B.sz, fmaf(r.R[1], B.fy, r.R[0] * B.fx));
+        const float w1 = fmaf(r.R[5], B.sz, fmaf(r.R[4], B.fy, r.R[3] * B.fx));
+        const float w2 = fmaf(r.R[8], B.sz, fmaf(r.R[7], B.fy, r.R[6] * B.fx));
+        const float ks0 = fmaf(w0, opa2, -r.ea[0] * opa);
+        const float ks1 = fmaf(w1, opa2, -r.ea[1] * opa);
+        const float ks2 = fmaf(w2, opa2, -r.ea[2] * opa);
+        const float so = B.sg * opa2;
+        const float kx = fmaf(so, r.inc[0], ks0);
+        const float ky = fmaf(so, r.inc[1], ks1);
+        const float kz = fmaf(so, r.inc[2], ks2);
         bool use = valid[q];
         if (FAST) {
             // lab-frame direction from the centre: u - eps + u a
@@ -467,15 +476,18 @@ __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const
         const float d = fmaf(r.hkz_cf, s, -(kz * rs) * r.hicf);
         const float e = fmaf(r.hkxky_cf, s, -(kx * kyrs) * r.hicf);
         // vector perpendicular to the scattering plane (forward bodge near the poles)
-        float qx = kx, qy = kyc, qz = kz;
+        // h = inc x (kx, kyc, kz) = inc x (ks0, ks1 + kyc - ky, ks2)
+        float qx = ks0, qy = ks1 + (kyc - ky), qz = ks2;
         const float dinc = fmaf(r.inc[2], kz, fmaf(r.inc[1], kyc, r.inc[0] * kx));
         if (!(fabsf(dinc) < 0.999f)) {
-            const float ah = fmaf(B.hz, r.eps[2], fmaf(B.hy, r.eps[1], B.hx * r.eps[0]));
+            // bodge direction in the s form: uh . eps = hs . eps - sgh eps_z
+            const float ah = fmaf(-sgh, r.eps[2],
+                                  fmaf(B.hsz, r.eps[2], fmaf(B.hy, r.eps[1], B.hx * r.eps[0])));
             const float oh = 1.0f + ah;
             const float oh2 = fmaf(ah, fmaf(1.5f, ah, 1.0f), fmaf(-0.5f, r.b, 1.0f));
-            qx = fmaf(fmaf(r.R[2], B.hz, fmaf(r.R[1], B.hy, r.R[0] * B.hx)), oh2, -r.ea[0] * oh);
-            qy = fmaf(fmaf(r.R[5], B.hz, fmaf(r.R[4], B.hy, r.R[3] * B.hx)), oh2, -r.ea[1] * oh);
-            qz = fmaf(fmaf(r.R[8], B.hz, fmaf(r.R[7], B.hy, r.R[6] * B.hx)), oh2, -r.ea[2] * oh);
+            qx = fmaf(fmaf(r.R[2], B.hsz, fmaf(r.R[1], B.hy, r.R[0] * B.hx)), oh2, -r.ea[0] * oh);
+            qy = fmaf(fmaf(r.R[5], B.hsz, fmaf(r.R[4], B.hy, r.R[3] * B.hx)), oh2, -r.ea[1] * oh);
+            qz = fmaf(fmaf(r.R[8], B.hsz, fmaf(r.R[7], B.hy, r.R[6] * B.hx)), oh2, -r.ea[2] * oh);
         }
         float hx = fmaf(r.inc[1], qz, -r.inc[2] * qy);
         float hy = fmaf(r.inc[2], qx, -r.inc[0] * qz);
@@ -569,12 +581,15 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
             bd[q].fx = (float)bd[q].ux;
             bd[q].fy = (float)bd[q].uy;
             bd[q].fz = (float)bd[q].uz;
+            const double sg = bd[q].uz <= 0.0 ? 1.0 : -1.0;
+            bd[q].sz = (float)(bd[q].uz + sg);
+            bd[q].sg = (float)sg;
             const int64_t oh = (o % P.nphi) + P.nphi * P.theta_i;
             const double Xh = P.xyz[oh], Yh = P.xyz[P.nb + oh], Zh = P.xyz[2 * P.nb + oh];
             const double irh = 1.0 / sqrt(Xh * Xh + Yh * Yh + Zh * Zh);
             bd[q].hx = (float)(Xh * irh);
             bd[q].hy = (float)(Yh * irh);
-            bd[q].hz = (float)(Zh * irh);
+            bd[q].hsz = (float)(Zh * irh + (double)P.sgh);
         }
         double acc64[BPT][8];
 #pragma unroll
@@ -611,7 +626,7 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
             const K2Fov *fv = FAST ? P.fovs + rbeg + c * K2_CH : nullptr;
             for (int j = 0; j < n; j++)
                 k2_record<BPT, FAST>(sbuf[st][j], FAST ? fv + j : nullptr, bd, valid, acc, P.k,
-                                     P.hkR, P.xyz, P.nb);
+                                     P.hkR, P.sgh, P.xyz, P.nb);
 #pragma unroll
             for (int q = 0; q < BPT; q++)
 #pragma unroll
@@ -679,12 +694,19 @@ __device__ __forceinline__ float2 sel2(bool px, bool py, float2 a, float2 b) {
     return make_float2(px ? a.x : b.x, py ? a.y : b.y);
 }
 
+// A bin of the packed kernel.  The direction is held as s = u + sg z, sg = +1 in
+// the hemisphere of the incidence direction (0,0,-1) and -1 in the other, so
+// that sz = uz + sg (formed in FP64, rounded once) is small and exact to FP32
+// precision near both poles; u = (fx, fy, sz - sg).  The forward-bodge bin
+// direction, used near the poles only, is kept in shared memory (slot hslot of
+// the kernel's bodge table) in the same form with the kernel's sgh.
 struct BinPk {
     double ux, uy, uz;     // unit bin direction, FP64
-    float2 fx, fy, fz;     // same, broadcast FP32 pairs
-    float2 hx, hy, hz;     // forward-bodge bin direction, broadcast pairs
+    float2 fx, fy, sz, sg; // broadcast FP32 pairs
+    int hslot;
     int64_t bin;           // bin index
 };
+constexpr int K2P_HB = K2_THREADS * 2;  // bodge table slots (bins per thread <= 2)
 
 // Taylor series of sin(h)/h, used below h = 0.5 where the MUFU sine's
 // absolute error would be a large relative one
@@ -768,53 +790,80 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
     }
 }
 
+// Two adjacent float2 fields of a record pair from one 16-byte shared-memory load
+// (every such field pair of K2Pair starts on a 16-byte boundary).
+__device__ __forceinline__ void ld22(const float2 *p, float2 &a, float2 &b) {
+    const float4 v = *reinterpret_cast<const float4 *>(p);
+    a = make_float2(v.x, v.y);
+    b = make_float2(v.z, v.w);
+}
+
 template <bool FAST>
 __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const BinPk &B,
-                                        float2 (&acc)[8], float2 nk, float2 hkR, bool lo_ok,
-                                        bool hi_ok, const double *__restrict__ xyz, int64_t nb) {
+                                        float2 (&acc)[8], float2 nk, float2 hkR, float2 sgh,
+                                        const float (&hb)[3][K2P_HB], bool lo_ok, bool hi_ok,
+                                        const double *__restrict__ xyz, int64_t nb) {
     // far-field phase per facet: FP64 k u.c, reduced mod 2 pi
     float2 rf;
     {
-        const double ka = fma(B.uz, P.kc[2][0], fma(B.uy, P.kc[1][0], B.ux * P.kc[0][0]));
+        const double2 k0 = *reinterpret_cast<const double2 *>(&P.kc[0][0]);
+        const double2 k1 = *reinterpret_cast<const double2 *>(&P.kc[1][0]);
+        const double2 k2 = *reinterpret_cast<const double2 *>(&P.kc[2][0]);
+        const double ka = fma(B.uz, k2.x, fma(B.uy, k1.x, B.ux * k0.x));
         const double nq = fma(ka, kInv2Pi, kMagic) - kMagic;
         rf.x = (float)fma(-nq, kTwoPi, ka);
-        const double kb = fma(B.uz, P.kc[2][1], fma(B.uy, P.kc[1][1], B.ux * P.kc[0][1]));
+        const double kb = fma(B.uz, k2.y, fma(B.uy, k1.y, B.ux * k0.y));
         const double nb = fma(kb, kInv2Pi, kMagic) - kMagic;
         rf.y = (float)fma(-nb, kTwoPi, kb);
     }
     const float2 one = bc2(1.0f);
-    const float2 a = fma2(B.fz, P.eps[2], fma2(B.fy, P.eps[1], mul2(B.fx, P.eps[0])));
+    float2 eps0, eps1, eps2, pb;
+    ld22(&P.eps[0], eps0, eps1);
+    ld22(&P.eps[2], eps2, pb);
+    // a = u . eps = s . eps - sg eps_z
+    const float2 a = fma2(neg2(B.sg), eps2, fma2(B.sz, eps2, fma2(B.fy, eps1, mul2(B.fx, eps0))));
     const float2 opa = add2(one, a);
-    const float2 ph = fma2(mul2(hkR, fma2(neg2(a), a, P.b)), opa, neg2(rf));
-    const float2 opa2 = fma2(a, fma2(bc2(1.5f), a, one), fma2(bc2(-0.5f), P.b, one));
-    const float2 w0 = fma2(P.R[2], B.fz, fma2(P.R[1], B.fy, mul2(P.R[0], B.fx)));
-    const float2 w1 = fma2(P.R[5], B.fz, fma2(P.R[4], B.fy, mul2(P.R[3], B.fx)));
-    const float2 w2 = fma2(P.R[8], B.fz, fma2(P.R[7], B.fy, mul2(P.R[6], B.fx)));
-    const float2 kx = fma2(w0, opa2, mul2(P.nea[0], opa));
-    const float2 ky = fma2(w1, opa2, mul2(P.nea[1], opa));
-    const float2 kz = fma2(w2, opa2, mul2(P.nea[2], opa));
-    bool ok_x = lo_ok, ok_y = hi_ok;
-    if (FAST) {
-        const float2 dx = fma2(B.fx, opa, neg2(P.eps[0]));
-        const float2 dy = fma2(B.fy, opa, neg2(P.eps[1]));
-        const float2 dz = fma2(B.fz, opa, neg2(P.eps[2]));
-        const K2Fov &fa = fv[0], &fb = fv[1];
-        const float dpx = fmaf(dz.x, fa.p0[2], fmaf(dy.x, fa.p0[1], dx.x * fa.p0[0]));
-        const float dpy = fmaf(dz.y, fb.p0[2], fmaf(dy.y, fb.p0[1], dx.y * fb.p0[0]));
-        bool in_x = !(dpx < fa.cos_fov), in_y = !(dpy < fb.cos_fov);
-        if (ok_x && fabsf(dpx - fa.cos_fov) < fa.tol) in_x = fov_exact(fa, xyz, nb, B.bin);
-        if (ok_y && fabsf(dpy - fb.cos_fov) < fb.tol) in_y = fov_exact(fb, xyz, nb, B.bin);
-        ok_x = ok_x && in_x;
-        ok_y = ok_y && in_y;
+    const float2 ph = fma2(mul2(hkR, fma2(neg2(a), a, pb)), opa, neg2(rf));
+    const float2 opa2 = fma2(a, fma2(bc2(1.5f), a, one), fma2(bc2(-0.5f), pb, one));
+    // The bin direction enters through s = u + sg z (sg = +1 in the hemisphere of
+    // the incidence direction (0,0,-1), -1 in the other), which is small and known
+    // to full FP32 precision near both poles.  With inc = -R z (the incidence
+    // direction in the aperture frame), k = R u opa2 + nea opa = ks + sg opa2 inc
+    // with ks = R s opa2 + nea opa, and the normal of the scattering plane is
+    // h = inc x k = inc x ks: no cancellation of nearly parallel unit vectors near
+    // the forward and backward directions, where |h| is small.
+    float2 ks0, ks1, ks2;
+    {
+        float2 r0, r1, r2, r3, r4, r5, r6, r7, r8, n0, n1, n2;
+        ld22(&P.R[0], r0, r1);
+        ld22(&P.R[2], r2, r3);
+        ld22(&P.R[4], r4, r5);
+        ld22(&P.R[6], r6, r7);
+        ld22(&P.R[8], r8, n0);
+        ld22(&P.nea[1], n1, n2);
+        const float2 w0 = fma2(r2, B.sz, fma2(r1, B.fy, mul2(r0, B.fx)));
+        const float2 w1 = fma2(r5, B.sz, fma2(r4, B.fy, mul2(r3, B.fx)));
+        const float2 w2 = fma2(r8, B.sz, fma2(r7, B.fy, mul2(r6, B.fx)));
+        ks0 = fma2(w0, opa2, mul2(n0, opa));
+        ks1 = fma2(w1, opa2, mul2(n1, opa));
+        ks2 = fma2(w2, opa2, mul2(n2, opa));
     }
-    // aperture integral
-    const float2 kxx = fma2(nk, kx, P.kp[0]);
-    const float2 kyy = fma2(nk, ky, P.kp[1]);
-    const float2 t1 = fma2(kyy, P.vy[0], fma2(kxx, P.vx[0], ph));
-    const float2 t2 = fma2(kyy, P.vy[1], fma2(kxx, P.vx[1], ph));
-    const float2 t3 = fma2(kyy, P.vy[2], fma2(kxx, P.vx[2], ph));
-    float2 gx, gy;
-    tri_dd_pk(t1, t2, t3, gx, gy);
+    float2 hkz_cf, hicf, hkxky_cf, inc0, inc1, inc2;
+    ld22(&P.hkz_cf, hkz_cf, hicf);
+    ld22(&P.hkxky_cf, hkxky_cf, inc0);
+    ld22(&P.inc[1], inc1, inc2);
+    const float2 so = mul2(B.sg, opa2);
+    const float2 kx = fma2(so, inc0, ks0);
+    const float2 ky = fma2(so, inc1, ks1);
+    const float2 kz = fma2(so, inc2, ks2);
+    // aperture wave vector
+    float2 kxx, kyy;
+    {
+        float2 kp0, kp1;
+        ld22(&P.kp[0], kp0, kp1);
+        kxx = fma2(nk, kx, kp0);
+        kyy = fma2(nk, ky, kp1);
+    }
     // polarisation matrix [[d, e], [-e, d]] (see k2_record for the forms) and
     // the rotation into the scattering plane, with their normalisations folded
     // into one factor: with s = sqrt(tt) and hc = h / |h|,
@@ -825,36 +874,47 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
                                    fminf(fmaxf(ky.y, -0.999999f), 0.999999f));
     const float2 tr = fma2(kx, kx, mul2(kz, kz));
     const float2 tt = make_float2(fmaxf(tr.x, kOneMinusClampSq), fmaxf(tr.y, kOneMinusClampSq));
-    const float2 d1 = fma2(P.hkz_cf, tt, neg2(mul2(kz, P.hicf)));
-    const float2 e1 = fma2(P.hkxky_cf, tt, neg2(mul2(mul2(kx, kyc), P.hicf)));
-    float2 qx = kx, qy = kyc, qz = kz;
-    const float2 dinc = fma2(P.inc[2], kz, fma2(P.inc[1], kyc, mul2(P.inc[0], kx)));
+    const float2 d1 = fma2(hkz_cf, tt, neg2(mul2(kz, hicf)));
+    const float2 e1 = fma2(hkxky_cf, tt, neg2(mul2(mul2(kx, kyc), hicf)));
+    // h = inc x (kx, kyc, kz) = inc x (ks0, ks1 + kyc - ky, ks2)
+    const float2 qy = add2(ks1, add2(kyc, neg2(ky)));
+    float2 hx = fma2(inc1, ks2, neg2(mul2(inc2, qy)));
+    float2 hy = fma2(inc2, ks0, neg2(mul2(inc0, ks2)));
+    float2 hz = fma2(inc0, qy, neg2(mul2(inc1, ks0)));
+    // P1 = p |h| s = hy tt - kyc (hx kx + hz kz), from m = (-kx ky / s, s, -kz ky / s).
+    // Where h is normal to q = (kx, kyc, kz), hx kx + hz kz = -hy kyc and
+    // P1 = hy (tt + kyc^2) = hy |q|^2 = hy (|q| = 1 up to rounding; on the clamp
+    // tt + kyc^2 = 1 - c^2 + c^2); the forward bodge takes the general form.
+    float2 P1 = hy;
+    const float2 dinc = fma2(inc2, kz, fma2(inc1, kyc, mul2(inc0, kx)));
     const bool bx = !(fabsf(dinc.x) < 0.999f), by = !(fabsf(dinc.y) < 0.999f);
     if (bx || by) {
-        const float2 ah = fma2(B.hz, P.eps[2], fma2(B.hy, P.eps[1], mul2(B.hx, P.eps[0])));
+        // the bodge direction in the s form: hs = uh + sgh z, uh . eps = hs . eps - sgh eps_z,
+        // h = inc x (R hs oh2 + nea oh)
+        const float2 hx_ = bc2(hb[0][B.hslot]), hy_ = bc2(hb[1][B.hslot]), hsz = bc2(hb[2][B.hslot]);
+        float2 ah = fma2(hsz, eps2, fma2(hy_, eps1, mul2(hx_, eps0)));
+        ah = fma2(neg2(sgh), eps2, ah);
         const float2 oh = add2(one, ah);
-        const float2 oh2 = fma2(ah, fma2(bc2(1.5f), ah, one), fma2(bc2(-0.5f), P.b, one));
-        const float2 vx = fma2(fma2(P.R[2], B.hz, fma2(P.R[1], B.hy, mul2(P.R[0], B.hx))), oh2,
+        const float2 oh2 = fma2(ah, fma2(bc2(1.5f), ah, one), fma2(bc2(-0.5f), pb, one));
+        const float2 vx = fma2(fma2(P.R[2], hsz, fma2(P.R[1], hy_, mul2(P.R[0], hx_))), oh2,
                                mul2(P.nea[0], oh));
-        const float2 vy = fma2(fma2(P.R[5], B.hz, fma2(P.R[4], B.hy, mul2(P.R[3], B.hx))), oh2,
+        const float2 vy = fma2(fma2(P.R[5], hsz, fma2(P.R[4], hy_, mul2(P.R[3], hx_))), oh2,
                                mul2(P.nea[1], oh));
-        const float2 vz = fma2(fma2(P.R[8], B.hz, fma2(P.R[7], B.hy, mul2(P.R[6], B.hx))), oh2,
+        const float2 vz = fma2(fma2(P.R[8], hsz, fma2(P.R[7], hy_, mul2(P.R[6], hx_))), oh2,
                                mul2(P.nea[2], oh));
-        qx = sel2(bx, by, vx, qx);
-        qy = sel2(bx, by, vy, qy);
-        qz = sel2(bx, by, vz, qz);
+        const float2 gx = fma2(inc1, vz, neg2(mul2(inc2, vy)));
+        const float2 gy = fma2(inc2, vx, neg2(mul2(inc0, vz)));
+        const float2 gz = fma2(inc0, vy, neg2(mul2(inc1, vx)));
+        const float2 gP = fma2(gy, tt, neg2(mul2(kyc, fma2(gx, kx, mul2(gz, kz)))));
+        hx = sel2(bx, by, gx, hx);
+        hy = sel2(bx, by, gy, hy);
+        hz = sel2(bx, by, gz, hz);
+        P1 = sel2(bx, by, gP, P1);
     }
-    // h = inc x q
-    const float2 hx = fma2(P.inc[1], qz, neg2(mul2(P.inc[2], qy)));
-    const float2 hy = fma2(P.inc[2], qx, neg2(mul2(P.inc[0], qz)));
-    const float2 hz = fma2(P.inc[0], qy, neg2(mul2(P.inc[1], qx)));
     const float2 hn2 = fma2(hz, hz, fma2(hy, hy, mul2(hx, hx)));
     const float2 ht = mul2(mul2(hn2, tt), tt);
     const float2 sc = make_float2(rsqrt_fz(ht.x), rsqrt_fz(ht.y));
-    // P1 = p |h| s = hy tt - ky (hx kx + hz kz), from m = (-kx ky / s, s, -kz ky / s);
     // inside the clamp evo2 = (-kz, 0, kx) / s, so R1 = rr |h| s = hz kx - hx kz
-    const float2 t = fma2(hx, kx, mul2(hz, kz));
-    const float2 P1 = fma2(hy, tt, neg2(mul2(kyc, t)));
     float2 R1 = fma2(hz, kx, neg2(mul2(hx, kz)));
     const bool cx = tt.x <= kOneMinusClampSq, cy = tt.y <= kOneMinusClampSq;
     if (cx || cy) {
@@ -872,11 +932,39 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     }
     const float2 A = mul2(sc, fma2(P1, d1, mul2(R1, e1)));
     const float2 Bc = mul2(sc, fma2(P1, e1, neg2(mul2(R1, d1))));
+    // aperture integral (after the polarisation block, so that only A and B
+    // stay live across it)
+    float2 gx, gy;
+    {
+        float2 vx0, vx1, vx2, vy0, vy1, vy2;
+        ld22(&P.vx[0], vx0, vx1);
+        ld22(&P.vx[2], vx2, vy0);
+        ld22(&P.vy[1], vy1, vy2);
+        const float2 t1 = fma2(kyy, vy0, fma2(kxx, vx0, ph));
+        const float2 t2 = fma2(kyy, vy1, fma2(kxx, vx1, ph));
+        const float2 t3 = fma2(kyy, vy2, fma2(kxx, vx2, ph));
+        tri_dd_pk(t1, t2, t3, gx, gy);
+    }
     // [[A, B], [-B, A]] is diagonal in the circular basis: with z = A - iB the
     // columns' u+ take z, their u- take conj(z).  q+ = g z, q- = g conj(z).
     const float2 gyB = mul2(gy, Bc), gxB = mul2(gx, Bc);
     float2 qpr = fma2(gx, A, gyB), qmr = fma2(gx, A, neg2(gyB));
     float2 qpi = fma2(gy, A, neg2(gxB)), qmi = fma2(gy, A, gxB);
+    bool ok_x = lo_ok, ok_y = hi_ok;
+    if (FAST) {
+        // the field-of-view test (direction from the facet centre, lab frame)
+        const float2 dx = fma2(B.fx, opa, neg2(eps0));
+        const float2 dy = fma2(B.fy, opa, neg2(eps1));
+        const float2 dz = fma2(add2(B.sz, neg2(B.sg)), opa, neg2(eps2));
+        const K2Fov &fa = fv[0], &fb = fv[1];
+        const float dpx = fmaf(dz.x, fa.p0[2], fmaf(dy.x, fa.p0[1], dx.x * fa.p0[0]));
+        const float dpy = fmaf(dz.y, fb.p0[2], fmaf(dy.y, fb.p0[1], dx.y * fb.p0[0]));
+        bool in_x = !(dpx < fa.cos_fov), in_y = !(dpy < fb.cos_fov);
+        if (ok_x && fabsf(dpx - fa.cos_fov) < fa.tol) in_x = fov_exact(fa, xyz, nb, B.bin);
+        if (ok_y && fabsf(dpy - fb.cos_fov) < fb.tol) in_y = fov_exact(fb, xyz, nb, B.bin);
+        ok_x = ok_x && in_x;
+        ok_y = ok_y && in_y;
+    }
     if (FAST || !lo_ok || !hi_ok) {
         // a lane outside the item or outside the field of view adds nothing
         qpr = sel2(ok_x, ok_y, qpr, bc2(0.0f));
@@ -888,7 +976,8 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         const float2 qr = (c & 1) ? qmr : qpr, qi = (c & 1) ? qmi : qpi;
-        const float2 ur = P.amp[2 * c], ui = P.amp[2 * c + 1];
+        float2 ur, ui;
+        ld22(&P.amp[2 * c], ur, ui);
         acc[2 * c] = fma2(qr, ur, fma2(neg2(qi), ui, acc[2 * c]));
         acc[2 * c + 1] = fma2(qr, ui, fma2(qi, ur, acc[2 * c + 1]));
     }
@@ -920,17 +1009,19 @@ struct K2PkArgs {
     int64_t theta_i;
     float k;
     float hkR;
+    float sgh;   // +1 when the bodge row theta_i lies in the hemisphere of (0,0,-1), else -1
     float *ws;
     unsigned long long *counter;
     int *err;
 };
 
 template <int BPT, bool FAST>
-__global__ void __launch_bounds__(K2_THREADS, (BPT == 1 && FAST) ? 4 : 0) k2_main_pk_kernel(K2PkArgs P) {
+__global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kernel(K2PkArgs P) {
     __shared__ __align__(128) K2Pair sbuf[K2_NST][K2P_CH];
     __shared__ __align__(8) uint64_t bars[K2_NST];
     __shared__ long long s_item;
     __shared__ unsigned s_keep[2];  // is_fast_diff: records of the stage not culled for the tile
+    __shared__ float s_hb[3][K2P_HB];  // forward-bodge bin directions of this CTA's bins (s form)
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int s = 0; s < K2_NST; s++) mbar_init(smem_u32(&bars[s]), 1);
@@ -940,7 +1031,7 @@ __global__ void __launch_bounds__(K2_THREADS, (BPT == 1 && FAST) ? 4 : 0) k2_mai
     uint32_t parity = 0;  // bit s: phase of stage s
     const int64_t total = P.item_pre[P.nseg];
     constexpr int64_t TILE = (int64_t)K2_THREADS * BPT;
-    const float2 nk = bc2(-P.k), hkR = bc2(P.hkR);
+    const float2 nk = bc2(-P.k), hkR = bc2(P.hkR), sgh = bc2(P.sgh);
     for (;;) {
         if (tid == 0) s_item = (long long)atomicAdd(P.counter, 1ull);
         __syncthreads();
@@ -976,13 +1067,16 @@ __global__ void __launch_bounds__(K2_THREADS, (BPT == 1 && FAST) ? 4 : 0) k2_mai
             bd[q].uz = Zc * ir;
             bd[q].fx = bc2((float)bd[q].ux);
             bd[q].fy = bc2((float)bd[q].uy);
-            bd[q].fz = bc2((float)bd[q].uz);
+            const double sg = bd[q].uz <= 0.0 ? 1.0 : -1.0;
+            bd[q].sz = bc2((float)(bd[q].uz + sg));
+            bd[q].sg = bc2((float)sg);
             const int64_t oh = (o % P.nphi) + P.nphi * P.theta_i;
             const double Xh = P.xyz[oh], Yh = P.xyz[P.nb + oh], Zh = P.xyz[2 * P.nb + oh];
             const double irh = 1.0 / sqrt(Xh * Xh + Yh * Yh + Zh * Zh);
-            bd[q].hx = bc2((float)(Xh * irh));
-            bd[q].hy = bc2((float)(Yh * irh));
-            bd[q].hz = bc2((float)(Zh * irh));
+            bd[q].hslot = q * K2_THREADS + tid;
+            s_hb[0][bd[q].hslot] = (float)(Xh * irh);
+            s_hb[1][bd[q].hslot] = (float)(Yh * irh);
+            s_hb[2][bd[q].hslot] = (float)(Zh * irh + (double)P.sgh);
         }
         double acc64[BPT][8];
 #pragma unroll
@@ -1046,7 +1140,7 @@ __global__ void __launch_bounds__(K2_THREADS, (BPT == 1 && FAST) ? 4 : 0) k2_mai
                 }
 #pragma unroll
                 for (int q = 0; q < BPT; q++)
-                    k2_pair<FAST>(sbuf[st][j], fv, bd[q], acc[q], nk, hkR, lo_ok && valid[q],
+                    k2_pair<FAST>(sbuf[st][j], fv, bd[q], acc[q], nk, hkR, sgh, s_hb, lo_ok && valid[q],
                                   hi_ok && valid[q], P.xyz, P.nb);
             };
             if (FAST) {
@@ -1601,6 +1695,7 @@ int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, in
     A.theta_i = g.theta_i;
     A.k = (float)waveno;
     A.hkR = (float)(0.5 * waveno * kFarR);
+    A.sgh = -cos(g.theta[g.theta_i]) <= 0.0 ? 1.0f : -1.0f;  // sign rule of the bin set-up
     A.ws = ws;
     A.counter = counter;
     A.err = S.err;
@@ -1621,6 +1716,7 @@ int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, in
         B.theta_i = A.theta_i;
         B.k = A.k;
         B.hkR = A.hkR;
+        B.sgh = A.sgh;
         B.ws = ws;
         B.counter = counter;
         B.err = S.err;

@@ -102,6 +102,36 @@ def test_overlapped_trace_and_average(ctx):
     assert got[3].tobytes() == np.atleast_1d(ref[3]).tobytes()
 
 
+@pytest.mark.parametrize("plan", [(-1, 1, 2048), (0, 1, 2048), (1, 2, 1024)],
+                         ids=["packed", "one-record", "packed-2bins"])
+def test_large_column_traced_forward_rings(ctx, plan):
+    """The large column (r 50 um, L 100 um, 22,500 triangles, n = 1.31 + 0.01i)
+    traced in one orientation (about 34,000 outbeams), on a grid that keeps the
+    first dark rings of the forward diffraction peak (theta 0-10 deg at 0.125 deg).
+    The triangles of each face are translated copies, so per-face FP32 errors
+    add up coherently, and at the dark rings the faces' contributions cancel.
+    Near the forward direction the normal of the scattering plane is the cross
+    product of nearly parallel unit vectors: formed from FP32 unit vectors it
+    loses about six bits and left a 3e-4 Mueller error at theta = 0.25 deg.
+    The FP32 form must stay within its bars of the FP64 drop-in here."""
+    g = W.hex_prism(50.0, 100.0, n_side=25, n_len=50, roughness=0.0, seed=5)
+    P = T.Particle(g, g["apertures"])
+    e = W.uniform_euler(np.random.default_rng(5), 8)[0]
+    V, beam, ext, pin, _ = T.trace(P, e, LAM, RBI, ibi=0.01)
+    assert len(beam) > 20000 and len(ext) > 10000
+    gv = dict(P.geometry, verts=V)
+    theta, phi = make_angles([0, 10], [0.125]), make_angles([0, 356], [4])
+    a64 = ctx.diff_main(beam, ext, gv, theta, phi, LAM, precision="fp64")
+    ctx.set_plan(*plan)
+    try:
+        a32 = ctx.diff_main(beam, ext, gv, theta, phi, LAM, precision="fp32")
+    finally:
+        ctx.set_plan()
+    m64 = ctx.finalise(a64[0], a64[1], theta, phi, LAM, pin)[0]
+    m32 = ctx.finalise(a32[0], a32[1], theta, phi, LAM, pin)[0]
+    assert mueller_rel_err(m32, m64, 1e-6) < 1e-4
+
+
 def test_config1_analogue_traced(ctx):
     """The reference's first configuration, with the host tracer in place of
     the Fortran one: a hexagonal column r 5 um, L 10 um triangulated to about
