@@ -53,22 +53,27 @@ static_assert(sizeof(K2Cone) == 32, "K2Cone must be 32 bytes");
 
 namespace pbt {
 
-// Two K2Rec records interleaved field by field (x = even record, y = odd
+// Two triangle records interleaved field by field (x = even record, y = odd
 // record), so that a shared-memory load of a float2 yields the operand pair of
-// a packed FP32x2 instruction evaluating two facets at once.  352 bytes.
+// a packed FP32x2 instruction evaluating two facets at once.  The packed kernel
+// works with half phases (kc and kp are halved) and with the Karczewski-Wolf
+// block divided by its factor sqrt(1 - Ky^2) / 2, which goes into the
+// amplitudes together with the 1/2 of the half-phase divided difference.
+// Every pair of adjacent float2 fields from eps on starts on a 16-byte
+// boundary, so the kernel reads them two at a time.  336 bytes.
 struct __align__(16) K2Pair {
-    double kc[3][2];  // k * com, [component][half]
+    double kc[3][2];  // k * com / 2, [component][half]
     float2 eps[3];
     float2 b;
     float2 R[9];
     float2 nea[3];    // -R * com / R
-    float2 kp[2];
-    float2 hkz_cf, hicf, hkxky_cf;
+    float2 kp[2];     // k * prop2 (x, y) / 2
+    float2 kzc;       // -Kz / (1 - Ky^2)
     float2 inc[3];
     float2 vx[3], vy[3];
-    float2 amp[8];   // the amplitude columns in the circular basis: u+_1, u-_1, u+_2, u-_2
-                     // (u+- = a1c +- i a2c of K2Rec::amp), re/im
+    float2 amp[8];    // the amplitude columns in the circular basis, u+_1, u-_1, u+_2, u-_2
+                      // (u+- = a1c +- i a2c of K2Rec::amp) times sqrt(1 - Ky^2) / 4, re/im
 };
-static_assert(sizeof(K2Pair) == 352, "K2Pair must be 352 bytes");
+static_assert(sizeof(K2Pair) == 336, "K2Pair must be 336 bytes");
 
 }  // namespace pbt

@@ -50,6 +50,8 @@ constexpr int K2_NST = 3;   // stages
 constexpr double kTwoPi = 6.283185307179586;
 constexpr double kInv2Pi = 0.15915494309189535;
 constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52, round-to-integer constant
+constexpr double kPi = 3.141592653589793;
+constexpr double kInvPi = 0.3183098861837907;
 // 1 - c^2 for the reference's clamp c = 0.999999 (a float literal)
 constexpr float kOneMinusClampSq = (float)(1.0 - (double)0.999999f * (double)0.999999f);
 
@@ -132,8 +134,11 @@ __global__ void k2_count_kernel(RefSrc S, int64_t nrefs, const int64_t *__restri
     cnt[g] = face_off[fi] - face_off[fi - 1] - 2;
 }
 
-// Write record r into half r % 2 of pair r / 2.
-__device__ __forceinline__ void store_pair_half(K2Pair *pairs, int64_t r, const K2Rec &rec) {
+// Write record r into half r % 2 of pair r / 2 (K2Pair's half-phase and
+// scaled forms): kzc = -Kz / (1 - Ky^2) and the circular-basis amplitudes uc
+// times sqrt(1 - Ky^2) / 4, both formed in FP64 by the caller.
+__device__ __forceinline__ void store_pair_half(K2Pair *pairs, int64_t r, const K2Rec &rec,
+                                                double kzc, const double (&uc)[8]) {
     K2Pair &P = pairs[r >> 1];
     const int h = (int)(r & 1);
     auto put = [h](float2 &dst, float v) {
@@ -143,7 +148,7 @@ __device__ __forceinline__ void store_pair_half(K2Pair *pairs, int64_t r, const 
             dst.x = v;
     };
     for (int c = 0; c < 3; c++) {
-        P.kc[c][h] = rec.kc[c];
+        P.kc[c][h] = 0.5 * rec.kc[c];
         put(P.eps[c], rec.eps[c]);
         put(P.nea[c], -rec.ea[c]);
         put(P.inc[c], rec.inc[c]);
@@ -152,12 +157,10 @@ __device__ __forceinline__ void store_pair_half(K2Pair *pairs, int64_t r, const 
     }
     put(P.b, rec.b);
     for (int q = 0; q < 9; q++) put(P.R[q], rec.R[q]);
-    put(P.kp[0], rec.kp[0]);
-    put(P.kp[1], rec.kp[1]);
-    put(P.hkz_cf, rec.hkz_cf);
-    put(P.hicf, rec.hicf);
-    put(P.hkxky_cf, rec.hkxky_cf);
-    for (int q = 0; q < 8; q++) put(P.amp[q], rec.amp[q]);
+    put(P.kp[0], 0.5f * rec.kp[0]);
+    put(P.kp[1], 0.5f * rec.kp[1]);
+    put(P.kzc, (float)kzc);
+    for (int q = 0; q < 8; q++) put(P.amp[q], (float)uc[q]);
 }
 
 __global__ void k2_setup_kernel(RefSrc S, int64_t nrefs, const double *__restrict__ verts,
@@ -165,7 +168,8 @@ __global__ void k2_setup_kernel(RefSrc S, int64_t nrefs, const double *__restric
                                 const int64_t *__restrict__ face_vi, const int64_t *__restrict__ start,
                                 double waveno, double lambda, int fast_diff,
                                 K2Rec *__restrict__ recs, K2Pair *__restrict__ pairs,
-                                K2Fov *__restrict__ fovs, int *__restrict__ err) {
+                                K2Fov *__restrict__ fovs, int *__restrict__ err,
+                                unsigned *__restrict__ epsmax) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= nrefs) return;
     int64_t o;
@@ -195,6 +199,12 @@ __global__ void k2_setup_kernel(RefSrc S, int64_t nrefs, const double *__restric
     const double sign = fr.sign;
     const double *com = fr.com;
     const double R = kFarR;
+    if (epsmax) {
+        // an upper bound of |com| / R over the records (positive floats order as
+        // unsigned integers)
+        const double e = sqrt(com[0] * com[0] + com[1] * com[1] + com[2] * com[2]) / R;
+        atomicMax(epsmax, __float_as_uint((float)(e * (1.0 + 1e-6)) + 1e-30f));
+    }
     const double Ky = fr.prop2[1];
     const double cf = 1.0 / sqrt(1.0 - Ky * Ky);
     double ea[3];
@@ -236,11 +246,14 @@ __global__ void k2_setup_kernel(RefSrc S, int64_t nrefs, const double *__restric
         for (int q = 0; q < 8; q++) rec.amp[q] = (float)am[q];
         if (pairs) {
             // the packed kernel works on the columns in the circular basis
-            // u+ = a1c + i a2c, u- = a1c - i a2c (formed in FP64)
-            const double uc[8] = {am[0] - am[3], am[1] + am[2], am[0] + am[3], am[1] - am[2],
-                                  am[4] - am[7], am[5] + am[6], am[4] + am[7], am[5] - am[6]};
-            for (int q = 0; q < 8; q++) rec.amp[q] = (float)uc[q];
-            store_pair_half(pairs, r0 + t, rec);
+            // u+ = a1c + i a2c, u- = a1c - i a2c (formed in FP64), scaled by the
+            // Karczewski-Wolf factor sqrt(1 - Ky^2) / 2 and the 1/2 of the
+            // half-phase divided difference
+            const double sk = 0.25 / cf;
+            const double uc[8] = {sk * (am[0] - am[3]), sk * (am[1] + am[2]), sk * (am[0] + am[3]),
+                                  sk * (am[1] - am[2]), sk * (am[4] - am[7]), sk * (am[5] + am[6]),
+                                  sk * (am[4] + am[7]), sk * (am[5] - am[6])};
+            store_pair_half(pairs, r0 + t, rec, -fr.prop2[2] * cf * cf, uc);
         } else {
             recs[r0 + t] = rec;
         }
@@ -704,6 +717,7 @@ struct BinPk {
     double ux, uy, uz;     // unit bin direction, FP64
     float2 fx, fy, sz, sg; // broadcast FP32 pairs
     int hslot;
+    bool pole;             // within reach of the forward bodge (|uz| near 1) for some record
     int64_t bin;           // bin index
 };
 constexpr int K2P_HB = K2_THREADS * 2;  // bodge table slots (bins per thread <= 2)
@@ -718,8 +732,12 @@ __device__ __forceinline__ float2 sinc_series(float2 h) {
                 bc2(1.0f));
 }
 
-// Second divided difference of e^{ix} at the three phases of each lane.
-__device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float2 &gx, float2 &gy) {
+// 2 sc g for each lane, g the second divided difference of e^{ix} at the full
+// phases 2 t1, 2 t2, 2 t3, from the half phases t.  With the half phases
+// sorted (lo <= mid <= hi) the edge midpoints of the full phases are lo + mid
+// and mid + hi and the half gaps mid - lo and hi - mid, each one operation.
+__device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float2 sc, float2 &gx,
+                                          float2 &gy) {
     float2 lo, hi, mid;
     lo.x = fminf(t1.x, t2.x);
     hi.x = fmaxf(t1.x, t2.x);
@@ -731,19 +749,19 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
     mid.y = fmaxf(lo.y, fminf(hi.y, t3.y));
     lo.y = fminf(lo.y, t3.y);
     hi.y = fmaxf(hi.y, t3.y);
-    const float2 D = add2(hi, neg2(lo));
-    const float2 h1 = mul2(bc2(0.5f), add2(mid, neg2(lo)));
-    const float2 h2 = mul2(bc2(0.5f), add2(hi, neg2(mid)));
-    const float2 c1 = add2(lo, h1), c2 = add2(mid, h2);
+    const float2 Dh = add2(hi, neg2(lo));  // half of the largest gap D
+    const float2 h1 = add2(mid, neg2(lo));
+    const float2 h2 = add2(hi, neg2(mid));
+    const float2 c1 = add2(lo, mid), c2 = add2(mid, hi);
     float2 s1, k1, s2, k2;
     s1 = make_float2(sin_fz(c1.x), sin_fz(c1.y));
     k1 = make_float2(cos_fz(c1.x), cos_fz(c1.y));
     s2 = make_float2(sin_fz(c2.x), sin_fz(c2.y));
     k2 = make_float2(cos_fz(c2.x), cos_fz(c2.y));
-    // 1/max(h1,.5), 1/max(h2,.5) and 1/D from one reciprocal of their product
+    // 1/max(h1,.5), 1/max(h2,.5) and 2/D from one reciprocal of their product
     const float2 a1 = make_float2(fmaxf(h1.x, 0.5f), fmaxf(h1.y, 0.5f));
     const float2 a2 = make_float2(fmaxf(h2.x, 0.5f), fmaxf(h2.y, 0.5f));
-    const float2 Dg = make_float2(fmaxf(D.x, 0.25f), fmaxf(D.y, 0.25f));
+    const float2 Dg = make_float2(fmaxf(Dh.x, 0.125f), fmaxf(Dh.y, 0.125f));
     const float2 p12 = mul2(a1, a2);
     const float2 pr = mul2(p12, Dg);
     const float2 r = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
@@ -761,11 +779,14 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
             sc2 = sel2(bx, by, sinc_series(h2), sc2);
         }
     }
-    const float2 iD = mul2(p12, r);
+    const float2 iD = mul2(mul2(p12, r), sc);  // 2 sc / D
     gx = mul2(fma2(sc1, s1, neg2(mul2(sc2, s2))), iD);
     gy = mul2(fma2(sc2, k2, neg2(mul2(sc1, k1))), iD);
-    if (D.x < 0.25f || D.y < 0.25f) {
-        // all three phases within 0.25 rad: Taylor series about the middle phase
+    if (Dh.x < 0.125f || Dh.y < 0.125f) {
+        // all three full phases within 0.25 rad: Taylor series about the middle
+        // phase, g = e^{2i mid} sum_n i^(n+2)/(n+2)! q_n(ya, yc) with the complete
+        // homogeneous q_n of the full-phase offsets 2 ya, 2 yc (2^n folded into
+        // the coefficients)
         const float2 ya = add2(lo, neg2(mid)), yc = add2(hi, neg2(mid));
         const float2 q1 = add2(ya, yc);
         const float2 ya2 = mul2(ya, ya);
@@ -776,17 +797,19 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
         const float2 q4 = fma2(yc, q3, ya4);
         const float2 q5 = fma2(yc, q4, mul2(ya4, ya));
         const float2 q6 = fma2(yc, q5, mul2(ya4, ya2));
-        const float2 re = fma2(q6, bc2(1.0f / 40320.0f),
-                               fma2(q4, bc2(-1.0f / 720.0f), fma2(q2, bc2(1.0f / 24.0f), bc2(-0.5f))));
-        const float2 im = fma2(q5, bc2(-1.0f / 5040.0f),
-                               fma2(q3, bc2(1.0f / 120.0f), mul2(q1, bc2(-1.0f / 6.0f))));
+        const float2 tsc = add2(sc, sc);
+        const float2 re = mul2(tsc, fma2(q6, bc2(1.0f / 630.0f),
+                                         fma2(q4, bc2(-1.0f / 45.0f), fma2(q2, bc2(1.0f / 6.0f), bc2(-0.5f)))));
+        const float2 im = mul2(tsc, fma2(q5, bc2(-2.0f / 315.0f),
+                                         fma2(q3, bc2(1.0f / 15.0f), mul2(q1, bc2(-1.0f / 3.0f)))));
+        const float2 m2 = add2(mid, mid);
         float2 sm, cm;
-        sm = make_float2(sin_fz(mid.x), sin_fz(mid.y));
-        cm = make_float2(cos_fz(mid.x), cos_fz(mid.y));
+        sm = make_float2(sin_fz(m2.x), sin_fz(m2.y));
+        cm = make_float2(cos_fz(m2.x), cos_fz(m2.y));
         const float2 sx = fma2(cm, re, neg2(mul2(sm, im)));
         const float2 sy = fma2(cm, im, mul2(sm, re));
-        gx = sel2(D.x < 0.25f, D.y < 0.25f, sx, gx);
-        gy = sel2(D.x < 0.25f, D.y < 0.25f, sy, gy);
+        gx = sel2(Dh.x < 0.125f, Dh.y < 0.125f, sx, gx);
+        gy = sel2(Dh.x < 0.125f, Dh.y < 0.125f, sy, gy);
     }
 }
 
@@ -800,21 +823,21 @@ __device__ __forceinline__ void ld22(const float2 *p, float2 &a, float2 &b) {
 
 template <bool FAST>
 __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const BinPk &B,
-                                        float2 (&acc)[8], float2 nk, float2 hkR, float2 sgh,
+                                        float2 (&acc)[8], float2 nkh, float2 hkRh, float2 sgh,
                                         const float (&hb)[3][K2P_HB], bool lo_ok, bool hi_ok,
                                         const double *__restrict__ xyz, int64_t nb) {
-    // far-field phase per facet: FP64 k u.c, reduced mod 2 pi
+    // far-field half phase per facet: FP64 k u.c / 2, reduced mod pi
     float2 rf;
     {
         const double2 k0 = *reinterpret_cast<const double2 *>(&P.kc[0][0]);
         const double2 k1 = *reinterpret_cast<const double2 *>(&P.kc[1][0]);
         const double2 k2 = *reinterpret_cast<const double2 *>(&P.kc[2][0]);
         const double ka = fma(B.uz, k2.x, fma(B.uy, k1.x, B.ux * k0.x));
-        const double nq = fma(ka, kInv2Pi, kMagic) - kMagic;
-        rf.x = (float)fma(-nq, kTwoPi, ka);
+        const double nq = fma(ka, kInvPi, kMagic) - kMagic;
+        rf.x = (float)fma(-nq, kPi, ka);
         const double kb = fma(B.uz, k2.y, fma(B.uy, k1.y, B.ux * k0.y));
-        const double nb = fma(kb, kInv2Pi, kMagic) - kMagic;
-        rf.y = (float)fma(-nb, kTwoPi, kb);
+        const double nb = fma(kb, kInvPi, kMagic) - kMagic;
+        rf.y = (float)fma(-nb, kPi, kb);
     }
     const float2 one = bc2(1.0f);
     float2 eps0, eps1, eps2, pb;
@@ -823,7 +846,7 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     // a = u . eps = s . eps - sg eps_z
     const float2 a = fma2(neg2(B.sg), eps2, fma2(B.sz, eps2, fma2(B.fy, eps1, mul2(B.fx, eps0))));
     const float2 opa = add2(one, a);
-    const float2 ph = fma2(mul2(hkR, fma2(neg2(a), a, pb)), opa, neg2(rf));
+    const float2 ph = fma2(mul2(hkRh, fma2(neg2(a), a, pb)), opa, neg2(rf));  // half phase
     const float2 opa2 = fma2(a, fma2(bc2(1.5f), a, one), fma2(bc2(-0.5f), pb, one));
     // The bin direction enters through s = u + sg z (sg = +1 in the hemisphere of
     // the incidence direction (0,0,-1), -1 in the other), which is small and known
@@ -848,77 +871,90 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
         ks1 = fma2(w1, opa2, mul2(n1, opa));
         ks2 = fma2(w2, opa2, mul2(n2, opa));
     }
-    float2 hkz_cf, hicf, hkxky_cf, inc0, inc1, inc2;
-    ld22(&P.hkz_cf, hkz_cf, hicf);
-    ld22(&P.hkxky_cf, hkxky_cf, inc0);
+    float2 kzc, inc0, inc1, inc2;
+    ld22(&P.kzc, kzc, inc0);
     ld22(&P.inc[1], inc1, inc2);
     const float2 so = mul2(B.sg, opa2);
     const float2 kx = fma2(so, inc0, ks0);
     const float2 ky = fma2(so, inc1, ks1);
     const float2 kz = fma2(so, inc2, ks2);
-    // aperture wave vector
+    // aperture wave vector (halved with the phases)
     float2 kxx, kyy;
     {
         float2 kp0, kp1;
         ld22(&P.kp[0], kp0, kp1);
-        kxx = fma2(nk, kx, kp0);
-        kyy = fma2(nk, ky, kp1);
+        kxx = fma2(nkh, kx, kp0);
+        kyy = fma2(nkh, ky, kp1);
     }
-    // polarisation matrix [[d, e], [-e, d]] (see k2_record for the forms) and
+    // Polarisation matrix [[d, e], [-e, d]] (see k2_record for the forms) and
     // the rotation into the scattering plane, with their normalisations folded
     // into one factor: with s = sqrt(tt) and hc = h / |h|,
     //   d = d1 / s, e = e1 / s, p = P1 / (|h| s), rr = R1 / (|h| s),
     // so A = p d + rr e = sc (P1 d1 + R1 e1) and B = sc (P1 e1 - R1 d1) with
-    // sc = 1 / (|h| tt) = rsqrt(|h|^2 tt^2).
+    // sc = 1 / (|h| tt) = rsqrt(|h|^2 tt^2).  The in-plane rotation of the set-up
+    // puts prop2 in the x-z plane (src/diff_mod.f90:540-559), so Ky = 0 up to
+    // rounding and d1 = (sqrt(1 - Ky^2)/2) (kzc tt - kz), e1 = (sqrt(1 - Ky^2)/2)(-kx kyc)
+    // (the Kx Ky term is below 1e-16 and left out); the common factor is in the
+    // record's amplitudes and sc in the divided difference.
     const float2 kyc = make_float2(fminf(fmaxf(ky.x, -0.999999f), 0.999999f),
                                    fminf(fmaxf(ky.y, -0.999999f), 0.999999f));
     const float2 tr = fma2(kx, kx, mul2(kz, kz));
     const float2 tt = make_float2(fmaxf(tr.x, kOneMinusClampSq), fmaxf(tr.y, kOneMinusClampSq));
-    const float2 d1 = fma2(hkz_cf, tt, neg2(mul2(kz, hicf)));
-    const float2 e1 = fma2(hkxky_cf, tt, neg2(mul2(mul2(kx, kyc), hicf)));
-    // h = inc x (kx, kyc, kz) = inc x (ks0, ks1 + kyc - ky, ks2)
-    const float2 qy = add2(ks1, add2(kyc, neg2(ky)));
-    float2 hx = fma2(inc1, ks2, neg2(mul2(inc2, qy)));
+    const float2 d1 = fma2(kzc, tt, neg2(kz));
+    const float2 e1 = mul2(neg2(kx), kyc);
+    // h = inc x (kx, ky, kz) = inc x ks
+    float2 hx = fma2(inc1, ks2, neg2(mul2(inc2, ks1)));
     float2 hy = fma2(inc2, ks0, neg2(mul2(inc0, ks2)));
-    float2 hz = fma2(inc0, qy, neg2(mul2(inc1, ks0)));
+    float2 hz = fma2(inc0, ks1, neg2(mul2(inc1, ks0)));
     // P1 = p |h| s = hy tt - kyc (hx kx + hz kz), from m = (-kx ky / s, s, -kz ky / s).
     // Where h is normal to q = (kx, kyc, kz), hx kx + hz kz = -hy kyc and
     // P1 = hy (tt + kyc^2) = hy |q|^2 = hy (|q| = 1 up to rounding; on the clamp
     // tt + kyc^2 = 1 - c^2 + c^2); the forward bodge takes the general form.
     float2 P1 = hy;
-    const float2 dinc = fma2(inc2, kz, fma2(inc1, kyc, mul2(inc0, kx)));
-    const bool bx = !(fabsf(dinc.x) < 0.999f), by = !(fabsf(dinc.y) < 0.999f);
-    if (bx || by) {
-        // the bodge direction in the s form: hs = uh + sgh z, uh . eps = hs . eps - sgh eps_z,
-        // h = inc x (R hs oh2 + nea oh)
-        const float2 hx_ = bc2(hb[0][B.hslot]), hy_ = bc2(hb[1][B.hslot]), hsz = bc2(hb[2][B.hslot]);
-        float2 ah = fma2(hsz, eps2, fma2(hy_, eps1, mul2(hx_, eps0)));
-        ah = fma2(neg2(sgh), eps2, ah);
-        const float2 oh = add2(one, ah);
-        const float2 oh2 = fma2(ah, fma2(bc2(1.5f), ah, one), fma2(bc2(-0.5f), pb, one));
-        const float2 vx = fma2(fma2(P.R[2], hsz, fma2(P.R[1], hy_, mul2(P.R[0], hx_))), oh2,
-                               mul2(P.nea[0], oh));
-        const float2 vy = fma2(fma2(P.R[5], hsz, fma2(P.R[4], hy_, mul2(P.R[3], hx_))), oh2,
-                               mul2(P.nea[1], oh));
-        const float2 vz = fma2(fma2(P.R[8], hsz, fma2(P.R[7], hy_, mul2(P.R[6], hx_))), oh2,
-                               mul2(P.nea[2], oh));
-        const float2 gx = fma2(inc1, vz, neg2(mul2(inc2, vy)));
-        const float2 gy = fma2(inc2, vx, neg2(mul2(inc0, vz)));
-        const float2 gz = fma2(inc0, vy, neg2(mul2(inc1, vx)));
-        const float2 gP = fma2(gy, tt, neg2(mul2(kyc, fma2(gx, kx, mul2(gz, kz)))));
-        hx = sel2(bx, by, gx, hx);
-        hy = sel2(bx, by, gy, hy);
-        hz = sel2(bx, by, gz, hz);
-        P1 = sel2(bx, by, gP, P1);
+    bool bx = false, by = false;
+    if (B.pole) {
+        // the forward bodge (src/diff_mod.f90:630-633) can apply only in bins near
+        // the poles; dinc = inc . (kx, kyc, kz)
+        const float2 dinc = fma2(inc2, kz, fma2(inc1, kyc, mul2(inc0, kx)));
+        bx = !(fabsf(dinc.x) < 0.999f);
+        by = !(fabsf(dinc.y) < 0.999f);
+        if (bx || by) {
+            // the bodge direction in the s form: hs = uh + sgh z, uh . eps = hs . eps - sgh eps_z,
+            // h = inc x (R hs oh2 + nea oh)
+            const float2 hx_ = bc2(hb[0][B.hslot]), hy_ = bc2(hb[1][B.hslot]),
+                         hsz = bc2(hb[2][B.hslot]);
+            float2 ah = fma2(hsz, eps2, fma2(hy_, eps1, mul2(hx_, eps0)));
+            ah = fma2(neg2(sgh), eps2, ah);
+            const float2 oh = add2(one, ah);
+            const float2 oh2 = fma2(ah, fma2(bc2(1.5f), ah, one), fma2(bc2(-0.5f), pb, one));
+            const float2 vx = fma2(fma2(P.R[2], hsz, fma2(P.R[1], hy_, mul2(P.R[0], hx_))), oh2,
+                                   mul2(P.nea[0], oh));
+            const float2 vy = fma2(fma2(P.R[5], hsz, fma2(P.R[4], hy_, mul2(P.R[3], hx_))), oh2,
+                                   mul2(P.nea[1], oh));
+            const float2 vz = fma2(fma2(P.R[8], hsz, fma2(P.R[7], hy_, mul2(P.R[6], hx_))), oh2,
+                                   mul2(P.nea[2], oh));
+            const float2 gx = fma2(inc1, vz, neg2(mul2(inc2, vy)));
+            const float2 gy = fma2(inc2, vx, neg2(mul2(inc0, vz)));
+            const float2 gz = fma2(inc0, vy, neg2(mul2(inc1, vx)));
+            const float2 gP = fma2(gy, tt, neg2(mul2(kyc, fma2(gx, kx, mul2(gz, kz)))));
+            hx = sel2(bx, by, gx, hx);
+            hy = sel2(bx, by, gy, hy);
+            hz = sel2(bx, by, gz, hz);
+            P1 = sel2(bx, by, gP, P1);
+        }
     }
-    const float2 hn2 = fma2(hz, hz, fma2(hy, hy, mul2(hx, hx)));
-    const float2 ht = mul2(mul2(hn2, tt), tt);
-    const float2 sc = make_float2(rsqrt_fz(ht.x), rsqrt_fz(ht.y));
-    // inside the clamp evo2 = (-kz, 0, kx) / s, so R1 = rr |h| s = hz kx - hx kz
-    float2 R1 = fma2(hz, kx, neg2(mul2(hx, kz)));
     const bool cx = tt.x <= kOneMinusClampSq, cy = tt.y <= kOneMinusClampSq;
+    float2 rc = bc2(0.0f);
     if (cx || cy) {
-        // a lane on the clamp: evo2 = normalise(k x m) with the clamped ky, R1 = s (h . evo2)
+        // a lane on the clamp: outside the bodge, h = inc x (kx, kyc, kz) takes the
+        // clamped ky (q_y = ks1 + kyc - ky); evo2 = normalise(k x m) with the clamped
+        // ky, R1 = s (h . evo2)
+        const float2 qy = add2(ks1, add2(kyc, neg2(ky)));
+        const float2 fx = fma2(inc1, ks2, neg2(mul2(inc2, qy)));
+        const float2 fz = fma2(inc0, qy, neg2(mul2(inc1, ks0)));
+        const bool ux = cx && !bx, uy = cy && !by;
+        hx = sel2(ux, uy, fx, hx);
+        hz = sel2(ux, uy, fz, hz);
         const float2 rs = make_float2(rsqrtf(tt.x), rsqrtf(tt.y));
         const float2 s = mul2(tt, rs), kyrs = mul2(kyc, rs);
         const float2 m0 = neg2(mul2(kx, kyrs)), m1 = s, m2 = neg2(mul2(kz, kyrs));
@@ -927,13 +963,18 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
         float2 ez = fma2(kx, m1, neg2(mul2(kyc, m0)));
         const float2 en2 = fma2(ez, ez, fma2(ey, ey, mul2(ex, ex)));
         const float2 ne = make_float2(cx ? rsqrtf(en2.x) : 1.0f, cy ? rsqrtf(en2.y) : 1.0f);
-        const float2 rc = mul2(mul2(s, ne), fma2(hz, ez, fma2(hy, ey, mul2(hx, ex))));
-        R1 = sel2(cx, cy, rc, R1);
+        rc = mul2(mul2(s, ne), fma2(hz, ez, fma2(hy, ey, mul2(hx, ex))));
     }
-    const float2 A = mul2(sc, fma2(P1, d1, mul2(R1, e1)));
-    const float2 Bc = mul2(sc, fma2(P1, e1, neg2(mul2(R1, d1))));
-    // aperture integral (after the polarisation block, so that only A and B
-    // stay live across it)
+    const float2 hn2 = fma2(hz, hz, fma2(hy, hy, mul2(hx, hx)));
+    const float2 ht = mul2(mul2(hn2, tt), tt);
+    const float2 sc = make_float2(rsqrt_fz(ht.x), rsqrt_fz(ht.y));
+    // inside the clamp evo2 = (-kz, 0, kx) / s, so R1 = rr |h| s = hz kx - hx kz
+    float2 R1 = fma2(hz, kx, neg2(mul2(hx, kz)));
+    if (cx || cy) R1 = sel2(cx, cy, rc, R1);
+    const float2 A = fma2(P1, d1, mul2(R1, e1));
+    const float2 Bc = fma2(P1, e1, neg2(mul2(R1, d1)));
+    // aperture integral on the half phases (after the polarisation block, so
+    // that only A and B stay live across it): 2 sc g
     float2 gx, gy;
     {
         float2 vx0, vx1, vx2, vy0, vy1, vy2;
@@ -943,7 +984,7 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
         const float2 t1 = fma2(kyy, vy0, fma2(kxx, vx0, ph));
         const float2 t2 = fma2(kyy, vy1, fma2(kxx, vx1, ph));
         const float2 t3 = fma2(kyy, vy2, fma2(kxx, vx2, ph));
-        tri_dd_pk(t1, t2, t3, gx, gy);
+        tri_dd_pk(t1, t2, t3, sc, gx, gy);
     }
     // [[A, B], [-B, A]] is diagonal in the circular basis: with z = A - iB the
     // columns' u+ take z, their u- take conj(z).  q+ = g z, q- = g conj(z).
@@ -1010,6 +1051,7 @@ struct K2PkArgs {
     float k;
     float hkR;
     float sgh;   // +1 when the bodge row theta_i lies in the hemisphere of (0,0,-1), else -1
+    const unsigned *epsmax;  // float bits of a bound of |com| / R over the records
     float *ws;
     unsigned long long *counter;
     int *err;
@@ -1031,7 +1073,11 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
     uint32_t parity = 0;  // bit s: phase of stage s
     const int64_t total = P.item_pre[P.nseg];
     constexpr int64_t TILE = (int64_t)K2_THREADS * BPT;
-    const float2 nk = bc2(-P.k), hkR = bc2(P.hkR), sgh = bc2(P.sgh);
+    // half phases: -k/2 and k R / 4
+    const float2 nkh = bc2(-0.5f * P.k), hkRh = bc2(0.5f * P.hkR), sgh = bc2(P.sgh);
+    // bins with |uz| below pole_cos are out of reach of the forward bodge for every
+    // record: |inc . k - (-uz)| <= 2 |com| / R for the direction k from a facet centre
+    const float pole_cos = 0.999f - 2.0f * __uint_as_float(*P.epsmax) - 1e-5f;
     for (;;) {
         if (tid == 0) s_item = (long long)atomicAdd(P.counter, 1ull);
         __syncthreads();
@@ -1070,6 +1116,7 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
             const double sg = bd[q].uz <= 0.0 ? 1.0 : -1.0;
             bd[q].sz = bc2((float)(bd[q].uz + sg));
             bd[q].sg = bc2((float)sg);
+            bd[q].pole = !(fabs(bd[q].uz) < (double)pole_cos);
             const int64_t oh = (o % P.nphi) + P.nphi * P.theta_i;
             const double Xh = P.xyz[oh], Yh = P.xyz[P.nb + oh], Zh = P.xyz[2 * P.nb + oh];
             const double irh = 1.0 / sqrt(Xh * Xh + Yh * Yh + Zh * Zh);
@@ -1140,7 +1187,7 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
                 }
 #pragma unroll
                 for (int q = 0; q < BPT; q++)
-                    k2_pair<FAST>(sbuf[st][j], fv, bd[q], acc[q], nk, hkR, sgh, s_hb, lo_ok && valid[q],
+                    k2_pair<FAST>(sbuf[st][j], fv, bd[q], acc[q], nkh, hkRh, sgh, s_hb, lo_ok && valid[q],
                                   hi_ok && valid[q], P.xyz, P.nb);
             };
             if (FAST) {
@@ -1471,6 +1518,7 @@ struct K2Setup {
     int64_t *beam_off = nullptr;
     int64_t *ext_off = nullptr;
     int *err = nullptr;
+    unsigned *epsmax = nullptr;  // float bits of a bound of |com| / R over the records
 };
 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -1500,6 +1548,7 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
     S.beam_off = (int64_t *)(base + o_bo);
     S.ext_off = (int64_t *)(base + o_eo);
     S.err = (int *)(base + o_err);
+    S.epsmax = (unsigned *)(base + o_err + 8);
     void *tmp = base + o_tmp;
     // records (or record pairs; an even count so the last pair is whole)
     const int64_t nrec2 = (max_recs + 1) & ~(int64_t)1;
@@ -1531,7 +1580,7 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
         PBT_CUDA_TRY(cudaEventRecord(ctx->stage_ev, st));
         ctx->stage_pending = true;
     }
-    PBT_CUDA_TRY(cudaMemsetAsync(S.err, 0, sizeof(int), st));
+    PBT_CUDA_TRY(cudaMemsetAsync(S.err, 0, 16, st));  // error flags and epsmax
     RefSrc src{d_beam, d_ext, S.beam_off, S.ext_off, S.refbase, norient};
     const int th = 256;
     k2_count_kernel<<<(unsigned)((nrefs + 1 + th - 1) / th), th, 0, st>>>(src, nrefs, d_face_off,
@@ -1541,7 +1590,7 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
     if (nrefs > 0)
         k2_setup_kernel<<<(unsigned)((nrefs + th - 1) / th), th, 0, st>>>(
             src, nrefs, d_verts, nverts, d_face_off, d_face_vi, S.start, waveno, lambda, fast_diff,
-            S.recs, S.pairs, S.fovs, S.err);
+            S.recs, S.pairs, S.fovs, S.err, S.epsmax);
     ctx->launches += 3;
     PBT_CUDA_TRY(cudaGetLastError());
     return PBT_OK;
@@ -1717,6 +1766,7 @@ int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, in
         B.k = A.k;
         B.hkR = A.hkR;
         B.sgh = A.sgh;
+        B.epsmax = S.epsmax;
         B.ws = ws;
         B.counter = counter;
         B.err = S.err;
