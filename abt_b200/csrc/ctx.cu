@@ -198,7 +198,7 @@ extern "C" int pbt_ctx_destroy(pbt_ctx *ctx) {
         cudaStreamSynchronize(ctx->stream);
         DevBuf *bufs[] = {&ctx->d_fac, &ctx->d_edge, &ctx->d_out,  &ctx->d_mu,
                           &ctx->d_m1,  &ctx->d_misc, &ctx->d_in,   &ctx->d_rec,
-                          &ctx->d_ws,  &ctx->d_scan, &ctx->d_items, &ctx->d_k1part, &ctx->grid.xyz,
+                          &ctx->d_ws,  &ctx->d_scan, &ctx->d_items, &ctx->d_tk, &ctx->d_k1part, &ctx->grid.xyz,
                           &ctx->grid.phitab,
                           &ctx->grid.thtab, &ctx->grid.wbin, &ctx->grid.wphi,
                           &ctx->grid.fast_perm, &ctx->grid.fast_cone};

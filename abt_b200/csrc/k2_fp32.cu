@@ -406,6 +406,61 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
     return false;
 }
 
+// Work items of one (segment, bin tile) are facet splits.  Each adds its FP64
+// sums into the workspace after the previous split of the same tile: ticket
+// tk counts the splits added so far (split s waits for tk >= s, adds, and sets
+// tk = s + 1), so the sum over splits is in split order and the result is the
+// same from run to run.  The item of split s - 1 has the lower item index, so
+// it was claimed earlier by a running CTA and never waits on split s.  A wait
+// that gives up (2 s of global time or 2^26 polls), or a CTA whose bulk copy
+// timed out, sets the ticket to kTicketPoison: later splits of the tile then
+// skip their add at once and the call reports PBT_ETIMEOUT.
+constexpr unsigned kTicketPoison = 0xffffffffu;
+__device__ __forceinline__ bool ticket_wait(const unsigned *tk, unsigned s) {
+    uint64_t t0 = 0;
+    for (uint32_t it = 0; it < (1u << 26); ++it) {
+        unsigned v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(tk) : "memory");
+        if (v >= s) return v != kTicketPoison;
+        if (it == 0) t0 = gtimer();
+        else if ((it & 255) == 0 && gtimer() - t0 > kWaitLimitNs) return false;
+    }
+    return false;
+}
+
+// The item's sums (lin[bin][8], FP64) into the workspace in split order (see
+// ticket_wait); every thread of the CTA calls this.
+template <int BPT>
+__device__ __forceinline__ void ordered_add(double *__restrict__ out, int64_t nb, unsigned *tk,
+                                            unsigned split, const bool (&valid)[BPT],
+                                            const int64_t (&bin)[BPT], const double (&lin)[BPT][8],
+                                            int *s_ok, int *err) {
+    if (threadIdx.x == 0) *s_ok = ticket_wait(tk, split);
+    __syncthreads();
+    const bool go = *s_ok != 0;
+    if (go) {
+        __threadfence();
+#pragma unroll
+        for (int q = 0; q < BPT; q++)
+            if (valid[q])
+#pragma unroll
+                for (int cc = 0; cc < 8; cc++) {
+                    double *o = out + cc * nb + bin[q];
+                    *o = __ldcg(o) + lin[q][cc];
+                }
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (go) {
+            atomicMax(tk, split + 1u);
+        } else {
+            atomicOr(err, 4);
+            atomicMax(tk, kTicketPoison);
+        }
+    }
+}
+
 struct K2MainArgs {
     const K2Rec *recs;
     const K2Fov *fovs;
@@ -420,7 +475,8 @@ struct K2MainArgs {
     float k;      // wavenumber
     float hkR;    // k R / 2
     float sgh;    // +1 when the bodge row theta_i lies in the hemisphere of (0,0,-1), else -1
-    float *ws;    // [seg][8][nb]
+    double *ws;   // [seg][8][nb]
+    unsigned *tickets;  // [seg][tile], splits added so far
     unsigned long long *counter;
     int *err;
 };
@@ -548,6 +604,7 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
     __shared__ __align__(128) K2Rec sbuf[K2_NST][K2_CH];
     __shared__ __align__(8) uint64_t bars[K2_NST];
     __shared__ long long s_item;
+    __shared__ int s_ok;
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int s = 0; s < K2_NST; s++) mbar_init(smem_u32(&bars[s]), 1);
@@ -653,9 +710,11 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
                           (uint32_t)(n2 * sizeof(K2Rec)), smem_u32(&bars[st]));
             }
         }
+        unsigned *tk = P.tickets + seg * P.ntiles + tile;
         if (timed_out) {
             if (tid == 0) {
                 atomicOr(P.err, 4);
+                atomicMax(tk, kTicketPoison);
                 // bounded wait for this CTA's bulk copies still in flight
                 for (int64_t c2 = c_out; c2 < min(nchunk, c_out + K2_NST); c2++) {
                     const int s2 = (int)(c2 % K2_NST);
@@ -664,12 +723,8 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
             }
             return;
         }
-        float *out = P.ws + seg * 8 * P.nb;
-#pragma unroll
-        for (int q = 0; q < BPT; q++)
-            if (valid[q])
-#pragma unroll
-                for (int cc = 0; cc < 8; cc++) atomicAdd(out + cc * P.nb + bin[q], (float)acc64[q][cc]);
+        ordered_add<BPT>(P.ws + seg * 8 * P.nb, P.nb, tk, (unsigned)split, valid, bin, acc64, &s_ok,
+                         P.err);
     }
 }
 
@@ -1052,7 +1107,8 @@ struct K2PkArgs {
     float hkR;
     float sgh;   // +1 when the bodge row theta_i lies in the hemisphere of (0,0,-1), else -1
     const unsigned *epsmax;  // float bits of a bound of |com| / R over the records
-    float *ws;
+    double *ws;         // [seg][8][nb]
+    unsigned *tickets;  // [seg][tile], splits added so far
     unsigned long long *counter;
     int *err;
 };
@@ -1064,6 +1120,7 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
     __shared__ long long s_item;
     __shared__ unsigned s_keep[2];  // is_fast_diff: records of the stage not culled for the tile
     __shared__ float s_hb[3][K2P_HB];  // forward-bodge bin directions of this CTA's bins (s form)
+    __shared__ int s_ok;
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int s = 0; s < K2_NST; s++) mbar_init(smem_u32(&bars[s]), 1);
@@ -1224,9 +1281,11 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
                           (uint32_t)(n2 * sizeof(K2Pair)), smem_u32(&bars[st]));
             }
         }
+        unsigned *tk = P.tickets + seg * P.ntiles + tile;
         if (timed_out) {
             if (tid == 0) {
                 atomicOr(P.err, 4);
+                atomicMax(tk, kTicketPoison);
                 // bounded wait for this CTA's bulk copies still in flight
                 for (int64_t c2 = c_out; c2 < min(nchunk, c_out + K2_NST); c2++) {
                     const int s2 = (int)(c2 % K2_NST);
@@ -1236,19 +1295,22 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
             }
             return;
         }
-        float *out = P.ws + seg * 8 * P.nb;
+        // back from the circular basis: a1 = (U+ + U-)/2, a2 = -i (U+ - U-)/2
+        double lin[BPT][8];
 #pragma unroll
-        for (int q = 0; q < BPT; q++)
-            if (valid[q]) {
-                // back from the circular basis: a1 = (U+ + U-)/2, a2 = -i (U+ - U-)/2
-                const double *u = acc64[q];
-                const double lin[8] = {0.5 * (u[0] + u[2]), 0.5 * (u[1] + u[3]),
-                                       0.5 * (u[1] - u[3]), 0.5 * (u[2] - u[0]),
-                                       0.5 * (u[4] + u[6]), 0.5 * (u[5] + u[7]),
-                                       0.5 * (u[5] - u[7]), 0.5 * (u[6] - u[4])};
-#pragma unroll
-                for (int cc = 0; cc < 8; cc++) atomicAdd(out + cc * P.nb + bin[q], (float)lin[cc]);
-            }
+        for (int q = 0; q < BPT; q++) {
+            const double *u = acc64[q];
+            lin[q][0] = 0.5 * (u[0] + u[2]);
+            lin[q][1] = 0.5 * (u[1] + u[3]);
+            lin[q][2] = 0.5 * (u[1] - u[3]);
+            lin[q][3] = 0.5 * (u[2] - u[0]);
+            lin[q][4] = 0.5 * (u[4] + u[6]);
+            lin[q][5] = 0.5 * (u[5] + u[7]);
+            lin[q][6] = 0.5 * (u[5] - u[7]);
+            lin[q][7] = 0.5 * (u[6] - u[4]);
+        }
+        ordered_add<BPT>(P.ws + seg * 8 * P.nb, P.nb, tk, (unsigned)split, valid, bin, lin, &s_ok,
+                         P.err);
     }
 }
 
@@ -1284,14 +1346,14 @@ __device__ __forceinline__ void mueller16d(const Zd *S, double mu[16]) {
 
 // Amplitude of segment seg at bin o as reference-layout complex 2x2 (with
 // T(phi) applied and scaled by sc), common phase e^{ik|X|} omitted.
-__device__ __forceinline__ void ws_ampl(const float *ws, int64_t seg, int64_t nb, int64_t o, double cp,
+__device__ __forceinline__ void ws_ampl(const double *ws, int64_t seg, int64_t nb, int64_t o, double cp,
                                         double sp, double sc, Zd S[4]) {
-    const float *w = ws + seg * 8 * nb + o;
+    const double *w = ws + seg * 8 * nb + o;
     Zd a[4];
 #pragma unroll
     for (int c = 0; c < 4; c++) {
-        a[c].re = (double)w[(2 * c) * nb];
-        a[c].im = (double)w[(2 * c + 1) * nb];
+        a[c].re = w[(2 * c) * nb];
+        a[c].im = w[(2 * c + 1) * nb];
     }
     // (S T)(a,b) = S(a,1) T(1,b) + S(a,2) T(2,b); T = [[-s, -c], [c, -s]]
     // order (1,1),(2,1),(1,2),(2,2): a[0]=S11 a[1]=S21 a[2]=S12 a[3]=S22
@@ -1316,9 +1378,12 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 }
 
 // Pre-pass of -scaling: per-orientation scatt_beam / scatt_ext sums.
-__global__ void k2_scatt_be_kernel(const float *__restrict__ ws, int64_t no, int64_t o0, int64_t nb,
+// Per-orientation sums over the bins are reduced in two fixed-order steps (a
+// block sum into part[(q K + k) nblk + block], then k2_part_sum_kernel over the
+// blocks in order), so they are the same from run to run.
+__global__ void k2_scatt_be_kernel(const double *__restrict__ ws, int64_t no, int64_t o0, int64_t nb,
                                    int64_t nphi, const double *__restrict__ phitab, double waveno,
-                                   const double *__restrict__ wbin, double *__restrict__ sums) {
+                                   const double *__restrict__ wbin, double *__restrict__ part) {
     __shared__ double red[32];
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = o < nb;
@@ -1335,10 +1400,24 @@ __global__ void k2_scatt_be_kernel(const float *__restrict__ ws, int64_t no, int
         const double vb = block_sum(W * mb[0], red);
         const double ve = block_sum(W * me[0], red);
         if (threadIdx.x == 0) {
-            atomicAdd(&sums[2 * (o0 + q)], vb);
-            atomicAdd(&sums[2 * (o0 + q) + 1], ve);
+            part[(2 * q) * gridDim.x + blockIdx.x] = vb;
+            part[(2 * q + 1) * gridDim.x + blockIdx.x] = ve;
         }
     }
+    (void)o0;
+}
+// out[k0 + r] = sum over b of part[r nblk + b] in block order, r < nrow (one warp
+// per row: lanes take blocks b = lane + 32 i in order, then a fixed shuffle tree).
+__global__ void k2_part_sum_kernel(const double *__restrict__ part, int64_t nrow, int64_t nblk,
+                                   double *__restrict__ out) {
+    const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= nrow) return;
+    double v = 0.0;
+    for (int64_t b = lane; b < nblk; b += 32) v += part[r * nblk + b];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (lane == 0) out[r] = v;
 }
 
 // sqrt(scatt_part / energy_part) per orientation (src/outputs_mod.f90:151,154)
@@ -1353,12 +1432,12 @@ __global__ void k2_scale_kernel(double *__restrict__ scale, const pbt_output_par
 
 // Main epilogue: Mueller sum over the chunk's orientations and per-orientation
 // weighted sums  red[o] = {scatt, scatt_beam, scatt_ext, g_num, g_num_beam, g_num_ext}.
-__global__ void k2_epi_kernel(const float *__restrict__ ws, int64_t no, int64_t o0, int64_t nb,
+__global__ void k2_epi_kernel(const double *__restrict__ ws, int64_t no, int64_t o0, int64_t nb,
                               int64_t nphi, const double *__restrict__ phitab,
                               const double *__restrict__ cth, double waveno,
                               const double *__restrict__ wbin, int64_t back_bin,
                               const double *__restrict__ scale, double *__restrict__ mu_sum,
-                              double *__restrict__ redo, double *__restrict__ bs) {
+                              double *__restrict__ part, double *__restrict__ bs) {
     __shared__ double red[32];
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = o < nb;
@@ -1391,7 +1470,7 @@ __global__ void k2_epi_kernel(const float *__restrict__ ws, int64_t no, int64_t 
 #pragma unroll
         for (int k = 0; k < 6; k++) {
             const double s = block_sum(v[k], red);
-            if (threadIdx.x == 0) atomicAdd(&redo[6 * og + k], s);
+            if (threadIdx.x == 0) part[(6 * q + k) * gridDim.x + blockIdx.x] = s;
         }
         if (in && o == back_bin) bs[og] = m[0] * 4.0 * kPiRef / (waveno * waveno);
     }
@@ -1456,7 +1535,7 @@ __global__ void k2_phi_int_kernel(const double *__restrict__ mu, const double *_
 }
 
 // FP32 diff_main output: reference-layout complex(8) grids, e^{ik|X|} S' T(phi).
-__global__ void k2_ampl_out_kernel(const float *__restrict__ ws, int64_t nb, int64_t nphi,
+__global__ void k2_ampl_out_kernel(const double *__restrict__ ws, int64_t nb, int64_t nphi,
                                    const double *__restrict__ phitab, const double *__restrict__ xyz,
                                    double waveno, double *__restrict__ afb, double *__restrict__ afe) {
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1715,7 +1794,7 @@ int k2_fast_tiles(pbt_ctx *ctx, cudaStream_t st, int64_t tile) {
 }
 
 int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, int64_t no,
-                 double lambda, int fast_diff, const K2Plan &plan, float *ws, int64_t *seg_rec,
+                 double lambda, int fast_diff, const K2Plan &plan, double *ws, int64_t *seg_rec,
                  int64_t *item_pre, unsigned long long *counter) {
     const GridCache &g = ctx->grid;
     const int64_t tile = (int64_t)K2_THREADS * plan.bpt;
@@ -1728,7 +1807,11 @@ int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, in
     k2_plan_kernel<<<1, 32, 0, st>>>(S.start, S.refbase, S.beam_off, o0, no, plan.rpi, ntiles,
                                      seg_rec, item_pre, counter);
     ctx->launches++;
-    PBT_CUDA_TRY(cudaMemsetAsync(ws, 0, (size_t)2 * no * 8 * g.nb * sizeof(float), st));
+    PBT_CUDA_TRY(cudaMemsetAsync(ws, 0, (size_t)2 * no * 8 * g.nb * sizeof(double), st));
+    // split tickets of every (segment, tile)
+    const size_t tk_bytes = (size_t)2 * no * ntiles * sizeof(unsigned);
+    PBT_TRY(ctx->d_tk.ensure(tk_bytes));
+    PBT_CUDA_TRY(cudaMemsetAsync(ctx->d_tk.p, 0, tk_bytes, st));
     const double waveno = 2.0 * kPiRef / lambda;
     K2MainArgs A;
     A.recs = S.recs;
@@ -1746,6 +1829,7 @@ int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, in
     A.hkR = (float)(0.5 * waveno * kFarR);
     A.sgh = -cos(g.theta[g.theta_i]) <= 0.0 ? 1.0f : -1.0f;  // sign rule of the bin set-up
     A.ws = ws;
+    A.tickets = ctx->d_tk.as<unsigned>();
     A.counter = counter;
     A.err = S.err;
     if (plan.variant == 1) {
@@ -1768,6 +1852,7 @@ int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, in
         B.sgh = A.sgh;
         B.epsmax = S.epsmax;
         B.ws = ws;
+        B.tickets = A.tickets;
         B.counter = counter;
         B.err = S.err;
         if (plan.bpt == 1)
@@ -1850,9 +1935,9 @@ int k2_batch_begin(pbt_ctx *ctx, cudaStream_t st, int64_t norient, int64_t max_r
     const int64_t nb = g.nb;
     B.norient = norient;
     B.plan = k2_plan_for(ctx);
-    // orientation chunks of the workspace, capped at 8 GiB
-    const size_t per_orient = (size_t)2 * 8 * nb * sizeof(float);
-    const size_t cap = (size_t)8 << 30;
+    // orientation chunks of the FP64 workspace, capped at 16 GiB
+    const size_t per_orient = (size_t)2 * 8 * nb * sizeof(double);
+    const size_t cap = (size_t)16 << 30;
     B.wchunk = std::max<int64_t>(1, std::min<int64_t>(max_run, (int64_t)(cap / per_orient)));
     const int64_t chunk = B.wchunk;
     // d_ws: workspace | mu_sum | per-orient red (6) | bs | scale (2) | per-orient params | seg/items
@@ -1861,12 +1946,15 @@ int k2_batch_begin(pbt_ctx *ctx, cudaStream_t st, int64_t norient, int64_t max_r
                  o_sc = align_up(o_bs + norient * 8), o_pp = align_up(o_sc + 2 * norient * 8),
                  o_seg = align_up(o_pp + norient * sizeof(pbt_output_params)),
                  o_it = align_up(o_seg + (2 * chunk + 1) * 8), o_cnt = align_up(o_it + (2 * chunk + 1) * 8),
-                 o_err = align_up(o_cnt + 64), o_end = align_up(o_err + 64);
+                 o_err = align_up(o_cnt + 64),
+                 o_part = align_up(o_err + 64),
+                 o_end = align_up(o_part + (size_t)6 * chunk * ((nb + 255) / 256) * 8);
     PBT_TRY(ctx->d_ws.ensure(o_end));
     char *base = ctx->d_ws.as<char>();
     B.err = (int *)(base + o_err);
+    B.part = (double *)(base + o_part);
     PBT_CUDA_TRY(cudaMemsetAsync(B.err, 0, sizeof(int), st));
-    B.ws = (float *)(base + o_ws);
+    B.ws = (double *)(base + o_ws);
     B.mu_sum = (double *)(base + o_mu);
     B.redo = (double *)(base + o_red);
     B.bs = (double *)(base + o_bs);
@@ -1907,14 +1995,18 @@ int k2_batch_add(pbt_ctx *ctx, cudaStream_t st, K2Batch &B, int64_t o0, int64_t 
         const int64_t og = o0 + l0;  // global orientation of the workspace's first slot
         if (scaling) {
             k2_scatt_be_kernel<<<egrid, eb, 0, st>>>(B.ws, n, og, nb, nphi, phitab, waveno,
-                                                     g.wbin.as<double>(), B.scale);
+                                                     g.wbin.as<double>(), B.part);
+            k2_part_sum_kernel<<<(unsigned)((2 * n + 3) / 4), 128, 0, st>>>(B.part, 2 * n, egrid,
+                                                                          B.scale + 2 * og);
             k2_scale_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(B.scale, d_params_in, og, n);
-            ctx->launches += 2;
+            ctx->launches += 3;
         }
         k2_epi_kernel<<<egrid, eb, 0, st>>>(B.ws, n, og, nb, nphi, phitab, cth, waveno,
                                             g.wbin.as<double>(), back_bin, scaling ? B.scale : nullptr,
-                                            B.mu_sum, B.redo, B.bs);
-        ctx->launches++;
+                                            B.mu_sum, B.part, B.bs);
+        k2_part_sum_kernel<<<(unsigned)((6 * n + 3) / 4), 128, 0, st>>>(B.part, 6 * n, egrid,
+                                                                      B.redo + 6 * og);
+        ctx->launches += 2;
         PBT_CUDA_TRY(cudaGetLastError());
     }
     // the run's error flags (its set-up buffer is reused by the next run)
@@ -1972,11 +2064,11 @@ int k2_diff_main_impl(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *d_beam, 
     const int64_t hbo[2] = {0, nbeam}, heo[2] = {0, next};
     PBT_TRY(k2_prepare(ctx, st, 1, d_beam, hbo, d_ext, heo, d_verts, nverts, d_face_off, d_face_vi,
                        nfaces, max_face_nv(h_face_off, nfaces), lambda, fast_diff, plan.variant, S));
-    const size_t o_ws = 0, o_seg = align_up(o_ws + (size_t)2 * 8 * nb * sizeof(float)),
+    const size_t o_ws = 0, o_seg = align_up(o_ws + (size_t)2 * 8 * nb * sizeof(double)),
                  o_it = align_up(o_seg + 3 * 8), o_cnt = align_up(o_it + 3 * 8), o_end = align_up(o_cnt + 64);
     PBT_TRY(ctx->d_ws.ensure(o_end));
     char *base = ctx->d_ws.as<char>();
-    float *ws = (float *)(base + o_ws);
+    double *ws = (double *)(base + o_ws);
     PBT_TRY(k2_run_chunk(ctx, st, S, 0, 1, lambda, fast_diff, plan, ws, (int64_t *)(base + o_seg),
                          (int64_t *)(base + o_it), (unsigned long long *)(base + o_cnt)));
     const double waveno = 2.0 * kPiRef / lambda;

@@ -134,6 +134,7 @@ struct pbt_ctx {
     pbt::GridCache grid;
     // scratch (grow-only)
     pbt::DevBuf d_fac, d_edge, d_out, d_mu, d_m1, d_misc, d_in, d_rec, d_ws, d_scan, d_items;
+    pbt::DevBuf d_tk;  // split tickets of the FP32 kernel's (segment, tile) pairs
     pbt::DevBuf d_k1part;  // FP64 drop-in: partial grids of the facet splits (small grids)
     pbt::HostBuf h_stage;
     cudaEvent_t stage_ev = nullptr;  // last copy out of h_stage (wait before reuse)
@@ -194,8 +195,9 @@ struct K2Plan {
 struct K2Batch {
     int64_t norient = 0, wchunk = 1;
     K2Plan plan;
-    float *ws = nullptr;
+    double *ws = nullptr;
     double *mu_sum = nullptr, *redo = nullptr, *bs = nullptr, *scale = nullptr;
+    double *part = nullptr;  // per-block partial sums of the epilogue (6 per orientation and block)
     pbt_output_params *pp = nullptr;
     int64_t *seg_rec = nullptr, *item_pre = nullptr;
     unsigned long long *counter = nullptr;
