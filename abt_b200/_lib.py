@@ -43,7 +43,7 @@ EXPORTS = ("pbt_ctx_create", "pbt_ctx_destroy", "pbt_last_error_string", "pbt_ve
            "pbt_make_far_field_bins_c", "pbt_selftest_bounded_wait_c", "pbt_diff_batch_list_c",
            "pbt_particle_create", "pbt_particle_info", "pbt_particle_verts",
            "pbt_particle_destroy", "pbt_trace_orientation_c", "pbt_trace_batch_c", "pbt_trace_sizes",
-           "pbt_trace_copy", "pbt_trace_destroy")
+           "pbt_trace_copy", "pbt_trace_destroy", "pbt_test_fail_next_alloc")
 
 # pbt_trace_params / pbt_trace_energy
 TRACE_PARAMS_DTYPE = np.dtype([("lambda", "<f8"), ("rbi", "<f8"), ("ibi", "<f8"), ("rec", "<i8"),
@@ -101,6 +101,7 @@ def lib():
         "pbt_beamlist_free": (C, [P]),
         "pbt_make_far_field_bins_c": (C, [P, I64, P, I64, P, P, P]),
         "pbt_selftest_bounded_wait_c": (C, [P, I32]),
+        "pbt_test_fail_next_alloc": (C, [I32]),
         "pbt_diff_batch_list_c": (C, [P, I64, P, P, P, P, P, I64, P, P, I64, P, I64, P, I64, D,
                                       I32, I32, I32, P, P, P, P, P]),
         "pbt_graph_kernel_count": (I64, [P]),

@@ -2,6 +2,8 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <atomic>
+
 #include "pbt_internal.h"
 
 namespace pbt {
@@ -19,10 +21,20 @@ void set_error(const char *fmt, ...) {
 void clear_error() { g_last_error.clear(); }
 const char *last_error() { return g_last_error.c_str(); }
 
+// pending injected allocation failures (pbt_test_fail_next_alloc)
+static std::atomic<int32_t> g_fail_allocs{0};
+
 int DevBuf::ensure(size_t bytes) {
     if (bytes <= cap && p) return PBT_OK;
     release();
     size_t want = bytes < 256 ? 256 : bytes;
+    int32_t pending = g_fail_allocs.load();
+    while (pending > 0 && !g_fail_allocs.compare_exchange_weak(pending, pending - 1)) {
+    }
+    if (pending > 0) {
+        set_error("cudaMalloc(%zu) failed: out of memory (injected by pbt_test_fail_next_alloc)", want);
+        return PBT_ENOMEM;
+    }
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         p = nullptr;
@@ -223,3 +235,7 @@ extern "C" int pbt_ctx_destroy(pbt_ctx *ctx) {
 }
 
 extern "C" int64_t pbt_last_launch_count(pbt_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+extern "C" int pbt_test_fail_next_alloc(int32_t count) {
+    return pbt::g_fail_allocs.exchange(count > 0 ? count : 0);
+}

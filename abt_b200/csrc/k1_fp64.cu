@@ -266,6 +266,7 @@ __global__ void k1_sum_kernel(const double *__restrict__ part, int64_t nsplit, i
 
 int k1_launch(pbt_ctx *ctx, cudaStream_t st, const K1Facet *d_fac, int64_t nf,
               const K1Edge *d_edges, double lambda, int fast_diff, double *d_grid) {
+    pbt::NvtxRange nvtx_("pbt: far-field sum (FP64)");
     const GridCache &g = ctx->grid;
     const double waveno = 2.0 * kPiRef / lambda;
     const int threads = 128;
@@ -320,13 +321,21 @@ int k1_launch(pbt_ctx *ctx, cudaStream_t st, const K1Facet *d_fac, int64_t nf,
 // vertices; larger inputs are rejected with PBT_EINVAL.  The array takes
 // about 5.6 MB on every GPU that loads the library, until the process exits.
 //
-// Set-up: the first call on a device (with that device current) looks up the
-// array's device address with cudaGetSymbolAddress; make that first call
-// before any stream capture.  Every call on a device shares the one array and
-// overwrites what the previous call left there; the result grid is written in
-// full, so nothing has to start at zero.  Calls in one process are serialised
-// by a host lock and finish before they return; calls that overlapped on the
-// GPU would race on the shared array.
+// Set-up: every call looks up the array's device address on the current
+// device with cudaGetSymbolAddress (cheap once the library's device code is
+// loaded, and correct again after a cudaDeviceReset).  The first call on a
+// device loads that code and commits the array there, which makes the CUDA
+// runtime allocate device memory (and may create the device's primary
+// context): make that first call at start-up, before a pool reserves the
+// device's memory and outside any stream capture, or run with
+// CUDA_MODULE_LOADING=EAGER so that the array is committed when the program
+// initialises CUDA.  Each call enqueues its copies and its kernel on the
+// calling thread's per-thread default stream (cudaStreamPerThread, not the
+// legacy default stream) and waits for them.  Every call on a device shares the
+// one array and overwrites what the previous call left there; the result grid
+// is written in full, so nothing has to start at zero.  Calls in one process
+// are serialised by a host lock and finish before they return; calls that
+// overlapped on the GPU would race on the shared array.
 namespace pbt {
 namespace {
 
@@ -344,9 +353,7 @@ static_assert(sizeof(K1Facet) <= 512, "facet slot");
 // the device scratch of pbt_diffraction_noalloc_c
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
 
-constexpr int kNaMaxDevices = 64;
 static std::mutex g_na_mu;
-static void *g_na_dev[kNaMaxDevices];  // device address of g_noalloc_scratch, per device
 static double g_na_host[3 * kNaMaxBins + 2 * kNaMaxPhi];  // host staging of the bin grid
 
 int na_fail(int status, const char *msg) {
@@ -392,20 +399,17 @@ extern "C" int pbt_diffraction_noalloc_c(const pbt_outbeam *outbeam, const doubl
     if (theta_i < 0) return na_fail(PBT_EINVAL, "no theta value above 1 degree");
 
     std::lock_guard<std::mutex> lock(g_na_mu);
-    int dev = 0;
-    PBT_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kNaMaxDevices) return na_fail(PBT_ENODEV, "device index out of range");
-    if (!g_na_dev[dev]) {
-        // once per device, with that device current
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
+    // the array's address on the current device (host code cannot name it directly)
+    void *sym = nullptr;
+    {
+        const cudaError_t e = cudaGetSymbolAddress(&sym, g_noalloc_scratch);
+        if (e != cudaSuccess || !sym) {
+            (void)cudaGetLastError();
             set_error("cudaGetSymbolAddress(g_noalloc_scratch) failed: %s", cudaGetErrorString(e));
             return PBT_ECUDA;
         }
-        g_na_dev[dev] = p;
     }
-    unsigned char *base = static_cast<unsigned char *>(g_na_dev[dev]);
+    unsigned char *base = static_cast<unsigned char *>(sym);
 
     // bin grid (make_far_field_bins, phi fastest) and cos/sin(phi), libm values
     const int64_t nb = ntheta * nphi;
@@ -472,21 +476,23 @@ extern "C" int pbt_diffraction_noalloc_c(const pbt_outbeam *outbeam, const doubl
         E[i] = K1Edge{xs[i], ys[i], mj, nj, xs[in] - xs[i], ys[in] - ys[i]};
     }
 
-    // stage into the fixed array, run, copy the grid out (legacy default stream)
+    // stage into the fixed array, run, copy the grid out (per-thread default stream)
+    const cudaStream_t st = cudaStreamPerThread;
     double *d_xyz = reinterpret_cast<double *>(base + kNaOffXyz);
     double *d_phi = reinterpret_cast<double *>(base + kNaOffPhi);
     K1Facet *d_fac = reinterpret_cast<K1Facet *>(base + kNaOffFacet);
     K1Edge *d_edges = reinterpret_cast<K1Edge *>(base + kNaOffEdges);
     double *d_out = reinterpret_cast<double *>(base + kNaOffOut);
-    PBT_CUDA_TRY(cudaMemcpy(d_xyz, hx, 3 * nb * sizeof(double), cudaMemcpyHostToDevice));
-    PBT_CUDA_TRY(cudaMemcpy(d_phi, hp, 2 * nphi * sizeof(double), cudaMemcpyHostToDevice));
-    PBT_CUDA_TRY(cudaMemcpy(d_fac, &F, sizeof(K1Facet), cudaMemcpyHostToDevice));
-    PBT_CUDA_TRY(cudaMemcpy(d_edges, E, nv * sizeof(K1Edge), cudaMemcpyHostToDevice));
+    PBT_CUDA_TRY(cudaMemcpyAsync(d_xyz, hx, 3 * nb * sizeof(double), cudaMemcpyHostToDevice, st));
+    PBT_CUDA_TRY(cudaMemcpyAsync(d_phi, hp, 2 * nphi * sizeof(double), cudaMemcpyHostToDevice, st));
+    PBT_CUDA_TRY(cudaMemcpyAsync(d_fac, &F, sizeof(K1Facet), cudaMemcpyHostToDevice, st));
+    PBT_CUDA_TRY(cudaMemcpyAsync(d_edges, E, nv * sizeof(K1Edge), cudaMemcpyHostToDevice, st));
     const int threads = 128;
-    k1_kernel<<<(unsigned)((nb + threads - 1) / threads), threads>>>(
+    k1_kernel<<<(unsigned)((nb + threads - 1) / threads), threads, 0, st>>>(
         d_fac, 1, d_edges, d_xyz, d_phi, nphi, nb, theta_i, waveno, lambda, is_fast_diff ? 1 : 0,
         d_out);
     PBT_CUDA_TRY(cudaGetLastError());
-    PBT_CUDA_TRY(cudaMemcpy(amplC, d_out, 8 * nb * sizeof(double), cudaMemcpyDeviceToHost));
+    PBT_CUDA_TRY(cudaMemcpyAsync(amplC, d_out, 8 * nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PBT_CUDA_TRY(cudaStreamSynchronize(st));
     return PBT_OK;
 }

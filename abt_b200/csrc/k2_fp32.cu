@@ -1607,6 +1607,7 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
                const double *d_verts, int64_t nverts, const int64_t *d_face_off,
                const int64_t *d_face_vi, int64_t nfaces, int64_t max_nv, double lambda,
                int fast_diff, int variant, K2Setup &S) {
+    pbt::NvtxRange nvtx_("pbt: set-up (records)");
     const int64_t nrefs = h_beam_off[norient] + h_ext_off[norient];
     const int64_t max_recs = std::max<int64_t>(1, nrefs * std::max<int64_t>(1, max_nv - 2));
     // scan temp size
@@ -1796,6 +1797,7 @@ int k2_fast_tiles(pbt_ctx *ctx, cudaStream_t st, int64_t tile) {
 int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, int64_t no,
                  double lambda, int fast_diff, const K2Plan &plan, double *ws, int64_t *seg_rec,
                  int64_t *item_pre, unsigned long long *counter) {
+    pbt::NvtxRange nvtx_("pbt: far-field sum (FP32)");
     const GridCache &g = ctx->grid;
     const int64_t tile = (int64_t)K2_THREADS * plan.bpt;
     int64_t ntiles = (g.nb + tile - 1) / tile;
@@ -1993,6 +1995,7 @@ int k2_batch_add(pbt_ctx *ctx, cudaStream_t st, K2Batch &B, int64_t o0, int64_t 
         PBT_TRY(k2_run_chunk(ctx, st, S, l0, n, lambda, fast_diff, B.plan, B.ws, B.seg_rec,
                              B.item_pre, B.counter));
         const int64_t og = o0 + l0;  // global orientation of the workspace's first slot
+        pbt::NvtxRange nvtx_epi("pbt: epilogue (Mueller, orientation sums)");
         if (scaling) {
             k2_scatt_be_kernel<<<egrid, eb, 0, st>>>(B.ws, n, og, nb, nphi, phitab, waveno,
                                                      g.wbin.as<double>(), B.part);
@@ -2019,6 +2022,7 @@ int k2_batch_add(pbt_ctx *ctx, cudaStream_t st, K2Batch &B, int64_t o0, int64_t 
 int k2_batch_finish(pbt_ctx *ctx, cudaStream_t st, K2Batch &B, const pbt_output_params *d_params_in,
                     double *d_mueller_avg, double *d_m1d_avg, pbt_output_params *d_params_avg,
                     int check_errors) {
+    pbt::NvtxRange nvtx_("pbt: orientation average");
     const GridCache &g = ctx->grid;
     const int64_t nb = g.nb, nphi = (int64_t)g.phi.size(), ntheta = (int64_t)g.theta.size();
     const int64_t norient = B.norient;

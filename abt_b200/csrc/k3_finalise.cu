@@ -290,6 +290,7 @@ int totals_divide_device(pbt_ctx *ctx, DevTotals &T, cudaStream_t st, int64_t nu
 int k3_finalise(pbt_ctx *ctx, cudaStream_t st, const double *d_afb, const double *d_afe,
                 double lambda, int scaling, const pbt_output_params *h_params_in,
                 double *d_mueller, double *d_m1d, double *d_params, DevTotals *acc) {
+    pbt::NvtxRange nvtx_("pbt: finalise");
     const GridCache &g = ctx->grid;
     const int64_t nb = g.nb, nphi = (int64_t)g.phi.size(), ntheta = (int64_t)g.theta.size();
     const double waveno = 2.0 * kPiRef / lambda;  // src/outputs_mod.f90:98

@@ -805,6 +805,7 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
                const int64_t *face_off, const int64_t *face_vi, int64_t nfaces, double lambda,
                int fast_diff, const double *gafb, const double *gafe, double *gverts,
                double *gbeam, double *gext) {
+    pbt::NvtxRange nvtx_("pbt: adjoint");
     const GridCache &g = ctx->grid;
     const int64_t nb = g.nb, nphi = (int64_t)g.phi.size();
     const double k = 2.0 * kPiRef / lambda, Rf = kFarR;

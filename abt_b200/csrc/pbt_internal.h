@@ -1,6 +1,7 @@
 // pbt_internal.h -- shared declarations of the library's host and device code.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <mutex>
@@ -10,6 +11,17 @@
 #include "../../include/pbt_diff.h"
 
 namespace pbt {
+
+// A named NVTX range over a host-side stage (set-up, far-field sum, epilogue,
+// finalise, adjoint), the counterpart of the reference's timing spans
+// (src/diff_mod.f90:705-707, 740-742, 810-822).  NVTX is header-only and costs
+// nothing unless a profiler is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // ------------------------------------------------------------------ errors
 void set_error(const char *fmt, ...);

@@ -26,6 +26,13 @@
 // complex division as gfortran lowers a/b); the unit is built without FMA
 // contraction.
 //
+// Provenance: the physics routines restate the reference project's
+// algorithms (hballington12/abt, GPL-3.0) step by step and in its operation
+// order, because the outbeam lists must agree with a run of the reference bit
+// for bit.  The data layout, the bucket assignment of the visibility tests, the
+// per-level parallel propagation with ordered appends, and the C interface
+// are this file's own.
+//
 // Order of work.  The reference propagates the beams of one recursion level
 // on OpenMP threads and appends their children and outbeams inside critical
 // sections, so its list order depends on thread timing.  Here the beams of a
@@ -566,25 +573,30 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
             }
 }
 
-// get_theta_t_complex (src/beam_loop_mod.f90:342-383): complex Snell's law
-// (Macke 1996), angle of refraction from medium m1 into m2
+// Angle of refraction from medium m1 into m2 with complex indices: Macke's
+// (1996) form of Snell's law for absorbing media, as get_theta_t_complex has
+// it (src/beam_loop_mod.f90:342-383).  With kappa = Im/Re of each index, the
+// relative index n_rel (1 + i kappa_rel) gives a complex
+// c = 1 - sin^2(theta_i) (1 - kappa_rel^2 - 2 i kappa_rel) / (n_rel^2 (1 + kappa_rel^2)^2);
+// the real effective index n_eff then satisfies sin(theta_t) = sin(theta_i) / n_eff.
+// Operations in the reference's order.
 double theta_t_complex(double theta_i, Z m1, Z m2) {
-    const double k1 = m1.im / m1.re, k2 = m2.im / m2.re;
-    const double krel = (k2 - k1) / (1 + k1 * k2);
-    const double nrel = m2.re / m1.re * (1 + k1 * k2) / (1 + k1 * k1);
-    const double ref1 = nrel * nrel, ref2 = krel * krel;
-    const double ref3 = (1 + ref2) * (1 + ref2);
-    const double ref6 = ref1 * ref3 / (1 + krel * k2) / (1 + krel * k2);
-    const double sintiq = sin(theta_i) * sin(theta_i);
-    const double ref4 = 1 - (1 - ref2) / ref1 / ref3 * sintiq;
-    const double ref5 = 2 * krel / ref1 / ref3 * sintiq;
-    const double q4 = ref4 * ref4 + ref5 * ref5;
-    const double q2 = sqrt(q4);
-    const double g = acos(ref4 / q2) / 2;
-    const double cg = cos(g) - k2 * sin(g);
-    const double ref7 = cg * cg;
-    const double rnstar = sqrt(sintiq + ref6 * q2 * ref7);
-    return asin(sin(theta_i) / rnstar);
+    const double kappa1 = m1.im / m1.re, kappa2 = m2.im / m2.re;
+    const double kap_rel = (kappa2 - kappa1) / (1 + kappa1 * kappa2);
+    const double n_rel = m2.re / m1.re * (1 + kappa1 * kappa2) / (1 + kappa1 * kappa1);
+    const double n_rel2 = n_rel * n_rel, kap_rel2 = kap_rel * kap_rel;
+    const double damp2 = (1 + kap_rel2) * (1 + kap_rel2);
+    const double scale = n_rel2 * damp2 / (1 + kap_rel * kappa2) / (1 + kap_rel * kappa2);
+    const double sin2_i = sin(theta_i) * sin(theta_i);
+    const double c_re = 1 - (1 - kap_rel2) / n_rel2 / damp2 * sin2_i;
+    const double c_im = 2 * kap_rel / n_rel2 / damp2 * sin2_i;
+    const double c_abs2 = c_re * c_re + c_im * c_im;
+    const double c_abs = sqrt(c_abs2);
+    const double half_arg = acos(c_re / c_abs) / 2;
+    const double proj = cos(half_arg) - kappa2 * sin(half_arg);
+    const double proj2 = proj * proj;
+    const double n_eff = sqrt(sin2_i + scale * c_abs * proj2);
+    return asin(sin(theta_i) / n_eff);
 }
 
 // get_trans_prop (src/beam_loop_mod.f90:1010-1051)

@@ -9,8 +9,10 @@
 ! diffraction reads (ampl, vk7, prop_out, fov, fi) into pbt_outbeam records
 ! and the facet vertex lists of geometry_type into a CSR.
 !
-! This file is not compiled on the build machine (it has no Fortran
-! compiler); INTEGRATION.md gives the build steps.
+! Build: compile this module with the reference's sources in place of
+! diff_mod.f90 and link libpbt_b200.so (e.g. gfortran -c pbt_b200_diff_mod.f90
+! after types_mod.o; link with -L<dir> -lpbt_b200).  It has not been compiled
+! on the machine that built the library, which has no Fortran compiler.
 module pbt_b200_diff_mod
 
     use, intrinsic :: iso_c_binding

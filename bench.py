@@ -79,6 +79,12 @@ def parse():
                     help="orientations of the large absorbing column timed (0: skip)")
     ap.add_argument("--large-traced-orient", type=int, default=8,
                     help="orientations of the large column traced on the host (0: skip)")
+    ap.add_argument("--config5", type=int, default=0,
+                    help="orientations of the large absorbing column at its full size "
+                         "(2048 in the configuration; opt-in, about ten minutes; 0: skip)")
+    ap.add_argument("--config5-fp64", type=int, default=64,
+                    help="orientations of the large absorbing column averaged in FP64 too, "
+                         "for the FP32 error")
     ap.add_argument("--diff-orient", type=int, default=64,
                     help="orientations of the differentiation workload (0: skip)")
     ap.add_argument("--adjoint-facets", type=int, default=20000,
@@ -348,6 +354,91 @@ def large_traced(ctx, args):
                 for k in ("scatt", "ext", "asymmetry", "back_scatt", "albedo"))}
 
 
+def config5(ctx, args):
+    """The large absorbing case at its stated size: the smooth hexagonal column
+    r 50 um, L 100 um in 2 um^2 triangles (22,500, its 8 parent faces as
+    apertures), n = 1.31 + 0.01i, --config5 orientations uniform on SO(3)
+    (seed 55), 1441 theta x 720 phi.  Beam lists come from the host tracer
+    (8 recursions, the reference's thresholds), traced chunk c+1 on the host
+    cores while the GPU averages chunk c in FP32 (pbt_diff_batch_list_c); the
+    whole loop is timed.  The FP32 average of the first --config5-fp64
+    orientations is compared with their FP64 drop-in average."""
+    from concurrent.futures import ThreadPoolExecutor
+    import abt_b200
+    from abt_b200 import tracer as T
+    from abt_b200 import workloads as W
+    from tests.helpers import mueller_rel_err
+    g = W.hex_prism(50.0, 100.0, n_side=25, n_len=50, roughness=0.0, seed=5)
+    P = T.Particle(g, g["apertures"])
+    th = abt_b200.make_angles([0, 180], [0.125])
+    ph = abt_b200.make_angles([0, 359.5], [0.5])
+    nb = len(th) * len(ph)
+    n = args.config5
+    eul = W.uniform_euler(np.random.default_rng(55), n)
+    chunk = 64
+    geo = P.geometry
+
+    def trace(s0):
+        return T.trace_batch(P, eul[s0:s0 + chunk], LAM, 1.31, ibi=0.01)
+
+    nout, per_orient, kept = [], [], None
+    ctx.set_kernel_timing(True)
+    ctx.kernel_time_ms()
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=1) as ex:
+        starts = list(range(0, n, chunk))
+        fut = ex.submit(trace, 0)
+        for c, s0 in enumerate(starts):
+            Vs, beams, exts, pins, _ = fut.result()
+            if c + 1 < len(starts):
+                fut = ex.submit(trace, starts[c + 1])
+            r = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pins, precision="fp32")
+            nout += [len(b) + len(e) for b, e in zip(beams, exts)]
+            per_orient.append(np.atleast_1d(r[3]))
+            if c == 0:
+                kept = (Vs, beams, exts, pins)
+    t_all = time.perf_counter() - t0
+    k_ms, k_n = ctx.kernel_time_ms()
+    ctx.set_kernel_timing(False)
+    F = np.array(nout, dtype=np.float64)
+    work = float(F.sum()) * nb
+    # FP32 against FP64 on the first orientations (the first chunk's lists)
+    m = min(args.config5_fp64, len(kept[1]))
+    Vs, beams, exts, pins = (x[:m] for x in kept)
+    r32 = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pins, precision="fp32")
+    t0 = time.perf_counter()
+    r64 = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pins, precision="fp64")
+    t64 = time.perf_counter() - t0
+    sms = torch_sm_count()
+    hz = 1965.0e6
+    kern_s = k_ms / 1e3
+    return {"workload": "smooth hexagonal column r 50 um, L 100 um, 2 um^2 triangles (22,500, "
+                        "8 apertures), n = 1.31 + 0.01i, beam lists traced on the host (rec 8), "
+                        "%d orientations uniform on SO(3), 1441 theta x 720 phi" % n,
+            "orientations": n, "bins": nb,
+            "outbeams_per_orientation": [int(F.min()), int(F.mean()), int(F.max())],
+            "trace_and_fp32_average_s": t_all, "orientations_per_s": n / t_all,
+            "facet_bin_per_s": work / t_all, "fp32_kernel_s": kern_s,
+            "fp32_kernel_facet_bin_per_s": work / kern_s,
+            "mufu_term_frac": W_SFU * work / kern_s / (sms * SFU_PER_SM_CLK * hz),
+            "fp32_term_frac": W_FP32 * work / kern_s / (sms * FP32_PER_SM_CLK * hz),
+            "roofline_basis": "convention per triangle facet-bin (20 MUFU, 170 FP32 flops) over "
+                              "the summed kernel time; %d SMs x 1965 MHz" % sms,
+            "error_subset_orientations": m, "fp64_dropin_subset_s": t64,
+            "fp64_dropin_orientations_per_s": m / t64,
+            "speedup_fp32_vs_fp64_dropin": (n / t_all) / (m / t64),
+            "max_rel_mueller_err_vs_fp64_subset": mueller_rel_err(r32[0], r64[0], 1e-6),
+            "mueller_err_above_1e-5_of_peak": mueller_rel_err(r32[0], r64[0], 1e-5),
+            "max_rel_param_err_vs_fp64_subset": max(
+                abs(float(r32[2][k]) - float(r64[2][k])) / abs(float(r64[2][k]))
+                for k in ("scatt", "ext", "asymmetry", "albedo"))}
+
+
+def torch_sm_count():
+    import torch
+    return torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+
+
 def _worst_bin(mu, mu_ref, theta, thresh=1e-6):
     """theta (degrees) of the bin with the largest M11-normalised Mueller error
     above thresh of the peak M11, and that bin's M11 over the peak."""
@@ -526,6 +617,42 @@ def cpu_baseline(geo, beam, th, ph, seconds, nthreads):
             "sample": "%d facets x %d bins (first facets of the workload), %.1f s" % (n2, nb, dt)}
 
 
+def workload_config(nf, nb):
+    """The `config` both arms print: the workload only, so that the two lines
+    compare like for like (arm-specific details are keys of their own)."""
+    return {"workload": "precision-study beam list: 200000 facets (2000 beams), 721 theta x 360 "
+                        "phi, lambda 0.532 um",
+            "facets": int(nf), "bins": int(nb), "orientations_per_step": 1,
+            "l2": "GPU arm: a 256 MB buffer is written before every step, inside the timed "
+                  "region; CPU arm: each step streams the facet list through the whole grid"}
+
+
+def fast_diff_kept_fraction(beam, geo, th, ph, sample=20000, tile_theta=8, tile_phi=16):
+    """Fraction of (record, bin tile) pairs that the -fast_diff tile cull keeps,
+    estimated on the host on the first `sample` records with the kernel's test:
+    a record is skipped for a tile when the angle between its prop_out and the
+    tile's centre exceeds fov + 2|com|/R + 1e-5 plus the tile's angular radius."""
+    ob = beam[:sample]
+    TH, PH = np.meshgrid(th, ph, indexing="ij")  # (ntheta, nphi)
+    u = np.stack([np.sin(TH) * np.cos(PH), np.sin(TH) * np.sin(PH), -np.cos(TH)], -1)
+    cen, psi = [], []
+    for a in range(0, len(th), tile_theta):
+        for b in range(0, len(ph), tile_phi):
+            t = u[a:a + tile_theta, b:b + tile_phi].reshape(-1, 3)
+            c = t.mean(0)
+            c /= np.linalg.norm(c)
+            cen.append(c)
+            psi.append(np.arccos(np.clip(t @ c, -1, 1)).max())
+    cen, psi = np.array(cen), np.array(psi)
+    fo, fv, V = geo["face_off"], geo["face_vi"], geo["verts"]
+    com = np.array([V[fv[fo[f - 1]:fo[f]] - 1].mean(0) for f in ob["fi"]])
+    fovm = ob["fov"] + 2 * np.linalg.norm(com, axis=1) / 1e6 + 1e-5
+    ang = np.arccos(np.clip(ob["prop_out"] @ cen.T, -1, 1))
+    lim = fovm[:, None] + psi[None, :]
+    kept = (lim >= np.pi) | (ang <= lim)
+    return float(kept.mean())
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -546,8 +673,9 @@ def run_reference(args, world, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "precision-study beam list, 200000 facets x 721x360 bins",
-                       "facets": int(len(beam)), "bins": nb},
+            "config": workload_config(len(beam), nb),
+            "ms_per_step_basis": "extrapolated: the step's facet-bin count divided by the rate "
+                                 "measured on each step's bounded facet sample",
             "cpu_baseline": dict(last, value=value),
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -745,6 +873,8 @@ def main():
         extra["large_column"] = large_case(ctx, args)
     if args.large_traced_orient > 0 and solo:
         extra["large_column_traced"] = large_traced(ctx, args)
+    if args.config5 > 0 and solo:
+        extra["large_column_config5"] = config5(ctx, args)
 
     # -fast_diff: the same workload with the field-of-view test (fov = 8 lambda / d);
     # error against the FP64 drop-in with is_fast_diff on the first 20,000 facets
@@ -762,7 +892,15 @@ def main():
         a64 = ctx.diff_main(sub, None, geo, th, ph, LAM, is_fast_diff=True, precision="fp64")
         m32, _, _ = ctx.finalise(a32[0], a32[1], th, ph, LAM, pin[0])
         m64, _, _ = ctx.finalise(a64[0], a64[1], th, ph, LAM, pin[0])
+        kept = fast_diff_kept_fraction(beam, geo, th, ph)
         extra["fast_diff"] = {"kernel_ms": kf_ms, "value": work / (kf_ms / 1e3), "unit": UNIT,
+                              "value_basis": "effective: every facet-bin of the workload over "
+                                             "the kernel time, culled pairs included",
+                              "kept_pair_fraction": kept,
+                              "evaluated_value": kept * work / (kf_ms / 1e3),
+                              "evaluated_basis": "facet-bins of the (record, tile) pairs the "
+                                                 "cull keeps (fraction estimated on the host on "
+                                                 "20,000 records) over the kernel time",
                               "speedup_vs_full_kernel": (kern_ms / max(kern_n, 1)) / kf_ms,
                               "max_rel_mueller_err_vs_fp64_fast_20000_facets":
                                   mueller_rel_err(m32, m64, 1e-6),
@@ -813,18 +951,18 @@ def main():
     cpu = None
     if solo and not args.no_cpu_baseline:
         cpu = cpu_baseline(geo, beam, th, ph, args.cpu_seconds, os.cpu_count() or 1)
+        # the single-thread path (the reference's seq build at -mt 0)
+        cpu["single_thread"] = cpu_baseline(geo, beam, th, ph, args.cpu_seconds / 2, 1)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "precision-study beam list: 200000 facets (2000 beams), "
-                                   "721 theta x 360 phi, lambda 0.532 um, FP32 with FP64 phase",
-                       "facets": nf, "bins": nb, "orientations_per_step": 1,
-                       "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "256 MB buffer written before every step, inside the timed region",
-                       "step": "CUDA graph replay of pbt_diff_batch_dev_c" if not args.no_graph
-                               else "pbt_diff_batch_dev_c",
-                       "launch_plan": plan},
+            "config": workload_config(nf, nb),
+            "precision": "FP32 with FP64 phase",
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "step": "CUDA graph replay of pbt_diff_batch_dev_c" if not args.no_graph
+                    else "pbt_diff_batch_dev_c",
+            "launch_plan": plan,
             "orientations_per_s": world * 1e3 / ms_step,
             "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof,
             "cpu_baseline": cpu}

@@ -114,8 +114,13 @@ int pbt_make_far_field_bins_c(const double *theta, int64_t ntheta, const double 
  * calls no allocation routine; it needs no context.  Limits: at most
  * PBT_NOALLOC_MAX_BINS bins (ntheta * nphi), PBT_NOALLOC_MAX_PHI phi values
  * and PBT_NOALLOC_MAX_VERTS vertices per face; larger inputs return
- * PBT_EINVAL.  The first call on a device (made with that device current)
- * looks up the array's address; make it before any stream capture.  All
+ * PBT_EINVAL.  The first call on a device loads the library's device code
+ * there and commits the array, which makes the CUDA runtime allocate device
+ * memory (and may create the device's primary context): make the first call
+ * at start-up, before a pool reserves the device's memory and outside any
+ * stream capture, or run with CUDA_MODULE_LOADING=EAGER.  Every call looks up
+ * the array's address on the current device and runs on the calling thread's
+ * per-thread default stream (cudaStreamPerThread), waiting for its work.  All
  * calls on a device share the array; calls in one process are serialised and
  * complete before returning, and calls that overlapped on the GPU would race. */
 #define PBT_NOALLOC_MAX_BINS 65536
@@ -378,6 +383,14 @@ int pbt_trace_destroy(pbt_trace *t);
  * the far-field kernels; it gives up after limit_ms (1..5000) and the call
  * returns PBT_ETIMEOUT, leaving the context usable. */
 int pbt_selftest_bounded_wait_c(pbt_ctx *ctx, int32_t limit_ms);
+
+/* Failure injection for tests (no counterpart in the reference, which stops
+ * the program when an allocation fails, src/misc_submod.f90:2453-2459): the
+ * next `count` device allocations the library makes, in any context of the
+ * process, fail as a failing cudaMalloc would, so the calls that need them
+ * return PBT_ENOMEM with a message and leave their context usable; a count of
+ * 0 clears the injection.  Returns the count that was pending before. */
+int pbt_test_fail_next_alloc(int32_t count);
 
 #ifdef __cplusplus
 }

@@ -115,3 +115,13 @@ def test_make_far_field_bins_matches_oracle():
         assert np.array_equal(a.ravel(order="F"), r)
     with pytest.raises(abt_b200.PbtError):
         abt_b200.make_far_field_bins(th[:0], ph)
+
+
+def test_allocation_failure_hook_counts():
+    """pbt_test_fail_next_alloc (host-side failure injection) keeps a count of
+    pending failures and returns the previous one; 0 clears it."""
+    L = _lib.lib()
+    assert L.pbt_test_fail_next_alloc(3) == 0
+    assert L.pbt_test_fail_next_alloc(0) == 3
+    assert L.pbt_test_fail_next_alloc(-5) == 0
+    assert L.pbt_test_fail_next_alloc(0) == 0

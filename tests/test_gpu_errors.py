@@ -157,3 +157,31 @@ def test_no_outbeams_at_all(ctx, precision):
     mu, mu1, _, _ = ctx.diff_batch([ob[:0]] * 3, [ob[:0]] * 3, [geo["verts"]] * 3, geo, th, ph,
                                    LAM, pin, precision=precision)
     assert not mu.any() and not mu1.any()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_injected_allocation_failure_reports_enomem(precision):
+    """A device allocation that fails (injected on the host with
+    pbt_test_fail_next_alloc) makes the call return PBT_ENOMEM with a message;
+    the context stays usable and the next call gives the result of a context
+    that never failed.  A fresh context has no buffers yet, so its first call
+    allocates."""
+    from abt_b200 import _lib
+    from abt_b200._lib import PBT_ENOMEM
+    th, ph, geo, ob = _inputs()
+    ext = ob[:1].copy()
+    ext["prop_out"] = (0.0, 0.0, -1.0)
+    with abt_b200.Context(0) as ref_ctx:
+        ref = ref_ctx.diff_main(ob, ext, geo, th, ph, LAM, precision=precision)
+    with abt_b200.Context(0) as c:
+        assert _lib.lib().pbt_test_fail_next_alloc(1) == 0
+        try:
+            with pytest.raises(PbtError) as e:
+                c.diff_main(ob, ext, geo, th, ph, LAM, precision=precision)
+        finally:
+            _lib.lib().pbt_test_fail_next_alloc(0)
+        assert e.value.status == PBT_ENOMEM and "injected" in str(e.value)
+        got = c.diff_main(ob, ext, geo, th, ph, LAM, precision=precision)
+        assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+        mu = c.finalise(got[0], got[1], th, ph, LAM, abt_b200.params(geo_cross_sec=1.0))[0]
+        assert np.isfinite(mu).all()

@@ -60,3 +60,8 @@ def test_reference_arm_under_torchrun():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"
+    # the same `config` as the GPU arm prints for this workload (40 facets, 721 x 360 bins)
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["config"] == bench.workload_config(40, 721 * 360)
+    assert "extrapolated" in d["ms_per_step_basis"]

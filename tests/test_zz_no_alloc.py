@@ -63,3 +63,49 @@ def test_no_alloc_rejects_grids_beyond_its_scratch():
     st, _ = noalloc(ob, geo, th, ph, False)
     assert st == _lib.PBT_EINVAL
     assert b"scratch" in _lib.lib().pbt_last_error_string()
+
+
+def test_no_alloc_rejects_too_many_phi_values_and_large_faces():
+    """4,097 phi values (in only 12,291 bins) and a 65-vertex face are over the
+    fixed limits and are refused before anything is copied."""
+    rng = np.random.default_rng(79)
+    geo = mixed_polygon_geometry(rng)
+    ob = outbeams(1, rng, len(geo["face_off"]) - 1)
+    th = np.radians([0.0, 2.0, 4.0])
+    ph = np.linspace(0.0, 2 * np.pi, 4097, endpoint=False)
+    st, _ = noalloc(ob, geo, th, ph, False)
+    assert st == _lib.PBT_EINVAL and b"4096" in _lib.lib().pbt_last_error_string()
+    # a regular 65-gon in the z = 0 plane, and a 64-gon that is accepted
+    for n, want in ((65, _lib.PBT_EINVAL), (64, _lib.PBT_OK)):
+        a = 2 * np.pi * np.arange(n) / n
+        verts = np.stack([3 * np.cos(a), 3 * np.sin(a), np.zeros(n)], 1)
+        g = abt_b200.make_geometry(verts, [list(range(1, n + 1))])
+        o = outbeams(1, rng, 1)
+        st, out = noalloc(o, g, abt_b200.make_angles([0, 180], [5]),
+                          abt_b200.make_angles([0, 350], [10]), False)
+        assert st == want, _lib.lib().pbt_last_error_string()
+        if want == _lib.PBT_EINVAL:
+            assert b"64" in _lib.lib().pbt_last_error_string()
+        else:
+            assert np.isfinite(out).all()
+
+
+def test_no_alloc_calls_leave_device_memory_unchanged():
+    """After a first call (which loads the device code and commits the fixed
+    array), further calls change the device's free memory by nothing."""
+    import torch
+    rng = np.random.default_rng(80)
+    geo = mixed_polygon_geometry(rng)
+    ob = outbeams(1, rng, len(geo["face_off"]) - 1)
+    th, ph = abt_b200.make_angles([0, 180], [2]), abt_b200.make_angles([0, 356], [4])
+    st, first = noalloc(ob, geo, th, ph, False)
+    assert st == _lib.PBT_OK
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for fast in (False, True, False):
+        st, out = noalloc(ob, geo, th, ph, fast)
+        assert st == _lib.PBT_OK
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
+    assert np.array_equal(out, first)
