@@ -87,6 +87,9 @@ def parse():
                          "for the FP32 error")
     ap.add_argument("--diff-orient", type=int, default=64,
                     help="orientations of the differentiation workload (0: skip)")
+    ap.add_argument("--fd-coords", type=int, default=200,
+                    help="vertex coordinates checked by FP64 central differences on each of the "
+                         "first two orientations of the differentiation workload (0: skip)")
     ap.add_argument("--adjoint-facets", type=int, default=20000,
                     help="facet sample for the adjoint / forward kernel-time ratio (0: skip)")
     return ap.parse_args()
@@ -534,7 +537,7 @@ def differentiation(ctx, args):
     noise = rng.normal(0.0, 0.02, size=geo["verts"].shape)
     fwd_ms = adj_ms = wall = 0.0
     nrec = []
-    fd = None
+    fds = []
     for i, (a, b, c) in enumerate(eul):
         R = W.euler_rotation(a, b, c)
         V, beam, ext, _ = W.standin_orientation(geo, R, rng, n_internal=(0, 2))
@@ -559,32 +562,10 @@ def differentiation(ctx, args):
         if i > 0:  # the first orientation warms up
             fwd_ms += f_ms
             adj_ms += a_ms
-        if i == 0:
-            def loss64(Vm, bm=beam, em=ext):
-                x, y = ctx.diff_main(bm, em, dict(geo, verts=Vm), th, ph, LAM, precision="fp64")
-                p, q = AG.mueller11_12(torch.from_numpy(x), torch.from_numpy(y), LAM)
-                return float(AG.mueller_loss(p, q, t11, t12, th))
-            gV = Vg.grad.numpy()
-            used = np.unique(geo["face_vi"].reshape(-1, 3)[beam["fi"][:2000] - 1]) - 1
-            picks = [(int(v), k) for v in rng.choice(used, 4, replace=False) for k in range(3)]
-            h = 1e-5
-            errs = []
-            for v, k in picks:
-                Vp, Vm = V.copy(), V.copy()
-                Vp[v, k] += h
-                Vm[v, k] -= h
-                errs.append(abs((loss64(Vp) - loss64(Vm)) / (2 * h) - gV[v, k]))
-            gb = ab.grad.numpy()
-            aerr = []
-            for j in (0, len(beam) // 2):
-                bp, bm = beam.copy(), beam.copy()
-                bp["ampl"][j, 2] += 1e-6
-                bm["ampl"][j, 2] -= 1e-6
-                aerr.append(abs((loss64(V, bp) - loss64(V, bm)) / 2e-6 - gb[j, 2]))
-            fd = {"h_um": h, "vertex_coords": len(picks),
-                  "max_abs_err_over_max_grad_vertex": float(max(errs) / np.abs(gV).max()),
-                  "ampl_components": len(aerr),
-                  "max_abs_err_over_max_grad_ampl": float(max(aerr) / np.abs(gb).max())}
+        if i < min(2, args.diff_orient) and args.fd_coords > 0:
+            fds.append(_fd_check(ctx, geo, V, beam, ext, th, ph, t11, t12, Vg.grad.numpy(),
+                                 ab.grad.numpy(), ae.grad.numpy(), np.random.default_rng(100 + i),
+                                 args.fd_coords))
     n = max(1, args.diff_orient - 1)
     return {"workload": "rough hexagonal plate r 8 um, L 4 um, sigma 0.05 um (20,808 triangles), "
                         "stand-in beam lists, %d orientations, 181 theta x 90 phi, target from "
@@ -594,7 +575,93 @@ def differentiation(ctx, args):
             "adjoint_kernel_ms_per_orientation": adj_ms / n,
             "adjoint_over_forward": adj_ms / fwd_ms if fwd_ms > 0 else None,
             "gradient_wall_ms_per_orientation": wall * 1e3 / args.diff_orient,
-            "fd_check_first_orientation": fd}
+            "fd_checks_first_two_orientations": fds}
+
+
+def _fd_check(ctx, geo, V, beam, ext, th, ph, t11, t12, gV, gb, ge, rng, ncoords, h=1e-5):
+    """The adjoint's gradient of one orientation against FP64 central
+    differences of the loss of the FP64 drop-in: ncoords random vertex
+    coordinates of emitting facets one by one (only the outbeams on the moved
+    vertex are recomputed, with pbt_diffraction_c), all 8 amplitude components of
+    two beam and two external-diffraction outbeams, and four random directions
+    in vertex space (relative to |grad| |direction|).  The drop-in keeps the
+    reference's clamps (|kxx|, |kyy| >= 1e-6, edge slopes) and its cancellation
+    where kxx or kyy is small, so its loss has kinks and round-off steps at a few
+    vertices: each coordinate is differenced with steps h and h/10, and where
+    the two differ by more than 1e-4 of the largest gradient component the
+    coordinate is counted as not smooth and reported apart."""
+    import torch
+    from abt_b200 import autograd as AG
+
+    def loss_of(A):
+        p, q = AG.mueller11_12(torch.from_numpy(A), torch.from_numpy(np.zeros_like(A)), LAM)
+        return float(AG.mueller_loss(p, q, t11, t12, th))
+
+    ab, ae = ctx.diff_main(beam, ext, dict(geo, verts=V), th, ph, LAM, precision="fp64")
+    A = ab + ae
+    faces = geo["face_vi"].reshape(-1, 3) - 1
+    allrec = np.concatenate([beam, ext])
+    fi = allrec["fi"]
+    used = np.unique(faces[fi - 1])
+    gmax = np.abs(gV).max()
+
+    one_face = {"face_off": np.array([0, 3], dtype=np.int64),
+                "face_vi": np.array([1, 2, 3], dtype=np.int64)}
+
+    def one(r, Vx):
+        # the outbeam's facet alone, so that each call handles three vertices
+        r1 = r.reshape(1).copy()
+        f = int(r1["fi"][0]) - 1
+        r1["fi"] = 1
+        return ctx.diffraction(r1, dict(one_face, verts=Vx[faces[f]]), th, ph, LAM)
+
+    def fd_coord(v, k, step):
+        recs = allrec[np.any(faces[fi - 1] == v, axis=1)]
+        Vp, Vm = V.copy(), V.copy()
+        Vp[v, k] += step
+        Vm[v, k] -= step
+        dp = dm = 0.0
+        for r in recs:
+            a0 = one(r, V)
+            dp = dp + one(r, Vp) - a0
+            dm = dm + one(r, Vm) - a0
+        return (loss_of(A + dp) - loss_of(A + dm)) / (2 * step)
+
+    smooth_err, kink = [], []
+    for v in rng.choice(used, ncoords):
+        k = int(rng.integers(0, 3))
+        d1, d2 = fd_coord(int(v), k, h), fd_coord(int(v), k, h / 10)
+        if abs(d1 - d2) > 1e-4 * gmax:
+            kink.append(abs(d1 - d2) / gmax)
+        else:
+            smooth_err.append(abs(d2 - gV[v, k]) / gmax)
+    aerr = []
+    for recs, g, j0 in ((beam, gb, 0), (ext, ge, len(beam))):
+        for j in (0, len(recs) // 2):
+            base = one(recs[j], V)
+            for c in range(8):
+                r2 = recs[j:j + 1].copy()
+                r2["ampl"][0, c] += 1e-6
+                dA = one(r2[0], V) - base
+                d = (loss_of(A + dA) - loss_of(A - dA)) / 2e-6
+                aerr.append(abs(d - g[j, c]) / np.abs(g).max())
+    derr = []
+    for _ in range(4):
+        dvec = rng.normal(size=V.shape)
+        dvec /= np.linalg.norm(dvec)
+        lp = loss_of(sum(ctx.diff_main(beam, ext, dict(geo, verts=V + h * dvec), th, ph, LAM,
+                                       precision="fp64")))
+        lm = loss_of(sum(ctx.diff_main(beam, ext, dict(geo, verts=V - h * dvec), th, ph, LAM,
+                                       precision="fp64")))
+        derr.append(abs((lp - lm) / (2 * h) - float((gV * dvec).sum())) / np.linalg.norm(gV))
+    return {"h_um": [h, h / 10], "vertex_coords": int(ncoords),
+            "smooth_coords": len(smooth_err),
+            "max_abs_err_over_max_grad_vertex_smooth": float(max(smooth_err)) if smooth_err else None,
+            "not_smooth_coords": len(kink),
+            "not_smooth_fd_spread_over_max_grad": [float(x) for x in sorted(kink)[-4:]],
+            "ampl_components": len(aerr), "max_abs_err_over_max_grad_ampl": float(max(aerr)),
+            "random_directions": len(derr),
+            "max_directional_err_over_grad_norm": float(max(derr))}
 
 
 def cpu_baseline(geo, beam, th, ph, seconds, nthreads):

@@ -144,7 +144,7 @@ def test_adjoint_kernel_matches_fp64_gradient(ctx):
             for g, r in ((V.grad.numpy(), gV_ref), (ab.grad.numpy(), gb_ref),
                          (ae.grad.numpy(), ge_ref)):
                 err = np.abs(g - r).max() / np.abs(r).max()
-                assert err < 2e-3, err
+                assert err < 1e-4, err
         else:
             assert np.all(np.isfinite(V.grad.numpy()))
 
