@@ -585,11 +585,13 @@ def _fd_check(ctx, geo, V, beam, ext, th, ph, t11, t12, gV, gb, ge, rng, ncoords
     vertex are recomputed, with pbt_diffraction_c), all 8 amplitude components of
     two beam and two external-diffraction outbeams, and four random directions
     in vertex space (relative to |grad| |direction|).  The drop-in keeps the
-    reference's clamps (|kxx|, |kyy| >= 1e-6, edge slopes) and its cancellation
-    where kxx or kyy is small, so its loss has kinks and round-off steps at a few
-    vertices: each coordinate is differenced with steps h and h/10, and where
-    the two differ by more than 1e-4 of the largest gradient component the
-    coordinate is counted as not smooth and reported apart."""
+    reference's clamps (|kxx|, |kyy| >= 1e-6, edge slopes), its cancellation
+    where kxx or kyy is small and its discontinuous frame choices (the
+    anti-parallel flip, the frame flip of get_rotation_matrix2), so its loss has
+    kinks and steps at a few vertices: each coordinate and each direction is
+    differenced with steps h and h/10, and where the two differ by more than
+    1e-4 of the largest gradient component (of |grad| for a direction) it is
+    counted as not smooth and reported apart."""
     import torch
     from abt_b200 import autograd as AG
 
@@ -645,23 +647,32 @@ def _fd_check(ctx, geo, V, beam, ext, th, ph, t11, t12, gV, gb, ge, rng, ncoords
                 dA = one(r2[0], V) - base
                 d = (loss_of(A + dA) - loss_of(A - dA)) / 2e-6
                 aerr.append(abs(d - g[j, c]) / np.abs(g).max())
-    derr = []
+    def fd_dir(dvec, step):
+        lp = loss_of(sum(ctx.diff_main(beam, ext, dict(geo, verts=V + step * dvec), th, ph, LAM,
+                                       precision="fp64")))
+        lm = loss_of(sum(ctx.diff_main(beam, ext, dict(geo, verts=V - step * dvec), th, ph, LAM,
+                                       precision="fp64")))
+        return (lp - lm) / (2 * step)
+
+    derr, dkink = [], []
+    gnorm = np.linalg.norm(gV)
     for _ in range(4):
         dvec = rng.normal(size=V.shape)
         dvec /= np.linalg.norm(dvec)
-        lp = loss_of(sum(ctx.diff_main(beam, ext, dict(geo, verts=V + h * dvec), th, ph, LAM,
-                                       precision="fp64")))
-        lm = loss_of(sum(ctx.diff_main(beam, ext, dict(geo, verts=V - h * dvec), th, ph, LAM,
-                                       precision="fp64")))
-        derr.append(abs((lp - lm) / (2 * h) - float((gV * dvec).sum())) / np.linalg.norm(gV))
+        d1, d2 = fd_dir(dvec, h), fd_dir(dvec, h / 10)
+        if abs(d1 - d2) > 1e-4 * gnorm:
+            dkink.append(abs(d1 - d2) / gnorm)
+        else:
+            derr.append(abs(d2 - float((gV * dvec).sum())) / gnorm)
     return {"h_um": [h, h / 10], "vertex_coords": int(ncoords),
             "smooth_coords": len(smooth_err),
             "max_abs_err_over_max_grad_vertex_smooth": float(max(smooth_err)) if smooth_err else None,
             "not_smooth_coords": len(kink),
             "not_smooth_fd_spread_over_max_grad": [float(x) for x in sorted(kink)[-4:]],
             "ampl_components": len(aerr), "max_abs_err_over_max_grad_ampl": float(max(aerr)),
-            "random_directions": len(derr),
-            "max_directional_err_over_grad_norm": float(max(derr))}
+            "random_directions": 4, "smooth_directions": len(derr),
+            "max_directional_err_over_grad_norm_smooth": float(max(derr)) if derr else None,
+            "not_smooth_directions_fd_spread_over_grad_norm": [float(x) for x in dkink]}
 
 
 def cpu_baseline(geo, beam, th, ph, seconds, nthreads):
