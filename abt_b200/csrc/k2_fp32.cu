@@ -1207,12 +1207,36 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
             const int st = (int)(c % K2_NST);
             const bool ok = mbar_wait(smem_u32(&bars[st]), (parity >> st) & 1u);
             parity ^= 1u << st;
+            const int n = (int)min((int64_t)K2P_CH, npair - c * K2P_CH);
+            if (!FAST && ok && tid < 39) {
+                // The item's first pair (odd rbeg) and last pair (odd rend) hold a
+                // record of another item or the array's padding: that half takes a
+                // copy of the pair's other record with zero amplitude, so the pair
+                // loop needs no per-pair range test.  Threads 0-2 copy the FP64
+                // phase, threads 3-38 the 36 float2 fields from eps on (the last 8
+                // are the amplitudes); the barrier below publishes the copy.
+                auto patch = [&](int j, int src, int dst) {
+                    K2Pair &Q = sbuf[st][j];
+                    if (tid < 3) {
+                        Q.kc[tid][dst] = Q.kc[tid][src];
+                    } else {
+                        float2 *f = &Q.eps[0];
+                        const int i = tid - 3;
+                        const float v = i >= 28 ? 0.0f : (src ? f[i].y : f[i].x);
+                        if (dst)
+                            f[i].y = v;
+                        else
+                            f[i].x = v;
+                    }
+                };
+                if (c == 0 && (rbeg & 1)) patch(0, 1, 0);
+                if (c == nchunk - 1 && (rend & 1)) patch(n - 1, 0, 1);
+            }
             if (__syncthreads_or(!ok)) {
                 timed_out = true;
                 c_out = c;
                 break;
             }
-            const int n = (int)min((int64_t)K2P_CH, npair - c * K2P_CH);
             float2 acc[BPT][8];
 #pragma unroll
             for (int q = 0; q < BPT; q++)
@@ -1242,10 +1266,13 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
                     hi_ok = hi_ok && (m & 2u);
                     if (!lo_ok && !hi_ok) return;  // uniform over the CTA
                 }
+                // without the field-of-view test every lane adds (the edge pairs are
+                // patched above; a bin beyond nb is never written out)
 #pragma unroll
                 for (int q = 0; q < BPT; q++)
-                    k2_pair<FAST>(sbuf[st][j], fv, bd[q], acc[q], nkh, hkRh, sgh, s_hb, lo_ok && valid[q],
-                                  hi_ok && valid[q], P.xyz, P.nb);
+                    k2_pair<FAST>(sbuf[st][j], fv, bd[q], acc[q], nkh, hkRh, sgh, s_hb,
+                                  FAST ? (lo_ok && valid[q]) : true,
+                                  FAST ? (hi_ok && valid[q]) : true, P.xyz, P.nb);
             };
             if (FAST) {
                 // visit only the pairs with a record the tile cull kept: bit j of pm
