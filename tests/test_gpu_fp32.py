@@ -251,3 +251,19 @@ def test_fp32_poles_and_bodge_row_hemispheres(ctx, plan, theta_deg):
     # exact forward bin is ~1e-5 of that bin for these facet sizes)
     assert rel_err(afb + afe, rfb + rfe) <= 1e-4
     assert mueller_rel_err(_mueller(afb, afe), _mueller(rfb, rfe)) <= TOL_MU
+
+
+def test_fp32_precision_study_grid_100k_facets(ctx):
+    """The precision-study grid at full size (721 theta x 360 phi, 259,560 bins)
+    with half of its list (100,000 synthetic facets in a 100 um cube, phases up to
+    ~1,000 rad): the FP32 batch within its bars of the FP64 drop-in, Mueller
+    elements and cross sections."""
+    geo, beam, _ = W.synthetic_beam_list(n_beams=1000, facets_per_beam=100, seed=2024)
+    th, ph = W.grid_precision_study()
+    ext = np.zeros(0, dtype=beam.dtype)
+    pin = abt_b200.params(geo_cross_sec=1.0)
+    f = ctx.diff_batch([beam], [ext], [geo["verts"]], geo, th, ph, LAM, pin[None], precision="fp32")
+    r = ctx.diff_batch([beam], [ext], [geo["verts"]], geo, th, ph, LAM, pin[None], precision="fp64")
+    assert mueller_rel_err(f[0], r[0]) <= TOL_MU
+    for n in ("scatt", "asymmetry", "scatt_beam"):
+        assert abs(float(f[2][n]) - float(r[2][n])) <= TOL_PARAM * abs(float(r[2][n])), n
