@@ -62,11 +62,20 @@ enum {
 // record's constants scale into A_P2 at the end
 enum { P_TK = 0, P_WU01 = 3, P_KW = 6, K4_NPAIR = 7 };
 
-struct K4Rec {
+// Fields in groups of four floats on 16-byte boundaries, in the order the
+// bin loop reads them, so that the shared-memory reads can be 16 bytes wide.
+struct __align__(16) K4Rec {
     double kc[3];
-    float eps[3], b, R[9], ea[3], kp[2], p2[3], cf, icf, inc[3], xa[3], ya[3], amp[8];
-    float kw1, kw2, hicf;  // -p2z cf / 2, p2x p2y cf / 2, icf / 2
+    double pad0;
+    float eps[3], b;
+    float R[9], ea[3];
+    float kp[2], kw1, hicf;  // kw1 = -p2z cf / 2, hicf = icf / 2
+    float inc[3], kw2;       // kw2 = p2x p2y cf / 2
+    float xa[3], ya[3], cf, icf;
+    float p2[3], pad1;
+    float amp[8];
 };
+static_assert(sizeof(K4Rec) == 208, "K4Rec layout");
 
 // Per-bin input in HBM: the unit bin direction in FP64, 32 B (two 16-byte
 // loads).  The forward-bodge direction (same phi, first row above 1 degree)
@@ -78,6 +87,7 @@ struct __align__(16) K4Bin {
 struct Bin4 {
     double ux, uy, uz;
     float fx, fy, fz;
+    bool pole;     // within reach of the forward bodge for some record (|uz| near 1)
     int64_t o;     // bin index
     float2 G[4];   // cotangent of S' (pre-T, common phase removed) for the record's kind,
                    // circular basis of the columns: H+_1, H-_1, H+_2, H-_2
@@ -267,8 +277,12 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const float dd = fmaf(r.kw1, s, -kz * e);
     const float ee = fmaf(r.kw2, s, -kxkyc * e);
     const float kc3[3] = {kx, kyc, kz};
-    const float dinc = fmaf(r.inc[2], kz, fmaf(r.inc[1], kyc, r.inc[0] * kx));
-    const bool bodge = !(fabsf(dinc) < 0.999f);
+    // the forward bodge (src/diff_mod.f90:630-633) can apply only in bins near the poles
+    bool bodge = false;
+    if (B.pole) {
+        const float dinc = fmaf(r.inc[2], kz, fmaf(r.inc[1], kyc, r.inc[0] * kx));
+        bodge = !(fabsf(dinc) < 0.999f);
+    }
     Dir4 dh;
     float q[3] = {kx, kyc, kz};
     float hx = 0.0f, hy = 0.0f, hz = 0.0f;
@@ -462,7 +476,7 @@ template <bool FAST, int MINB>
 __global__ void __launch_bounds__(K4_WARPS * 32, MINB) k4_adjoint_kernel(
     const K4Rec *__restrict__ recs, const int *__restrict__ kinds, const float *__restrict__ fovdat,
     int64_t nrec, const K4Bin *__restrict__ bins, const float4 *__restrict__ gbin, int64_t nb,
-    int64_t nphi, int64_t theta_i, int64_t chunk, float k, float hkR, float iRf,
+    int64_t nphi, int64_t theta_i, int64_t chunk, float k, float hkR, float iRf, float pole_cos,
     double *__restrict__ out) {
     __shared__ K4Rec s_rec[K4_WARPS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -503,6 +517,7 @@ __global__ void __launch_bounds__(K4_WARPS * 32, MINB) k4_adjoint_kernel(
         B.fx = (float)B.ux;
         B.fy = (float)B.uy;
         B.fz = (float)B.uz;
+        B.pole = !(fabs(B.uz) < (double)pole_cos);
         B.o = o;
         const float4 *pg = G + 2 * o;
         const float4 g0 = pg[0], g1 = pg[1];
@@ -867,6 +882,15 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
     const int64_t chunk = (((nb + nsplit - 1) / nsplit) + 31) / 32 * 32;
     nsplit = (nb + chunk - 1) / chunk;
     const dim3 grid((unsigned)ncta_rec, (unsigned)nsplit);
+    // bins with |uz| below pole_cos are out of reach of the forward bodge: the
+    // direction from a facet centre c differs from the bin direction by at most
+    // 2 |c| / R, and |c| <= max |v| over the vertices
+    double vmax2 = 0.0;
+    for (int64_t i = 0; i < nverts; i++) {
+        const double x = verts[i], y = verts[i + nverts], z = verts[i + 2 * nverts];
+        vmax2 = std::max(vmax2, x * x + y * y + z * z);
+    }
+    const float pole_cos = (float)(0.999 - 2.0 * sqrt(vmax2) / Rf - 1e-5);
     timing_begin(ctx, st);
     // Minimum CTAs per SM for the register budget: 3 (168 registers, a few
     // bytes of spill) by default; PBT_K4_MINB=1|2|4 selects another build.
@@ -881,7 +905,7 @@ int k4_adjoint(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *beam, int64_t n
                 (const K4Rec *)(base + o_rec), (const int *)(base + o_kind), (const float *)(base + o_fov),
                 nrec, (const K4Bin *)(base + o_bin), (const float4 *)(base + o_gbin), nb, nphi,
                 g.theta_i, chunk, (float)k,
-                (float)(0.5 * k * Rf), (float)(1.0 / Rf), (double *)(base + o_out));
+                (float)(0.5 * k * Rf), (float)(1.0 / Rf), pole_cos, (double *)(base + o_out));
         };
         if (fast_diff) {
             if (minb == 1) launch(k4_adjoint_kernel<true, 1>);
