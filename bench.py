@@ -1018,10 +1018,29 @@ def main():
         terms[name] = {"achieved": a_ / 1e12, "peak": p_ / 1e12, "unit": unit, "frac": a_ / p_,
                        "per_facet_bin": w}
     bound = max(terms, key=lambda n: terms[n]["frac"])
+    # what the hardware actually runs (ncu counters of the same kernel on the
+    # 20,000-facet case): MUFU ops issued per facet-bin and the pipe loads
+    counters = None
+    cprof = os.path.join(ROOT, "profiles", "k2_main_pk_counters.json")
+    if os.path.exists(cprof):
+        try:
+            cj = json.load(open(cprof))
+            mi = float(cj["mufu_instructions_per_facet_bin"])
+            counters = {"mufu_issued_per_facet_bin": mi,
+                        "xu_frac_issued": terms["mufu"]["frac"] * mi / W_SFU,
+                        "issue_active": cj["issue_active"],
+                        "fma_pipe_cycles_active": cj["fma_pipe_cycles_active"],
+                        "thread_instructions_per_facet_bin": cj["thread_instructions_per_facet_bin"],
+                        "limiter": "instruction issue, then the FMA pipe; the convention's MUFU "
+                                   "term counts 20 special-function ops per facet-bin where the "
+                                   "kernel issues %.1f" % mi,
+                        "source": "profiles/k2_main_pk_counters.json (ncu)"}
+        except Exception:
+            counters = None
     roof = {"bound": bound, "achieved": terms[bound]["achieved"], "peak": terms[bound]["peak"],
             "unit": terms[bound]["unit"], "frac": terms[bound]["frac"], "traffic": traffic,
             "kernel": "k2_main_pk_kernel", "kernel_ms": kms, "units_per_launch": work,
-            "terms": terms,
+            "terms": terms, "issued": counters,
             "peak_basis": "%d SMs x %.0f MHz (median sampled SM clock) x per-clock issue width "
                           "(FP32 128 lanes, MUFU 16, FP64 64); MEASURED_PEAKS.json has no "
                           "FP32/MUFU/FP64 figure" % (sms, mhz)}
