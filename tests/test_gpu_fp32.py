@@ -1,6 +1,6 @@
 """FP32 form (FP64 phase) against the FP64 references.
 
-Bar (north-star precision target): <= 1e-4 relative on every Mueller element
+Bar (the FP32 precision target): <= 1e-4 relative on every Mueller element
 at bins whose M11 exceeds 1e-6 of the peak (normalised by the bin's M11, see
 helpers.mueller_rel_err); cross sections and asymmetry parameters within
 1e-5 relative.
