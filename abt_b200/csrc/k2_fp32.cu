@@ -781,9 +781,7 @@ constexpr int K2P_HB = K2_THREADS * 2;  // bodge table slots (bins per thread <=
 // absolute error would be a large relative one
 __device__ __forceinline__ float2 sinc_series(float2 h) {
     const float2 hh = mul2(h, h);
-    return fma2(hh, fma2(hh, fma2(hh, fma2(hh, bc2(2.7557319e-6f), bc2(-1.9841270e-4f)),
-                                  bc2(8.3333333e-3f)),
-                         bc2(-1.6666667e-1f)),
+    return fma2(hh, fma2(hh, fma2(hh, bc2(-1.9841270e-4f), bc2(8.3333333e-3f)), bc2(-1.6666667e-1f)),
                 bc2(1.0f));
 }
 
@@ -816,55 +814,55 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
     // 1/max(h1,.5), 1/max(h2,.5) and 2/D from one reciprocal of their product
     const float2 a1 = make_float2(fmaxf(h1.x, 0.5f), fmaxf(h1.y, 0.5f));
     const float2 a2 = make_float2(fmaxf(h2.x, 0.5f), fmaxf(h2.y, 0.5f));
-    const float2 Dg = make_float2(fmaxf(Dh.x, 0.125f), fmaxf(Dh.y, 0.125f));
     const float2 p12 = mul2(a1, a2);
-    const float2 pr = mul2(p12, Dg);
+    const float2 pr = mul2(p12, Dh);
     const float2 r = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
-    const float2 rD = mul2(Dg, r);
+    const float2 rD = mul2(Dh, r);
     // sinc(h1), sinc(h2) with the shared reciprocal (1/max(h, 0.5) = a2 rD,
     // a1 rD); the series is evaluated only when a lane of the warp needs it
     // (small gaps occur near a facet's specular and forward directions, so
     // whole warps of neighbouring bins mostly skip it), one vote for both
     float2 sc1 = mul2(make_float2(sin_fz(h1.x), sin_fz(h1.y)), mul2(a2, rD));
     float2 sc2 = mul2(make_float2(sin_fz(h2.x), sin_fz(h2.y)), mul2(a1, rD));
-    {
-        const bool ax = h1.x < 0.5f, ay = h1.y < 0.5f, bx = h2.x < 0.5f, by = h2.y < 0.5f;
-        if (__any_sync(0xffffffffu, ax || ay || bx || by)) {
-            sc1 = sel2(ax, ay, sinc_series(h1), sc1);
-            sc2 = sel2(bx, by, sinc_series(h2), sc2);
-        }
-    }
     const float2 iD = mul2(mul2(p12, r), sc);  // 2 sc / D
-    gx = mul2(fma2(sc1, s1, neg2(mul2(sc2, s2))), iD);
-    gy = mul2(fma2(sc2, k2, neg2(mul2(sc1, k1))), iD);
-    if (Dh.x < 0.125f || Dh.y < 0.125f) {
-        // all three full phases within 0.25 rad: Taylor series about the middle
-        // phase, g = e^{2i mid} sum_n i^(n+2)/(n+2)! q_n(ya, yc) with the complete
-        // homogeneous q_n of the full-phase offsets 2 ya, 2 yc (2^n folded into
-        // the coefficients)
-        const float2 ya = add2(lo, neg2(mid)), yc = add2(hi, neg2(mid));
-        const float2 q1 = add2(ya, yc);
-        const float2 ya2 = mul2(ya, ya);
-        const float2 q2 = fma2(yc, q1, ya2);
-        const float2 ya3 = mul2(ya2, ya);
-        const float2 q3 = fma2(yc, q2, ya3);
-        const float2 ya4 = mul2(ya3, ya);
-        const float2 q4 = fma2(yc, q3, ya4);
-        const float2 q5 = fma2(yc, q4, mul2(ya4, ya));
-        const float2 q6 = fma2(yc, q5, mul2(ya4, ya2));
-        const float2 tsc = add2(sc, sc);
-        const float2 re = mul2(tsc, fma2(q6, bc2(1.0f / 630.0f),
-                                         fma2(q4, bc2(-1.0f / 45.0f), fma2(q2, bc2(1.0f / 6.0f), bc2(-0.5f)))));
-        const float2 im = mul2(tsc, fma2(q5, bc2(-2.0f / 315.0f),
-                                         fma2(q3, bc2(1.0f / 15.0f), mul2(q1, bc2(-1.0f / 3.0f)))));
-        const float2 m2 = add2(mid, mid);
-        float2 sm, cm;
-        sm = make_float2(sin_fz(m2.x), sin_fz(m2.y));
-        cm = make_float2(cos_fz(m2.x), cos_fz(m2.y));
-        const float2 sx = fma2(cm, re, neg2(mul2(sm, im)));
-        const float2 sy = fma2(cm, im, mul2(sm, re));
-        gx = sel2(Dh.x < 0.125f, Dh.y < 0.125f, sx, gx);
-        gy = sel2(Dh.x < 0.125f, Dh.y < 0.125f, sy, gy);
+    const bool ax = h1.x < 0.5f, ay = h1.y < 0.5f, bx = h2.x < 0.5f, by = h2.y < 0.5f;
+    if (__any_sync(0xffffffffu, ax || ay || bx || by)) {
+        sc1 = sel2(ax, ay, sinc_series(h1), sc1);
+        sc2 = sel2(bx, by, sinc_series(h2), sc2);
+        gx = mul2(fma2(sc1, s1, neg2(mul2(sc2, s2))), iD);
+        gy = mul2(fma2(sc2, k2, neg2(mul2(sc1, k1))), iD);
+        if (Dh.x < 0.125f || Dh.y < 0.125f) {
+            // all three full phases within 0.25 rad: Taylor series about the middle
+            // phase, g = e^{2i mid} sum_n i^(n+2)/(n+2)! q_n(ya, yc) with the complete
+            // homogeneous q_n of the full-phase offsets 2 ya, 2 yc (2^n folded into
+            // the coefficients)
+            const float2 ya = add2(lo, neg2(mid)), yc = add2(hi, neg2(mid));
+            const float2 q1 = add2(ya, yc);
+            const float2 ya2 = mul2(ya, ya);
+            const float2 q2 = fma2(yc, q1, ya2);
+            const float2 ya3 = mul2(ya2, ya);
+            const float2 q3 = fma2(yc, q2, ya3);
+            const float2 ya4 = mul2(ya3, ya);
+            const float2 q4 = fma2(yc, q3, ya4);
+            const float2 q5 = fma2(yc, q4, mul2(ya4, ya));
+            const float2 q6 = fma2(yc, q5, mul2(ya4, ya2));
+            const float2 tsc = add2(sc, sc);
+            const float2 re = mul2(tsc, fma2(q6, bc2(1.0f / 630.0f),
+                                             fma2(q4, bc2(-1.0f / 45.0f), fma2(q2, bc2(1.0f / 6.0f), bc2(-0.5f)))));
+            const float2 im = mul2(tsc, fma2(q5, bc2(-2.0f / 315.0f),
+                                             fma2(q3, bc2(1.0f / 15.0f), mul2(q1, bc2(-1.0f / 3.0f)))));
+            const float2 m2 = add2(mid, mid);
+            float2 sm, cm;
+            sm = make_float2(sin_fz(m2.x), sin_fz(m2.y));
+            cm = make_float2(cos_fz(m2.x), cos_fz(m2.y));
+            const float2 sx = fma2(cm, re, neg2(mul2(sm, im)));
+            const float2 sy = fma2(cm, im, mul2(sm, re));
+            gx = sel2(Dh.x < 0.125f, Dh.y < 0.125f, sx, gx);
+            gy = sel2(Dh.x < 0.125f, Dh.y < 0.125f, sy, gy);
+        }
+    } else {
+        gx = mul2(fma2(sc1, s1, neg2(mul2(sc2, s2))), iD);
+        gy = mul2(fma2(sc2, k2, neg2(mul2(sc1, k1))), iD);
     }
 }
 
@@ -951,13 +949,12 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     // rounding and d1 = (sqrt(1 - Ky^2)/2) (kzc tt - kz), e1 = (sqrt(1 - Ky^2)/2)(-kx kyc)
     // (the Kx Ky term is below 1e-16 and left out); the common factor is in the
     // record's amplitudes and sc in the divided difference.
-    const float2 kyc = make_float2(fminf(fmaxf(ky.x, -0.999999f), 0.999999f),
-                                   fminf(fmaxf(ky.y, -0.999999f), 0.999999f));
+    // Main path: |ky| < 0.999999 (no clamp) and no forward bodge, so kyc = ky
+    // and tt = kx^2 + kz^2; h = inc x (kx, ky, kz) = inc x ks.
     const float2 tr = fma2(kx, kx, mul2(kz, kz));
-    const float2 tt = make_float2(fmaxf(tr.x, kOneMinusClampSq), fmaxf(tr.y, kOneMinusClampSq));
-    const float2 d1 = fma2(kzc, tt, neg2(kz));
-    const float2 e1 = mul2(neg2(kx), kyc);
-    // h = inc x (kx, ky, kz) = inc x ks
+    float2 tt = tr;
+    float2 d1 = fma2(kzc, tr, neg2(kz));
+    float2 e1 = mul2(neg2(kx), ky);
     float2 hx = fma2(inc1, ks2, neg2(mul2(inc2, ks1)));
     float2 hy = fma2(inc2, ks0, neg2(mul2(inc0, ks2)));
     float2 hz = fma2(inc0, ks1, neg2(mul2(inc1, ks0)));
@@ -965,67 +962,78 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     // Where h is normal to q = (kx, kyc, kz), hx kx + hz kz = -hy kyc and
     // P1 = hy (tt + kyc^2) = hy |q|^2 = hy (|q| = 1 up to rounding; on the clamp
     // tt + kyc^2 = 1 - c^2 + c^2); the forward bodge takes the general form.
-    float2 P1 = hy;
-    bool bx = false, by = false;
-    if (B.pole) {
-        // the forward bodge (src/diff_mod.f90:630-633) can apply only in bins near
-        // the poles; dinc = inc . (kx, kyc, kz)
-        const float2 dinc = fma2(inc2, kz, fma2(inc1, kyc, mul2(inc0, kx)));
-        bx = !(fabsf(dinc.x) < 0.999f);
-        by = !(fabsf(dinc.y) < 0.999f);
-        if (bx || by) {
-            // the bodge direction in the s form: hs = uh + sgh z, uh . eps = hs . eps - sgh eps_z,
-            // h = inc x (R hs oh2 + nea oh)
-            const float2 hx_ = bc2(hb[0][B.hslot]), hy_ = bc2(hb[1][B.hslot]),
-                         hsz = bc2(hb[2][B.hslot]);
-            float2 ah = fma2(hsz, eps2, fma2(hy_, eps1, mul2(hx_, eps0)));
-            ah = fma2(neg2(sgh), eps2, ah);
-            const float2 oh = add2(one, ah);
-            const float2 oh2 = fma2(ah, fma2(bc2(1.5f), ah, one), fma2(bc2(-0.5f), pb, one));
-            const float2 vx = fma2(fma2(P.R[2], hsz, fma2(P.R[1], hy_, mul2(P.R[0], hx_))), oh2,
-                                   mul2(P.nea[0], oh));
-            const float2 vy = fma2(fma2(P.R[5], hsz, fma2(P.R[4], hy_, mul2(P.R[3], hx_))), oh2,
-                                   mul2(P.nea[1], oh));
-            const float2 vz = fma2(fma2(P.R[8], hsz, fma2(P.R[7], hy_, mul2(P.R[6], hx_))), oh2,
-                                   mul2(P.nea[2], oh));
-            const float2 gx = fma2(inc1, vz, neg2(mul2(inc2, vy)));
-            const float2 gy = fma2(inc2, vx, neg2(mul2(inc0, vz)));
-            const float2 gz = fma2(inc0, vy, neg2(mul2(inc1, vx)));
-            const float2 gP = fma2(gy, tt, neg2(mul2(kyc, fma2(gx, kx, mul2(gz, kz)))));
-            hx = sel2(bx, by, gx, hx);
-            hy = sel2(bx, by, gy, hy);
-            hz = sel2(bx, by, gz, hz);
-            P1 = sel2(bx, by, gP, P1);
+    // Inside the clamp evo2 = (-kz, 0, kx) / s, so R1 = rr |h| s = hz kx - hx kz.
+    float2 P1 = hy, R1;
+    const bool cx = tr.x <= kOneMinusClampSq, cy = tr.y <= kOneMinusClampSq;
+    if (B.pole || cx || cy) {
+        // near the poles (the forward bodge) or on the clamp: ky clamped to
+        // +-0.999999 and tt to 1 - 0.999999^2 as in src/diff_mod.f90
+        const float2 kyc = make_float2(fminf(fmaxf(ky.x, -0.999999f), 0.999999f),
+                                       fminf(fmaxf(ky.y, -0.999999f), 0.999999f));
+        tt = make_float2(fmaxf(tr.x, kOneMinusClampSq), fmaxf(tr.y, kOneMinusClampSq));
+        d1 = fma2(kzc, tt, neg2(kz));
+        e1 = mul2(neg2(kx), kyc);
+        bool bx = false, by = false;
+        if (B.pole) {
+            // the forward bodge (src/diff_mod.f90:630-633) can apply only in bins near
+            // the poles; dinc = inc . (kx, kyc, kz)
+            const float2 dinc = fma2(inc2, kz, fma2(inc1, kyc, mul2(inc0, kx)));
+            bx = !(fabsf(dinc.x) < 0.999f);
+            by = !(fabsf(dinc.y) < 0.999f);
+            if (bx || by) {
+                // the bodge direction in the s form: hs = uh + sgh z, uh . eps = hs . eps - sgh eps_z,
+                // h = inc x (R hs oh2 + nea oh)
+                const float2 hx_ = bc2(hb[0][B.hslot]), hy_ = bc2(hb[1][B.hslot]),
+                             hsz = bc2(hb[2][B.hslot]);
+                float2 ah = fma2(hsz, eps2, fma2(hy_, eps1, mul2(hx_, eps0)));
+                ah = fma2(neg2(sgh), eps2, ah);
+                const float2 oh = add2(one, ah);
+                const float2 oh2 = fma2(ah, fma2(bc2(1.5f), ah, one), fma2(bc2(-0.5f), pb, one));
+                const float2 vx = fma2(fma2(P.R[2], hsz, fma2(P.R[1], hy_, mul2(P.R[0], hx_))), oh2,
+                                       mul2(P.nea[0], oh));
+                const float2 vy = fma2(fma2(P.R[5], hsz, fma2(P.R[4], hy_, mul2(P.R[3], hx_))), oh2,
+                                       mul2(P.nea[1], oh));
+                const float2 vz = fma2(fma2(P.R[8], hsz, fma2(P.R[7], hy_, mul2(P.R[6], hx_))), oh2,
+                                       mul2(P.nea[2], oh));
+                const float2 gx = fma2(inc1, vz, neg2(mul2(inc2, vy)));
+                const float2 gy = fma2(inc2, vx, neg2(mul2(inc0, vz)));
+                const float2 gz = fma2(inc0, vy, neg2(mul2(inc1, vx)));
+                const float2 gP = fma2(gy, tt, neg2(mul2(kyc, fma2(gx, kx, mul2(gz, kz)))));
+                hx = sel2(bx, by, gx, hx);
+                hy = sel2(bx, by, gy, hy);
+                hz = sel2(bx, by, gz, hz);
+                P1 = sel2(bx, by, gP, P1);
+            }
         }
-    }
-    const bool cx = tt.x <= kOneMinusClampSq, cy = tt.y <= kOneMinusClampSq;
-    float2 rc = bc2(0.0f);
-    if (cx || cy) {
-        // a lane on the clamp: outside the bodge, h = inc x (kx, kyc, kz) takes the
-        // clamped ky (q_y = ks1 + kyc - ky); evo2 = normalise(k x m) with the clamped
-        // ky, R1 = s (h . evo2)
-        const float2 qy = add2(ks1, add2(kyc, neg2(ky)));
-        const float2 fx = fma2(inc1, ks2, neg2(mul2(inc2, qy)));
-        const float2 fz = fma2(inc0, qy, neg2(mul2(inc1, ks0)));
-        const bool ux = cx && !bx, uy = cy && !by;
-        hx = sel2(ux, uy, fx, hx);
-        hz = sel2(ux, uy, fz, hz);
-        const float2 rs = make_float2(rsqrtf(tt.x), rsqrtf(tt.y));
-        const float2 s = mul2(tt, rs), kyrs = mul2(kyc, rs);
-        const float2 m0 = neg2(mul2(kx, kyrs)), m1 = s, m2 = neg2(mul2(kz, kyrs));
-        float2 ex = fma2(kyc, m2, neg2(mul2(kz, m1)));
-        float2 ey = fma2(kz, m0, neg2(mul2(kx, m2)));
-        float2 ez = fma2(kx, m1, neg2(mul2(kyc, m0)));
-        const float2 en2 = fma2(ez, ez, fma2(ey, ey, mul2(ex, ex)));
-        const float2 ne = make_float2(cx ? rsqrtf(en2.x) : 1.0f, cy ? rsqrtf(en2.y) : 1.0f);
-        rc = mul2(mul2(s, ne), fma2(hz, ez, fma2(hy, ey, mul2(hx, ex))));
+        if (cx || cy) {
+            // a lane on the clamp: outside the bodge, h = inc x (kx, kyc, kz) takes the
+            // clamped ky (q_y = ks1 + kyc - ky); evo2 = normalise(k x m) with the clamped
+            // ky, R1 = s (h . evo2)
+            const float2 qy = add2(ks1, add2(kyc, neg2(ky)));
+            const float2 fx = fma2(inc1, ks2, neg2(mul2(inc2, qy)));
+            const float2 fz = fma2(inc0, qy, neg2(mul2(inc1, ks0)));
+            const bool ux = cx && !bx, uy = cy && !by;
+            hx = sel2(ux, uy, fx, hx);
+            hz = sel2(ux, uy, fz, hz);
+            const float2 rs = make_float2(rsqrtf(tt.x), rsqrtf(tt.y));
+            const float2 s = mul2(tt, rs), kyrs = mul2(kyc, rs);
+            const float2 m0 = neg2(mul2(kx, kyrs)), m1 = s, m2 = neg2(mul2(kz, kyrs));
+            float2 ex = fma2(kyc, m2, neg2(mul2(kz, m1)));
+            float2 ey = fma2(kz, m0, neg2(mul2(kx, m2)));
+            float2 ez = fma2(kx, m1, neg2(mul2(kyc, m0)));
+            const float2 en2 = fma2(ez, ez, fma2(ey, ey, mul2(ex, ex)));
+            const float2 ne = make_float2(cx ? rsqrtf(en2.x) : 1.0f, cy ? rsqrtf(en2.y) : 1.0f);
+            const float2 rc = mul2(mul2(s, ne), fma2(hz, ez, fma2(hy, ey, mul2(hx, ex))));
+            R1 = sel2(cx, cy, rc, fma2(hz, kx, neg2(mul2(hx, kz))));
+        } else {
+            R1 = fma2(hz, kx, neg2(mul2(hx, kz)));
+        }
+    } else {
+        R1 = fma2(hz, kx, neg2(mul2(hx, kz)));
     }
     const float2 hn2 = fma2(hz, hz, fma2(hy, hy, mul2(hx, hx)));
     const float2 ht = mul2(mul2(hn2, tt), tt);
     const float2 sc = make_float2(rsqrt_fz(ht.x), rsqrt_fz(ht.y));
-    // inside the clamp evo2 = (-kz, 0, kx) / s, so R1 = rr |h| s = hz kx - hx kz
-    float2 R1 = fma2(hz, kx, neg2(mul2(hx, kz)));
-    if (cx || cy) R1 = sel2(cx, cy, rc, R1);
     const float2 A = fma2(P1, d1, mul2(R1, e1));
     const float2 Bc = fma2(P1, e1, neg2(mul2(R1, d1)));
     // aperture integral on the half phases (after the polarisation block, so
