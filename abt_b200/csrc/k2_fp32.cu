@@ -786,11 +786,13 @@ __device__ __forceinline__ float2 sinc_series(float2 h) {
 }
 
 // 2 sc g for each lane, g the second divided difference of e^{ix} at the full
-// phases 2 t1, 2 t2, 2 t3, from the half phases t.  With the half phases
-// sorted (lo <= mid <= hi) the edge midpoints of the full phases are lo + mid
-// and mid + hi and the half gaps mid - lo and hi - mid, each one operation.
-__device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float2 sc, float2 &gx,
-                                          float2 &gy) {
+// phases 2 t1, 2 t2, 2 t3, from the half phases t, and sc = 1 / (|h| tt) =
+// rsqrt(hn2 tt^2) the normalisation of the polarisation block.  With the half
+// phases sorted (lo <= mid <= hi) the edge midpoints of the full phases are
+// lo + mid and mid + hi and the half gaps mid - lo and hi - mid, each one
+// operation.
+__device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float2 hn2, float2 tt,
+                                          float2 &gx, float2 &gy) {
     float2 lo, hi, mid;
     lo.x = fminf(t1.x, t2.x);
     hi.x = fmaxf(t1.x, t2.x);
@@ -811,26 +813,28 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
     k1 = make_float2(cos_fz(c1.x), cos_fz(c1.y));
     s2 = make_float2(sin_fz(c2.x), sin_fz(c2.y));
     k2 = make_float2(cos_fz(c2.x), cos_fz(c2.y));
-    // 1/max(h1,.5), 1/max(h2,.5) and 2/D from one reciprocal of their product
+    // With a1 = max(h1, .5) and a2 = max(h2, .5), 2 sc g = scr (S1 e^{i c1} -
+    // S2 e^{i c2}) (imaginary unit and sign aside), S1 = sinc(h1) a1 a2,
+    // S2 = sinc(h2) a1 a2 and scr = sc / (a1 a2 Dh): one reciprocal square root,
+    // rsqrt(hn2 (tt a1 a2 Dh)^2), gives the polarisation block's normalisation,
+    // 1/a1, 1/a2 and 2/D.  Where h >= 0.5, sinc(h1) a1 a2 = a2 sin(h1).
     const float2 a1 = make_float2(fmaxf(h1.x, 0.5f), fmaxf(h1.y, 0.5f));
     const float2 a2 = make_float2(fmaxf(h2.x, 0.5f), fmaxf(h2.y, 0.5f));
     const float2 p12 = mul2(a1, a2);
-    const float2 pr = mul2(p12, Dh);
-    const float2 r = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
-    const float2 rD = mul2(Dh, r);
-    // sinc(h1), sinc(h2) with the shared reciprocal (1/max(h, 0.5) = a2 rD,
-    // a1 rD); the series is evaluated only when a lane of the warp needs it
-    // (small gaps occur near a facet's specular and forward directions, so
-    // whole warps of neighbouring bins mostly skip it), one vote for both
-    float2 sc1 = mul2(make_float2(sin_fz(h1.x), sin_fz(h1.y)), mul2(a2, rD));
-    float2 sc2 = mul2(make_float2(sin_fz(h2.x), sin_fz(h2.y)), mul2(a1, rD));
-    const float2 iD = mul2(mul2(p12, r), sc);  // 2 sc / D
+    const float2 q = mul2(mul2(p12, Dh), tt);
+    const float2 hq = mul2(hn2, mul2(q, q));
+    const float2 scr = make_float2(rsqrt_fz(hq.x), rsqrt_fz(hq.y));
+    float2 S1 = mul2(make_float2(sin_fz(h1.x), sin_fz(h1.y)), a2);
+    float2 S2 = mul2(make_float2(sin_fz(h2.x), sin_fz(h2.y)), a1);
+    // below h = 0.5 sinc(h) from its series, evaluated only when a lane of the
+    // warp needs it (small gaps occur near a facet's specular and forward
+    // directions), one vote for both
     const bool ax = h1.x < 0.5f, ay = h1.y < 0.5f, bx = h2.x < 0.5f, by = h2.y < 0.5f;
     if (__any_sync(0xffffffffu, ax || ay || bx || by)) {
-        sc1 = sel2(ax, ay, sinc_series(h1), sc1);
-        sc2 = sel2(bx, by, sinc_series(h2), sc2);
-        gx = mul2(fma2(sc1, s1, neg2(mul2(sc2, s2))), iD);
-        gy = mul2(fma2(sc2, k2, neg2(mul2(sc1, k1))), iD);
+        S1 = sel2(ax, ay, mul2(sinc_series(h1), p12), S1);
+        S2 = sel2(bx, by, mul2(sinc_series(h2), p12), S2);
+        gx = mul2(fma2(S1, s1, neg2(mul2(S2, s2))), scr);
+        gy = mul2(fma2(S2, k2, neg2(mul2(S1, k1))), scr);
         if (Dh.x < 0.125f || Dh.y < 0.125f) {
             // all three full phases within 0.25 rad: Taylor series about the middle
             // phase, g = e^{2i mid} sum_n i^(n+2)/(n+2)! q_n(ya, yc) with the complete
@@ -846,7 +850,8 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
             const float2 q4 = fma2(yc, q3, ya4);
             const float2 q5 = fma2(yc, q4, mul2(ya4, ya));
             const float2 q6 = fma2(yc, q5, mul2(ya4, ya2));
-            const float2 tsc = add2(sc, sc);
+            const float2 ht = mul2(mul2(hn2, tt), tt);
+            const float2 tsc = make_float2(2.0f * rsqrt_fz(ht.x), 2.0f * rsqrt_fz(ht.y));
             const float2 re = mul2(tsc, fma2(q6, bc2(1.0f / 630.0f),
                                              fma2(q4, bc2(-1.0f / 45.0f), fma2(q2, bc2(1.0f / 6.0f), bc2(-0.5f)))));
             const float2 im = mul2(tsc, fma2(q5, bc2(-2.0f / 315.0f),
@@ -861,8 +866,8 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
             gy = sel2(Dh.x < 0.125f, Dh.y < 0.125f, sy, gy);
         }
     } else {
-        gx = mul2(fma2(sc1, s1, neg2(mul2(sc2, s2))), iD);
-        gy = mul2(fma2(sc2, k2, neg2(mul2(sc1, k1))), iD);
+        gx = mul2(fma2(S1, s1, neg2(mul2(S2, s2))), scr);
+        gy = mul2(fma2(S2, k2, neg2(mul2(S1, k1))), scr);
     }
 }
 
@@ -1032,8 +1037,6 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
         R1 = fma2(hz, kx, neg2(mul2(hx, kz)));
     }
     const float2 hn2 = fma2(hz, hz, fma2(hy, hy, mul2(hx, hx)));
-    const float2 ht = mul2(mul2(hn2, tt), tt);
-    const float2 sc = make_float2(rsqrt_fz(ht.x), rsqrt_fz(ht.y));
     const float2 A = fma2(P1, d1, mul2(R1, e1));
     const float2 Bc = fma2(P1, e1, neg2(mul2(R1, d1)));
     // aperture integral on the half phases (after the polarisation block, so
@@ -1047,7 +1050,7 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
         const float2 t1 = fma2(kyy, vy0, fma2(kxx, vx0, ph));
         const float2 t2 = fma2(kyy, vy1, fma2(kxx, vx1, ph));
         const float2 t3 = fma2(kyy, vy2, fma2(kxx, vx2, ph));
-        tri_dd_pk(t1, t2, t3, sc, gx, gy);
+        tri_dd_pk(t1, t2, t3, hn2, tt, gx, gy);
     }
     // [[A, B], [-B, A]] is diagonal in the circular basis: with z = A - iB the
     // columns' u+ take z, their u- take conj(z).  q+ = g z, q- = g conj(z).
