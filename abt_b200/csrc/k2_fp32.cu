@@ -777,12 +777,12 @@ struct BinPk {
 };
 constexpr int K2P_HB = K2_THREADS * 2;  // bodge table slots (bins per thread <= 2)
 
-// Taylor series of sin(h)/h, used below h = 0.5 where the MUFU sine's
-// absolute error would be a large relative one
+// sin(h)/h below h = 0.5, where the MUFU sine's absolute error would be a large
+// relative one: 1 + c1 h^2 + c2 h^4 with c1, c2 the minimax fit to the relative
+// error on [0, 0.5] (Lawson's iteration: 1.2e-7, 1.6e-7 evaluated in FP32)
 __device__ __forceinline__ float2 sinc_series(float2 h) {
     const float2 hh = mul2(h, h);
-    return fma2(hh, fma2(hh, fma2(hh, bc2(-1.9841270e-4f), bc2(8.3333333e-3f)), bc2(-1.6666667e-1f)),
-                bc2(1.0f));
+    return fma2(hh, fma2(hh, bc2(8.264339e-3f), bc2(-1.6666131e-1f)), bc2(1.0f));
 }
 
 // 2 sc g for each lane, g the second divided difference of e^{ix} at the full
