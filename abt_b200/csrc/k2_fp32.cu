@@ -903,9 +903,12 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     ld22(&P.eps[2], eps2, pb);
     // a = u . eps = s . eps - sg eps_z
     const float2 a = fma2(neg2(B.sg), eps2, fma2(B.sz, eps2, fma2(B.fy, eps1, mul2(B.fx, eps0))));
+    // with y = b - a^2: half phase hkRh y (1 + a) - rf, and
+    // opa2 = 1 + a + 1.5 a^2 - 0.5 b = (1 + a) - 0.5 y + a^2
     const float2 opa = add2(one, a);
-    const float2 ph = fma2(mul2(hkRh, fma2(neg2(a), a, pb)), opa, neg2(rf));  // half phase
-    const float2 opa2 = fma2(a, fma2(bc2(1.5f), a, one), fma2(bc2(-0.5f), pb, one));
+    const float2 y = fma2(neg2(a), a, pb);
+    const float2 ph = fma2(mul2(hkRh, y), opa, neg2(rf));
+    const float2 opa2 = fma2(a, a, fma2(bc2(-0.5f), y, opa));
     // The bin direction enters through s = u + sg z (sg = +1 in the hemisphere of
     // the incidence direction (0,0,-1), -1 in the other), which is small and known
     // to full FP32 precision near both poles.  With inc = -R z (the incidence
