@@ -141,6 +141,37 @@ __device__ __forceinline__ void sinc_d(float h, float rh, bool series, float &sc
     }
 }
 
+// g, dg/dlo, dg/dhi from the series about mid, for phases within 0.25 rad
+__device__ __forceinline__ void dd_series(float lo, float mid, float hi, float2 &g, float2 &dlo,
+                                          float2 &dhi) {
+    // series about mid: g = e^{i mid} sum_n c_n h_n(ya, yc), c_n = i^(n+2)/(n+2)!
+    const float ya = lo - mid, yc = hi - mid;
+    const float cr[8] = {-0.5f, 0.0f, 1.0f / 24.0f, 0.0f, -1.0f / 720.0f, 0.0f, 1.0f / 40320.0f, 0.0f};
+    const float ci[8] = {0.0f, -1.0f / 6.0f, 0.0f, 1.0f / 120.0f, 0.0f, -1.0f / 5040.0f, 0.0f,
+                         1.0f / 362880.0f};
+    float hq = 1.0f, da = 0.0f, dc = 0.0f, yap = 1.0f;
+    float2 sg = make_float2(cr[0], ci[0]), sa = make_float2(0, 0), sc = make_float2(0, 0);
+#pragma unroll
+    for (int n = 1; n < 8; n++) {
+        dc = fmaf(yc, dc, hq);
+        da = fmaf(yc, da, (float)n * yap);
+        yap *= ya;
+        hq = fmaf(yc, hq, yap);
+        sg.x = fmaf(cr[n], hq, sg.x);
+        sg.y = fmaf(ci[n], hq, sg.y);
+        sa.x = fmaf(cr[n], da, sa.x);
+        sa.y = fmaf(ci[n], da, sa.y);
+        sc.x = fmaf(cr[n], dc, sc.x);
+        sc.y = fmaf(ci[n], dc, sc.y);
+    }
+    float sm, cm;
+    sincos4(mid, &sm, &cm);
+    auto rot = [&](float2 z) { return make_float2(cm * z.x - sm * z.y, cm * z.y + sm * z.x); };
+    g = rot(sg);
+    dlo = rot(sa);
+    dhi = rot(sc);
+}
+
 // g = second divided difference of e^{ix} at t0, t1, t2, and dg/dlo, dg/dhi
 // for the smallest and largest phase (dg/dmid = i g - dg/dlo - dg/dhi, since
 // g(t + s) = e^{is} g(t)).
@@ -174,34 +205,54 @@ __device__ __forceinline__ void dd_grad(float t0, float t1, float t2, float2 &g,
         dlo = mul2(fma2(bc2(0.5f * dsc1), n1, fma2(bc2(-0.5f * sc1), in1, g)), iD2);
         dhi = mul2(fma2(bc2(0.5f * dsc2), n2, fma2(bc2(0.5f * sc2), in2, make_float2(-g.x, -g.y))), iD2);
     }
-    if (D < 0.25f) {
-        // series about mid: g = e^{i mid} sum_n c_n h_n(ya, yc), c_n = i^(n+2)/(n+2)!
-        const float ya = lo - mid, yc = hi - mid;
-        const float cr[8] = {-0.5f, 0.0f, 1.0f / 24.0f, 0.0f, -1.0f / 720.0f, 0.0f, 1.0f / 40320.0f, 0.0f};
-        const float ci[8] = {0.0f, -1.0f / 6.0f, 0.0f, 1.0f / 120.0f, 0.0f, -1.0f / 5040.0f, 0.0f,
-                             1.0f / 362880.0f};
-        float hq = 1.0f, da = 0.0f, dc = 0.0f, yap = 1.0f;
-        float2 sg = make_float2(cr[0], ci[0]), sa = make_float2(0, 0), sc = make_float2(0, 0);
-#pragma unroll
-        for (int n = 1; n < 8; n++) {
-            dc = fmaf(yc, dc, hq);
-            da = fmaf(yc, da, (float)n * yap);
-            yap *= ya;
-            hq = fmaf(yc, hq, yap);
-            sg.x = fmaf(cr[n], hq, sg.x);
-            sg.y = fmaf(ci[n], hq, sg.y);
-            sa.x = fmaf(cr[n], da, sa.x);
-            sa.y = fmaf(ci[n], da, sa.y);
-            sc.x = fmaf(cr[n], dc, sc.x);
-            sc.y = fmaf(ci[n], dc, sc.y);
+    if (D < 0.25f) dd_series(lo, mid, hi, g, dlo, dhi);
+}
+
+// dd_grad for the main bin step: D unguarded (below 0.25 the series about mid
+// replaces g, dlo and dhi, and D < 0.25 puts both half gaps below 0.5, inside
+// the warp's series branch), sinc and sinc' below h = 0.5 from minimax fits to
+// their relative error on [0, 0.5] (Lawson's iteration; 1.2e-7 and 3.3e-8),
+// and the outputs formed in scalar arithmetic.
+__device__ __forceinline__ void dd_grad_main(float t0, float t1, float t2, float2 &g, float2 &dlo,
+                                             float2 &dhi) {
+    const float lo = fminf(fminf(t0, t1), t2), hi = fmaxf(fmaxf(t0, t1), t2);
+    const float mid = fmaxf(fminf(t0, t1), fminf(fmaxf(t0, t1), t2));
+    const float D = hi - lo;
+    const float h1 = 0.5f * (mid - lo), h2 = 0.5f * (hi - mid);
+    float s1, c1, s2, c2, sn1, cs1, sn2, cs2;
+    sincos4(lo + h1, &s1, &c1);
+    sincos4(mid + h2, &s2, &c2);
+    sincos4(h1, &sn1, &cs1);
+    sincos4(h2, &sn2, &cs2);
+    // 1/max(h1,.5), 1/max(h2,.5) and 1/D from one reciprocal
+    const float a1 = fmaxf(h1, 0.5f), a2 = fmaxf(h2, 0.5f);
+    const float p12 = a1 * a2;
+    const float r = rcp4(p12 * D);
+    const float rD = D * r, iD = p12 * r;
+    const float rh1 = a2 * rD, rh2 = a1 * rD;
+    float sc1 = sn1 * rh1, sc2 = sn2 * rh2;
+    float dsc1 = (cs1 - sc1) * rh1, dsc2 = (cs2 - sc2) * rh2;
+    const bool series = __any_sync(__activemask(), fminf(h1, h2) < 0.5f);
+    if (series) {
+        const float x1 = h1 * h1, x2 = h2 * h2;
+        if (h1 < 0.5f) {
+            sc1 = fmaf(x1, fmaf(x1, 8.264339e-3f, -1.6666131e-1f), 1.0f);
+            dsc1 = h1 * fmaf(x1, fmaf(x1, -1.1822202e-3f, 3.3332558e-2f), -3.3333332e-1f);
         }
-        float sm, cm;
-        sincos4(mid, &sm, &cm);
-        auto rot = [&](float2 z) { return make_float2(cm * z.x - sm * z.y, cm * z.y + sm * z.x); };
-        g = rot(sg);
-        dlo = rot(sa);
-        dhi = rot(sc);
+        if (h2 < 0.5f) {
+            sc2 = fmaf(x2, fmaf(x2, 8.264339e-3f, -1.6666131e-1f), 1.0f);
+            dsc2 = h2 * fmaf(x2, fmaf(x2, -1.1822202e-3f, 3.3332558e-2f), -3.3333332e-1f);
+        }
     }
+    // E = i e^{ic} sinc(h) = sc n with n = (-s, c), i n = (-c, -s), dE/dh = dsc n:
+    // g = (E2 - E1) / D, dg/dlo = (g - (iE1 - H1)/2) / D, dg/dhi = ((iE2 + H2)/2 - g) / D
+    const float gx = iD * fmaf(sc1, s1, -sc2 * s2), gy = iD * fmaf(sc2, c2, -sc1 * c1);
+    g = make_float2(gx, gy);
+    dlo = make_float2(iD * fmaf(0.5f, fmaf(sc1, c1, -dsc1 * s1), gx),
+                      iD * fmaf(0.5f, fmaf(dsc1, c1, sc1 * s1), gy));
+    dhi = make_float2(iD * fmaf(-0.5f, fmaf(dsc2, s2, sc2 * c2), -gx),
+                      iD * fmaf(0.5f, fmaf(dsc2, c2, -sc2 * s2), -gy));
+    if (series && D < 0.25f) dd_series(lo, mid, hi, g, dlo, dhi);
 }
 
 // Bin direction from the facet centre in the aperture frame (second order in c/R)
@@ -241,6 +292,134 @@ __device__ __forceinline__ void dir4_back(const K4Rec &r, const Dir4 &d, const f
     bb = -0.5f * opa2b;
 }
 
+// Cotangents through the polarisation block and the amplitudes: g_bar, A_bar
+// and B_bar from the bin's cotangent G, and the amplitude sums.
+__device__ __forceinline__ void w_back(const K4Rec &r, const Bin4 &B, float2 g, float A, float Bm,
+                                       float2 *accA, float2 &gb, float &Ab, float &Bb) {
+    const float2 *u = reinterpret_cast<const float2 *>(r.amp);
+    // H conj(u) = Re(u) H + Im(u) (-i H)
+    const float2 Sp = fma2(bc2(u[0].x), B.G[0], fma2(bc2(u[0].y), B.Gm[0],
+                           fma2(bc2(u[2].x), B.G[2], mul2(bc2(u[2].y), B.Gm[2]))));
+    const float2 Sn = fma2(bc2(u[1].x), B.G[1], fma2(bc2(u[1].y), B.Gm[1],
+                           fma2(bc2(u[3].x), B.G[3], mul2(bc2(u[3].y), B.Gm[3]))));
+    const float2 Ss = add2(Sp, Sn), Sd = sub2(Sp, Sn);
+    gb = make_float2(fmaf(A, Ss.x, -Bm * Sd.y), fmaf(A, Ss.y, Bm * Sd.x));
+    Ab = fmaf(g.x, Ss.x, g.y * Ss.y);
+    Bb = fmaf(g.y, Sd.x, -g.x * Sd.y);
+    {
+        const float gyB = g.y * Bm, gyA = g.y * A;
+        // conj(g z+) and conj(g z-); H w = Re(w) H - Im(w) (-i H)
+        const float wpr = fmaf(g.x, A, gyB), wpi = fmaf(g.x, Bm, -gyA);
+        const float wnr = fmaf(g.x, A, -gyB), wni = fmaf(-g.x, Bm, -gyA);
+        accA[0] = fma2(bc2(wpr), B.G[0], fma2(bc2(-wpi), B.Gm[0], accA[0]));
+        accA[1] = fma2(bc2(wnr), B.G[1], fma2(bc2(-wni), B.Gm[1], accA[1]));
+        accA[2] = fma2(bc2(wpr), B.G[2], fma2(bc2(-wpi), B.Gm[2], accA[2]));
+        accA[3] = fma2(bc2(wnr), B.G[3], fma2(bc2(-wni), B.Gm[3], accA[3]));
+    }
+}
+
+// Cotangents of the phases t_j, the aperture wave vector and the bin direction,
+// given those of kx, ky, kz from the polarisation block (kxb, kyb, kzb).
+__device__ __forceinline__ void phase_back(const K4Rec &r, const Bin4 &B, const Dir4 &d, float2 g,
+                                           float2 dlo, float2 dhi, float2 gb, const float (&t)[3],
+                                           float kxx, float kyy, float kxb, float kyb, float kzb,
+                                           float k, float hkR, float iRf, float *acc, float2 *accP) {
+    // phases: t_j = ph + kxx xa_j + kyy ya_j.  t_bar = Re(conj(g_bar) dg/dt),
+    // assigned by rank (ties broken by index); phb = sum_j t_bar_j = Re(conj(g_bar) i g).
+    const float tlo = fmaf(gb.x, dlo.x, gb.y * dlo.y), thi = fmaf(gb.x, dhi.x, gb.y * dhi.y);
+    const float phb = fmaf(gb.y, g.x, -gb.x * g.y);
+    const float tmid = phb - tlo - thi;
+    // rank 0 (lowest) / 2 (highest) of each t_j, ties broken by index
+    const bool c01 = t[1] < t[0], c02 = t[2] < t[0], c12 = t[2] < t[1];
+    const bool is_lo[3] = {!c01 && !c02, c01 && !c12, c02 && c12};
+    const bool is_hi[3] = {c01 && c02, !c01 && c12, !c02 && !c12};
+    float kxxb = 0.0f, kyyb = 0.0f;
+    const float2 kk2 = make_float2(kxx, kyy);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const float tb = is_lo[j] ? tlo : (is_hi[j] ? thi : tmid);
+        kxxb = fmaf(tb, r.xa[j], kxxb);
+        kyyb = fmaf(tb, r.ya[j], kyyb);
+        accP[P_TK + j] = fma2(bc2(tb), kk2, accP[P_TK + j]);
+    }
+    // kxx = k p2x - k kx ; kyy = k p2y - k ky
+    kxb = fmaf(-k, kxxb, kxb);
+    kyb = fmaf(-k, kyyb, kyb);
+    acc[A_P2 + 0] += kxxb;  // times k after the loop
+    acc[A_P2 + 1] += kyyb;
+    const float kb3[3] = {kxb, kyb, kzb};
+    float ab, bb;
+    dir4_back(r, d, kb3, B.fx, B.fy, B.fz, acc, accP, ab, bb);
+    // ph = hkR (b - a^2)(1 + a) - rf with rf = k u.c (mod 2 pi), a = u.c/R, b = |c|^2/R^2:
+    // c_bar = (ab + phb dph/da) u / R - phb k u + (bb + phb dph/db) 2 c / R^2
+    const float dpa = hkR * fmaf(-2.0f * d.a, d.opa, fmaf(-d.a, d.a, r.b));
+    const float dpb = hkR * d.opa;
+    const float cu = fmaf(fmaf(phb, dpa, ab), iRf, -k * phb);
+    acc[A_CU + 0] = fmaf(cu, B.fx, acc[A_CU + 0]);
+    acc[A_CU + 1] = fmaf(cu, B.fy, acc[A_CU + 1]);
+    acc[A_CU + 2] = fmaf(cu, B.fz, acc[A_CU + 2]);
+    acc[A_CE] += fmaf(phb, dpb, bb);
+}
+
+// The bin step outside the clamps and the forward bodge (a bin away from the
+// poles, |ky| <= 0.999999 and kx^2 + kz^2 above the floor): the general step
+// below with kyc = ky, tt = kx^2 + kz^2 and q = k, its branches left out.
+__device__ __forceinline__ void k4_main(const K4Rec &r, const Bin4 &B, const Dir4 &d, float kx,
+                                        float ky, float kz, float kxx, float kyy,
+                                        const float (&t)[3], float tt, float k, float hkR,
+                                        float iRf, float *acc, float2 *accA, float2 *accP) {
+    float2 g, dlo, dhi;
+    dd_grad_main(t[0], t[1], t[2], g, dlo, dhi);
+    const float rs = rsqrt4(tt), s = tt * rs;
+    const float kyrs = ky * rs;
+    const float e = rs * r.hicf, kxky = kx * ky;
+    const float dd = fmaf(r.kw1, s, -kz * e);
+    const float ee = fmaf(r.kw2, s, -kxky * e);
+    const float hr[3] = {fmaf(r.inc[1], kz, -r.inc[2] * ky), fmaf(r.inc[2], kx, -r.inc[0] * kz),
+                         fmaf(r.inc[0], ky, -r.inc[1] * kx)};
+    const float hn = rsqrt4(fmaf(hr[2], hr[2], fmaf(hr[1], hr[1], hr[0] * hr[0])));
+    const float T1 = fmaf(hr[0], kx, hr[2] * kz);
+    const float P0 = fmaf(hr[1], s, -kyrs * T1);
+    const float R0 = fmaf(hr[2], kx, -hr[0] * kz);
+    const float pp = hn * P0, rr = hn * rs * R0;
+    const float A = fmaf(pp, dd, rr * ee), Bm = fmaf(pp, ee, -rr * dd);
+    float2 gb;
+    float Ab, Bb;
+    w_back(r, B, g, A, Bm, accA, gb, Ab, Bb);
+    const float ppb = fmaf(Ab, dd, Bb * ee), rrb = fmaf(Ab, ee, -Bb * dd);
+    const float ddb = fmaf(Ab, pp, -Bb * rr), eeb = fmaf(Ab, rr, Bb * pp);
+    const float Pb = ppb * hn, Rb = rrb * hn * rs;
+    const float hn3 = -fmaf(ppb, P0, rrb * rs * R0) * hn * hn * hn;
+    const float T1b = -Pb * kyrs;
+    const float hrb[3] = {fmaf(T1b, kx, fmaf(-Rb, kz, hn3 * hr[0])), fmaf(Pb, s, hn3 * hr[1]),
+                          fmaf(T1b, kz, fmaf(Rb, kx, hn3 * hr[2]))};
+    float kxb = fmaf(T1b, hr[0], Rb * hr[2]);
+    float kzb = fmaf(T1b, hr[2], -Rb * hr[0]);
+    float kyb = -Pb * rs * T1;
+    const float sbm = fmaf(Pb, fmaf(ky * T1, rs * rs, hr[1]), -Rb * R0 * rs);
+    // h = inc x k
+    kxb += hrb[1] * r.inc[2] - hrb[2] * r.inc[1];
+    kyb += hrb[2] * r.inc[0] - hrb[0] * r.inc[2];
+    kzb += hrb[0] * r.inc[1] - hrb[1] * r.inc[0];
+    acc[A_INC + 0] += ky * hrb[2] - kz * hrb[1];
+    acc[A_INC + 1] += kz * hrb[0] - kx * hrb[2];
+    acc[A_INC + 2] += kx * hrb[1] - ky * hrb[0];
+    // Karczewski-Wolf dd, ee (see k4_eval)
+    const float dde = ddb * e, eee = eeb * e;
+    kxb = fmaf(-eee, ky, kxb);
+    kyb = fmaf(-eee, kx, kyb);
+    kzb -= dde;
+    const float X = fmaf(dde, kz, eee * kxky);
+    const float sb = sbm + fmaf(ddb, r.kw1, fmaf(eeb, r.kw2, rs * X));
+    acc[A_P2 + 2] = fmaf(ddb, s, acc[A_P2 + 2]);
+    accP[P_KW].x = fmaf(eeb, s, accP[P_KW].x);
+    accP[P_KW].y += X;
+    const float ttb = 0.5f * sb * rs;  // s = sqrt(tt)
+    kxb = fmaf(2.0f * kx, ttb, kxb);
+    kzb = fmaf(2.0f * kz, ttb, kzb);
+    phase_back(r, B, d, g, dlo, dhi, gb, t, kxx, kyy, kxb, kyb, kzb, k, hkR, iRf, acc, accP);
+}
+
 // Cotangent contributions of one (record, bin).
 template <bool FAST>
 __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, float hkR, float iRf,
@@ -262,6 +441,13 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     const float kxx = fmaf(-k, kx, r.kp[0]), kyy = fmaf(-k, ky, r.kp[1]);
     float t[3];
     for (int j = 0; j < 3; j++) t[j] = fmaf(kyy, r.ya[j], fmaf(kxx, r.xa[j], ph));
+    {
+        const float tr = fmaf(kx, kx, kz * kz);
+        if (!B.pole && tr > kClampSq4 && fabsf(ky) <= 0.999999f) {
+            k4_main(r, B, d, kx, ky, kz, kxx, kyy, t, tr, k, hkR, iRf, acc, accA, accP);
+            return;
+        }
+    }
     float2 g, dlo, dhi;
     dd_grad(t[0], t[1], t[2], g, dlo, dhi);
     const bool yclamp = !(fabsf(ky) <= 0.999999f);
@@ -326,26 +512,9 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
     //   g_bar = conj(z+) S+ + conj(z-) S- = A (S+ + S-) + i B (S+ - S-)
     //   A_bar = Re conj(g) (S+ + S-),  B_bar = Im conj(g) (S- - S+)
     //   u+-_j_bar = H+-_j conj(g z+-)
-    const float2 *u = reinterpret_cast<const float2 *>(r.amp);
-    // H conj(u) = Re(u) H + Im(u) (-i H)
-    const float2 Sp = fma2(bc2(u[0].x), B.G[0], fma2(bc2(u[0].y), B.Gm[0],
-                           fma2(bc2(u[2].x), B.G[2], mul2(bc2(u[2].y), B.Gm[2]))));
-    const float2 Sn = fma2(bc2(u[1].x), B.G[1], fma2(bc2(u[1].y), B.Gm[1],
-                           fma2(bc2(u[3].x), B.G[3], mul2(bc2(u[3].y), B.Gm[3]))));
-    const float2 Ss = add2(Sp, Sn), Sd = sub2(Sp, Sn);
-    const float2 gb = make_float2(fmaf(A, Ss.x, -Bm * Sd.y), fmaf(A, Ss.y, Bm * Sd.x));
-    const float Ab = fmaf(g.x, Ss.x, g.y * Ss.y);
-    const float Bb = fmaf(g.y, Sd.x, -g.x * Sd.y);
-    {
-        const float gyB = g.y * Bm, gyA = g.y * A;
-        // conj(g z+) and conj(g z-); H w = Re(w) H - Im(w) (-i H)
-        const float wpr = fmaf(g.x, A, gyB), wpi = fmaf(g.x, Bm, -gyA);
-        const float wnr = fmaf(g.x, A, -gyB), wni = fmaf(-g.x, Bm, -gyA);
-        accA[0] = fma2(bc2(wpr), B.G[0], fma2(bc2(-wpi), B.Gm[0], accA[0]));
-        accA[1] = fma2(bc2(wnr), B.G[1], fma2(bc2(-wni), B.Gm[1], accA[1]));
-        accA[2] = fma2(bc2(wpr), B.G[2], fma2(bc2(-wpi), B.Gm[2], accA[2]));
-        accA[3] = fma2(bc2(wnr), B.G[3], fma2(bc2(-wni), B.Gm[3], accA[3]));
-    }
+    float2 gb;
+    float Ab, Bb;
+    w_back(r, B, g, A, Bm, accA, gb, Ab, Bb);
     // A = pp dd + rr ee, B = pp ee - rr dd
     const float ppb = fmaf(Ab, dd, Bb * ee), rrb = fmaf(Ab, ee, -Bb * dd);
     const float ddb = fmaf(Ab, pp, -Bb * rr), eeb = fmaf(Ab, rr, Bb * pp);
@@ -430,41 +599,7 @@ __device__ __forceinline__ void k4_eval(const K4Rec &r, const Bin4 &B, float k, 
         kzb = fmaf(2.0f * kz, ttb, kzb);
     }
     float kyb = yclamp ? 0.0f : kycb;
-    // phases: t_j = ph + kxx xa_j + kyy ya_j.  t_bar = Re(conj(g_bar) dg/dt),
-    // assigned by rank (ties broken by index); phb = sum_j t_bar_j = Re(conj(g_bar) i g).
-    const float tlo = fmaf(gb.x, dlo.x, gb.y * dlo.y), thi = fmaf(gb.x, dhi.x, gb.y * dhi.y);
-    const float phb = fmaf(gb.y, g.x, -gb.x * g.y);
-    const float tmid = phb - tlo - thi;
-    // rank 0 (lowest) / 2 (highest) of each t_j, ties broken by index
-    const bool c01 = t[1] < t[0], c02 = t[2] < t[0], c12 = t[2] < t[1];
-    const bool is_lo[3] = {!c01 && !c02, c01 && !c12, c02 && c12};
-    const bool is_hi[3] = {c01 && c02, !c01 && c12, !c02 && !c12};
-    float kxxb = 0.0f, kyyb = 0.0f;
-    const float2 kk2 = make_float2(kxx, kyy);
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-        const float tb = is_lo[j] ? tlo : (is_hi[j] ? thi : tmid);
-        kxxb = fmaf(tb, r.xa[j], kxxb);
-        kyyb = fmaf(tb, r.ya[j], kyyb);
-        accP[P_TK + j] = fma2(bc2(tb), kk2, accP[P_TK + j]);
-    }
-    // kxx = k p2x - k kx ; kyy = k p2y - k ky
-    kxb = fmaf(-k, kxxb, kxb);
-    kyb = fmaf(-k, kyyb, kyb);
-    acc[A_P2 + 0] += kxxb;  // times k after the loop
-    acc[A_P2 + 1] += kyyb;
-    const float kb3[3] = {kxb, kyb, kzb};
-    float ab, bb;
-    dir4_back(r, d, kb3, B.fx, B.fy, B.fz, acc, accP, ab, bb);
-    // ph = hkR (b - a^2)(1 + a) - rf with rf = k u.c (mod 2 pi), a = u.c/R, b = |c|^2/R^2:
-    // c_bar = (ab + phb dph/da) u / R - phb k u + (bb + phb dph/db) 2 c / R^2
-    const float dpa = hkR * fmaf(-2.0f * d.a, d.opa, fmaf(-d.a, d.a, r.b));
-    const float dpb = hkR * d.opa;
-    const float cu = fmaf(fmaf(phb, dpa, ab), iRf, -k * phb);
-    acc[A_CU + 0] = fmaf(cu, B.fx, acc[A_CU + 0]);
-    acc[A_CU + 1] = fmaf(cu, B.fy, acc[A_CU + 1]);
-    acc[A_CU + 2] = fmaf(cu, B.fz, acc[A_CU + 2]);
-    acc[A_CE] += fmaf(phb, dpb, bb);
+    phase_back(r, B, d, g, dlo, dhi, gb, t, kxx, kyy, kxb, kyb, kzb, k, hkR, iRf, acc, accP);
 }
 
 // One warp per record, K4_WARPS records per CTA; blockIdx.y selects a range
