@@ -1031,9 +1031,11 @@ def main():
                         "issue_active": cj["issue_active"],
                         "fma_pipe_cycles_active": cj["fma_pipe_cycles_active"],
                         "thread_instructions_per_facet_bin": cj["thread_instructions_per_facet_bin"],
-                        "limiter": "instruction issue, then the FMA pipe; the convention's MUFU "
-                                   "term counts 20 special-function ops per facet-bin where the "
-                                   "kernel issues %.1f" % mi,
+                        "limiter": "the FMA pipe (%.0f %% of cycles; a packed FP32x2 instruction "
+                                   "holds it two cycles) and instruction issue (%.0f %%); the "
+                                   "convention's MUFU term counts 20 special-function ops per "
+                                   "facet-bin where the kernel issues %.1f"
+                                   % (100 * cj["fma_pipe_cycles_active"], 100 * cj["issue_active"], mi),
                         "source": "profiles/k2_main_pk_counters.json (ncu)"}
         except Exception:
             counters = None
