@@ -1093,7 +1093,10 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     }
 }
 
-constexpr int K2P_CH = 32;  // record pairs per shared-memory stage (64 records)
+// Record pairs per shared-memory stage: 44 for the full sum (three stages, 44 KB,
+// four CTAs per SM); 32 with the field-of-view cull, whose per-stage keep masks are
+// two 32-bit ballot words of the stage's 64 records.
+constexpr int K2P_CH_FULL = 44, K2P_CH_FOV = 32;
 
 // The record's per-bin test passes no bin of the tile when the angle between
 // prop0 and the tile centre exceeds fovm + psi (fovm includes the parallax
@@ -1129,7 +1132,8 @@ struct K2PkArgs {
 
 template <int BPT, bool FAST>
 __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kernel(K2PkArgs P) {
-    __shared__ __align__(128) K2Pair sbuf[K2_NST][K2P_CH];
+    constexpr int CH = FAST ? K2P_CH_FOV : K2P_CH_FULL;
+    __shared__ __align__(128) K2Pair sbuf[K2_NST][CH];
     __shared__ __align__(8) uint64_t bars[K2_NST];
     __shared__ long long s_item;
     __shared__ unsigned s_keep[2];  // is_fast_diff: records of the stage not culled for the tile
@@ -1206,12 +1210,12 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
         // record pairs [p0, p1) cover records [rbeg, rend)
         const int64_t p0 = rbeg >> 1, p1 = (rend + 1) >> 1;
         const int64_t npair = p1 - p0;
-        const int64_t nchunk = (npair + K2P_CH - 1) / K2P_CH;
+        const int64_t nchunk = (npair + CH - 1) / CH;
         if (tid == 0) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             for (int64_t c = 0; c < nchunk && c < K2_NST; c++) {
-                const int64_t n = min((int64_t)K2P_CH, npair - c * K2P_CH);
-                bulk_load(smem_u32(&sbuf[c][0]), P.pairs + p0 + c * K2P_CH,
+                const int64_t n = min((int64_t)CH, npair - c * CH);
+                bulk_load(smem_u32(&sbuf[c][0]), P.pairs + p0 + c * CH,
                           (uint32_t)(n * sizeof(K2Pair)), smem_u32(&bars[c]));
             }
         }
@@ -1221,7 +1225,7 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
             const int st = (int)(c % K2_NST);
             const bool ok = mbar_wait(smem_u32(&bars[st]), (parity >> st) & 1u);
             parity ^= 1u << st;
-            const int n = (int)min((int64_t)K2P_CH, npair - c * K2P_CH);
+            const int n = (int)min((int64_t)CH, npair - c * CH);
             if (!FAST && ok && tid < 39) {
                 // The item's first pair (odd rbeg) and last pair (odd rend) hold a
                 // record of another item or the array's padding: that half takes a
@@ -1265,7 +1269,7 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
                 // tile adds nothing
                 if (tid < 64) {
                     const bool keep =
-                        tid < 2 * n && !cone_culled(P.fovs[2 * (p0 + c * K2P_CH) + tid], cone);
+                        tid < 2 * n && !cone_culled(P.fovs[2 * (p0 + c * CH) + tid], cone);
                     const unsigned m = __ballot_sync(0xffffffffu, keep);
                     if ((tid & 31) == 0) s_keep[tid >> 5] = m;
                 }
@@ -1273,7 +1277,7 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
             }
             auto pair_step = [&](int j) {
                 bool lo_ok = j != j_lo, hi_ok = j != j_hi;
-                const K2Fov *fv = FAST ? P.fovs + 2 * (p0 + c * K2P_CH + j) : nullptr;
+                const K2Fov *fv = FAST ? P.fovs + 2 * (p0 + c * CH + j) : nullptr;
                 if (FAST) {
                     const unsigned m = s_keep[j >> 4] >> (2 * (j & 15));
                     lo_ok = lo_ok && (m & 1u);
@@ -1317,8 +1321,8 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
             if (tid == 0 && c + K2_NST < nchunk) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 const int64_t c2 = c + K2_NST;
-                const int64_t n2 = min((int64_t)K2P_CH, npair - c2 * K2P_CH);
-                bulk_load(smem_u32(&sbuf[st][0]), P.pairs + p0 + c2 * K2P_CH,
+                const int64_t n2 = min((int64_t)CH, npair - c2 * CH);
+                bulk_load(smem_u32(&sbuf[st][0]), P.pairs + p0 + c2 * CH,
                           (uint32_t)(n2 * sizeof(K2Pair)), smem_u32(&bars[st]));
             }
         }
