@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-tune", action="store_true",
-                    help="keep the default launch plan instead of tuning it on a 20,000-facet sample")
+                    help="keep the default launch plan instead of tuning it on the step's facet list")
     ap.add_argument("--no-graph", action="store_true",
                     help="enqueue each step through the C ABI instead of replaying a CUDA graph")
     ap.add_argument("--orient", type=int, default=1024,
@@ -387,6 +387,8 @@ def config5(ctx, args):
     nout, per_orient, kept = [], [], None
     ctx.set_kernel_timing(True)
     ctx.kernel_time_ms()
+    clocks = ClockSampler(ctx.device)
+    clocks.start()
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=1) as ex:
         starts = list(range(0, n, chunk))
@@ -401,6 +403,7 @@ def config5(ctx, args):
             if c == 0:
                 kept = (Vs, beams, exts, pins)
     t_all = time.perf_counter() - t0
+    clk = clocks.stop()
     k_ms, k_n = ctx.kernel_time_ms()
     ctx.set_kernel_timing(False)
     F = np.array(nout, dtype=np.float64)
@@ -413,7 +416,7 @@ def config5(ctx, args):
     r64 = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pins, precision="fp64")
     t64 = time.perf_counter() - t0
     sms = torch_sm_count()
-    hz = 1965.0e6
+    hz = (clk.get("sm_mhz") or 1965.0) * 1e6
     kern_s = k_ms / 1e3
     return {"workload": "smooth hexagonal column r 50 um, L 100 um, 2 um^2 triangles (22,500, "
                         "8 apertures), n = 1.31 + 0.01i, beam lists traced on the host (rec 8), "
@@ -426,7 +429,9 @@ def config5(ctx, args):
             "mufu_term_frac": W_SFU * work / kern_s / (sms * SFU_PER_SM_CLK * hz),
             "fp32_term_frac": W_FP32 * work / kern_s / (sms * FP32_PER_SM_CLK * hz),
             "roofline_basis": "convention per triangle facet-bin (20 MUFU, 170 FP32 flops) over "
-                              "the summed kernel time; %d SMs x 1965 MHz" % sms,
+                              "the summed kernel time; %d SMs x %.0f MHz (median sampled SM "
+                              "clock of the loop)" % (sms, hz / 1e6),
+            "clocks": clk,
             "error_subset_orientations": m, "fp64_dropin_subset_s": t64,
             "fp64_dropin_orientations_per_s": m / t64,
             "speedup_fp32_vs_fp64_dropin": (n / t_all) / (m / t64),
@@ -804,12 +809,14 @@ def main():
         diff_batch_dev(ctx, stream.cuda_stream, 1, d_beam, boff, d_ext, eoff, d_verts, nverts,
                        geo["face_off"], d_fvi, th, ph, LAM, d_pin, d_mu, d_m1, d_pav, d_pper)
 
-    # launch plan (variant x bins per thread x records per item) tuned on a sample
+    # launch plan (variant x bins per thread x records per item) tuned on the step's
+    # own facet list (a smaller sample has fewer facet splits per bin tile, which
+    # favours smaller work items than the full list wants)
     plan = {"plan": "default (1, 1, 2048)"}
     if not args.no_tune:
         from abt_b200.tune import tune
-        best, times = tune(ctx, beam, geo, th, ph, LAM, sample_facets=20000)
-        plan = {"plan": list(best), "candidates_kernel_ms_20000_facets":
+        best, times = tune(ctx, beam, geo, th, ph, LAM, sample_facets=len(beam), repeats=1)
+        plan = {"plan": list(best), "candidates_kernel_ms_%d_facets" % len(beam):
                 {"%d,%d,%d" % k: round(v, 3) for k, v in times.items()}}
 
     # the step: one replay of the batch captured as a CUDA graph (the capture
