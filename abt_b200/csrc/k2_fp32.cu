@@ -168,8 +168,8 @@ __global__ void k2_setup_kernel(RefSrc S, int64_t nrefs, const double *__restric
                                 const int64_t *__restrict__ face_vi, const int64_t *__restrict__ start,
                                 double waveno, double lambda, int fast_diff,
                                 K2Rec *__restrict__ recs, K2Pair *__restrict__ pairs,
-                                K2Fov *__restrict__ fovs, int *__restrict__ err,
-                                unsigned *__restrict__ epsmax) {
+                                K2Fov *__restrict__ fovs, float2 *__restrict__ rlo,
+                                int *__restrict__ err, unsigned *__restrict__ epsmax) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= nrefs) return;
     int64_t o;
@@ -233,6 +233,15 @@ __global__ void k2_setup_kernel(RefSrc S, int64_t nrefs, const double *__restric
         }
         rec.b = (float)((com[0] * com[0] + com[1] * com[1] + com[2] * com[2]) / (R * R));
         for (int q = 0; q < 9; q++) rec.R[q] = (float)fr.R.m[q / 3][q % 3];
+        for (int i = 0; i < 3; i++) {
+            // the low part of the y row, read only by lanes on the ky clamp
+            float2 &l = rlo[((r0 + t) >> 1) * 3 + i];
+            const float lo = (float)(fr.R.m[1][i] - (double)rec.R[3 + i]);
+            if ((r0 + t) & 1)
+                l.y = lo;
+            else
+                l.x = lo;
+        }
         rec.kp[0] = (float)(waveno * fr.prop2[0]);
         rec.kp[1] = (float)(waveno * fr.prop2[1]);
         rec.hkz_cf = (float)(-0.5 * fr.prop2[2] * cf);
@@ -464,6 +473,7 @@ __device__ __forceinline__ void ordered_add(double *__restrict__ out, int64_t nb
 struct K2MainArgs {
     const K2Rec *recs;
     const K2Fov *fovs;
+    const float2 *rlo;  // R_1 - (float)R_1, pair layout (3 per pair)
     const int64_t *seg_rec;
     const int64_t *item_pre;
     int64_t nseg;
@@ -481,11 +491,23 @@ struct K2MainArgs {
     int *err;
 };
 
+// For a lane on the ky clamp: one component of v = u - sigma R_1, sigma the sign of
+// ky and R_1 the aperture frame's y axis (rounded row hi, low part lo), formed from
+// the FP64 bin direction.  On the clamp the reference divides kx and kz by
+// s = sqrt(1 - 0.999999^2) = 1.4e-3 (m = (-kx ky / s, s, -kz ky / s),
+// src/diff_mod.f90:151-158); formed in FP32 from u they are differences of O(1)
+// terms with an absolute error near 1e-7, which that division makes 1e-4.  With
+// R_0 . R_1 = 0, kx = R_0 . v opa2 + nea_0 opa and kz = R_2 . v opa2 + nea_2 opa,
+// where v is small and known to FP32 precision (absolute error near 1e-10).
+__device__ __forceinline__ float clamp_v(float hi, float lo, double u, float sigma) {
+    return fmaf(-sigma, lo, (float)fma(-(double)sigma, (double)hi, u));
+}
+
 template <int BPT, bool FAST>
 __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const BinDev (&bd)[BPT],
                                           const bool (&valid)[BPT], float (&acc)[BPT][8], float k,
                                           float hkR, float sgh, const double *__restrict__ xyz,
-                                          int64_t nb) {
+                                          int64_t nb, const float2 *__restrict__ rl, int half) {
     const double kc0 = r.kc[0], kc1 = r.kc[1], kc2 = r.kc[2];
 #pragma unroll
     for (int q = 0; q < BPT; q++) {
@@ -537,17 +559,27 @@ __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const
         // cancellation near |ky| = 1); the floor is the reference's clamp
         // |ky| <= 0.999999 (src/diff_mod.f90:151).
         const float kyc = fminf(fmaxf(ky, -0.999999f), 0.999999f);
-        const float tt = fmaxf(fmaf(kx, kx, kz * kz), kOneMinusClampSq);
+        const float tr = fmaf(kx, kx, kz * kz);
+        float kxv = kx, kzv = kz;  // kx, kz of the polarisation block
+        if (tr <= kOneMinusClampSq) {
+            auto lo = [&](int i) { return half ? rl[i].y : rl[i].x; };
+            const float sig = ky < 0.0f ? -1.0f : 1.0f;
+            const float v0 = clamp_v(r.R[3], lo(0), B.ux, sig), v1 = clamp_v(r.R[4], lo(1), B.uy, sig),
+                        v2 = clamp_v(r.R[5], lo(2), B.uz, sig);
+            kxv = fmaf(fmaf(r.R[2], v2, fmaf(r.R[1], v1, r.R[0] * v0)), opa2, -r.ea[0] * opa);
+            kzv = fmaf(fmaf(r.R[8], v2, fmaf(r.R[7], v1, r.R[6] * v0)), opa2, -r.ea[2] * opa);
+        }
+        const float tt = fmaxf(tr, kOneMinusClampSq);
         const float rs = rsqrtf(tt);
         const float s = tt * rs;
         const float kyrs = kyc * rs;
-        const float m0 = -kx * kyrs, m1 = s, m2 = -kz * kyrs;
-        const float d = fmaf(r.hkz_cf, s, -(kz * rs) * r.hicf);
-        const float e = fmaf(r.hkxky_cf, s, -(kx * kyrs) * r.hicf);
+        const float m0 = -kxv * kyrs, m1 = s, m2 = -kzv * kyrs;
+        const float d = fmaf(r.hkz_cf, s, -(kzv * rs) * r.hicf);
+        const float e = fmaf(r.hkxky_cf, s, -(kxv * kyrs) * r.hicf);
         // vector perpendicular to the scattering plane (forward bodge near the poles)
         // h = inc x (kx, kyc, kz) = inc x (ks0, ks1 + kyc - ky, ks2)
         float qx = ks0, qy = ks1 + (kyc - ky), qz = ks2;
-        const float dinc = fmaf(r.inc[2], kz, fmaf(r.inc[1], kyc, r.inc[0] * kx));
+        const float dinc = fmaf(r.inc[2], kzv, fmaf(r.inc[1], kyc, r.inc[0] * kxv));
         if (!(fabsf(dinc) < 0.999f)) {
             // bodge direction in the s form: uh . eps = hs . eps - sgh eps_z
             const float ah = fmaf(-sgh, r.eps[2],
@@ -565,9 +597,9 @@ __device__ __forceinline__ void k2_record(const K2Rec &r, const K2Fov *fv, const
         hx *= hn;
         hy *= hn;
         hz *= hn;
-        float ex = fmaf(kyc, m2, -kz * m1);
-        float ey = fmaf(kz, m0, -kx * m2);
-        float ez = fmaf(kx, m1, -kyc * m0);
+        float ex = fmaf(kyc, m2, -kzv * m1);
+        float ey = fmaf(kzv, m0, -kxv * m2);
+        float ez = fmaf(kxv, m1, -kyc * m0);
         if (tt <= kOneMinusClampSq) {
             // inside the clamp cone k and m are not unit vectors and the
             // reference's normalisation of k x m (src/diff_mod.f90:637) matters
@@ -694,9 +726,11 @@ __global__ void __launch_bounds__(K2_THREADS, 2) k2_main_kernel(K2MainArgs P) {
 #pragma unroll
                 for (int cc = 0; cc < 8; cc++) acc[q][cc] = 0.0f;
             const K2Fov *fv = FAST ? P.fovs + rbeg + c * K2_CH : nullptr;
-            for (int j = 0; j < n; j++)
+            for (int j = 0; j < n; j++) {
+                const int64_t ri = rbeg + c * K2_CH + j;
                 k2_record<BPT, FAST>(sbuf[st][j], FAST ? fv + j : nullptr, bd, valid, acc, P.k,
-                                     P.hkR, P.sgh, P.xyz, P.nb);
+                                     P.hkR, P.sgh, P.xyz, P.nb, P.rlo + (ri >> 1) * 3, (int)(ri & 1));
+            }
 #pragma unroll
             for (int q = 0; q < BPT; q++)
 #pragma unroll
@@ -883,7 +917,8 @@ template <bool FAST>
 __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const BinPk &B,
                                         float2 (&acc)[8], float2 nkh, float2 hkRh, float2 sgh,
                                         const float (&hb)[3][K2P_HB], bool lo_ok, bool hi_ok,
-                                        const double *__restrict__ xyz, int64_t nb) {
+                                        const double *__restrict__ xyz, int64_t nb,
+                                        const float2 *__restrict__ rl) {
     // far-field half phase per facet: FP64 k u.c / 2, reduced mod pi
     float2 rf;
     {
@@ -936,9 +971,9 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     ld22(&P.kzc, kzc, inc0);
     ld22(&P.inc[1], inc1, inc2);
     const float2 so = mul2(B.sg, opa2);
-    const float2 kx = fma2(so, inc0, ks0);
+    float2 kx = fma2(so, inc0, ks0);
     const float2 ky = fma2(so, inc1, ks1);
-    const float2 kz = fma2(so, inc2, ks2);
+    float2 kz = fma2(so, inc2, ks2);
     // aperture wave vector (halved with the phases)
     float2 kxx, kyy;
     {
@@ -974,6 +1009,25 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     float2 P1 = hy, R1;
     const bool cx = tr.x <= kOneMinusClampSq, cy = tr.y <= kOneMinusClampSq;
     if (B.pole || cx || cy) {
+        if (cx || cy) {
+            // on the clamp: kx and kz from v = u - sigma R_1 (see clamp_v)
+            float2 a0, a1, a2, a3, a4, a5, c6, c7, c8, n0, n1, n2;
+            ld22(&P.R[0], a0, a1);
+            ld22(&P.R[2], a2, a3);
+            ld22(&P.R[4], a4, a5);
+            ld22(&P.R[6], c6, c7);
+            ld22(&P.R[8], c8, n0);
+            ld22(&P.nea[1], n1, n2);
+            const float2 l0 = rl[0], l1 = rl[1], l2 = rl[2];
+            const float sx = ky.x < 0.0f ? -1.0f : 1.0f, sy = ky.y < 0.0f ? -1.0f : 1.0f;
+            const float2 v0 = make_float2(clamp_v(a3.x, l0.x, B.ux, sx), clamp_v(a3.y, l0.y, B.ux, sy));
+            const float2 v1 = make_float2(clamp_v(a4.x, l1.x, B.uy, sx), clamp_v(a4.y, l1.y, B.uy, sy));
+            const float2 v2 = make_float2(clamp_v(a5.x, l2.x, B.uz, sx), clamp_v(a5.y, l2.y, B.uz, sy));
+            const float2 kxa = fma2(fma2(a2, v2, fma2(a1, v1, mul2(a0, v0))), opa2, mul2(n0, opa));
+            const float2 kza = fma2(fma2(c8, v2, fma2(c7, v1, mul2(c6, v0))), opa2, mul2(n2, opa));
+            kx = sel2(cx, cy, kxa, kx);
+            kz = sel2(cx, cy, kza, kz);
+        }
         // near the poles (the forward bodge) or on the clamp: ky clamped to
         // +-0.999999 and tt to 1 - 0.999999^2 as in src/diff_mod.f90
         const float2 kyc = make_float2(fminf(fmaxf(ky.x, -0.999999f), 0.999999f),
@@ -1108,6 +1162,7 @@ __device__ __forceinline__ bool cone_culled(const K2Fov &f, const K2Cone &t) {
 }
 
 struct K2PkArgs {
+    const float2 *rlo;  // R_1 - (float)R_1, pair layout (3 per pair)
     const K2Pair *pairs;
     const K2Fov *fovs;
     const int *perm;        // is_fast_diff: tile-major bin order (-1: padding)
@@ -1290,7 +1345,8 @@ __global__ void __launch_bounds__(K2_THREADS, BPT == 1 ? 4 : 0) k2_main_pk_kerne
                 for (int q = 0; q < BPT; q++)
                     k2_pair<FAST>(sbuf[st][j], fv, bd[q], acc[q], nkh, hkRh, sgh, s_hb,
                                   FAST ? (lo_ok && valid[q]) : true,
-                                  FAST ? (hi_ok && valid[q]) : true, P.xyz, P.nb);
+                                  FAST ? (hi_ok && valid[q]) : true, P.xyz, P.nb,
+                                  P.rlo + (p0 + c * CH + j) * 3);
             };
             if (FAST) {
                 // visit only the pairs with a record the tile cull kept: bit j of pm
@@ -1637,6 +1693,7 @@ struct K2Setup {
     K2Rec *recs = nullptr;
     K2Pair *pairs = nullptr;
     K2Fov *fovs = nullptr;
+    float2 *rlo = nullptr;  // R_1 - (float)R_1 per record (the y row), pair layout (3 per pair)
     int64_t *start = nullptr;
     int64_t *refbase = nullptr;
     int64_t *beam_off = nullptr;
@@ -1678,10 +1735,12 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
     // records (or record pairs; an even count so the last pair is whole)
     const int64_t nrec2 = (max_recs + 1) & ~(int64_t)1;
     const size_t rec_bytes = variant ? (size_t)(nrec2 / 2) * sizeof(K2Pair) : (size_t)max_recs * sizeof(K2Rec);
-    PBT_TRY(ctx->d_rec.ensure(align_up(rec_bytes) + (fast_diff ? nrec2 * sizeof(K2Fov) : 0)));
+    const size_t fov_bytes = fast_diff ? align_up(nrec2 * sizeof(K2Fov)) : 0;
+    PBT_TRY(ctx->d_rec.ensure(align_up(rec_bytes) + fov_bytes + (size_t)(nrec2 / 2) * 3 * sizeof(float2)));
     S.recs = variant ? nullptr : ctx->d_rec.as<K2Rec>();
     S.pairs = variant ? ctx->d_rec.as<K2Pair>() : nullptr;
     S.fovs = fast_diff ? (K2Fov *)(ctx->d_rec.as<char>() + align_up(rec_bytes)) : nullptr;
+    S.rlo = (float2 *)(ctx->d_rec.as<char>() + align_up(rec_bytes) + fov_bytes);
     // host-side offsets -> device (pinned staging; the previous call's copy
     // out of the staging buffer must have run before it is overwritten)
     if (ctx->stage_pending && !ctx->capturing) {
@@ -1706,6 +1765,8 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
         ctx->stage_pending = true;
     }
     PBT_CUDA_TRY(cudaMemsetAsync(S.err, 0, 16, st));  // error flags and epsmax
+    // rotation low parts: zero in a pair's unused half (an odd record count)
+    PBT_CUDA_TRY(cudaMemsetAsync(S.rlo, 0, (size_t)(nrec2 / 2) * 3 * sizeof(float2), st));
     RefSrc src{d_beam, d_ext, S.beam_off, S.ext_off, S.refbase, norient};
     const int th = 256;
     k2_count_kernel<<<(unsigned)((nrefs + 1 + th - 1) / th), th, 0, st>>>(src, nrefs, d_face_off,
@@ -1715,7 +1776,7 @@ int k2_prepare(pbt_ctx *ctx, cudaStream_t st, int64_t norient, const pbt_outbeam
     if (nrefs > 0)
         k2_setup_kernel<<<(unsigned)((nrefs + th - 1) / th), th, 0, st>>>(
             src, nrefs, d_verts, nverts, d_face_off, d_face_vi, S.start, waveno, lambda, fast_diff,
-            S.recs, S.pairs, S.fovs, S.err, S.epsmax);
+            S.recs, S.pairs, S.fovs, S.rlo, S.err, S.epsmax);
     ctx->launches += 3;
     PBT_CUDA_TRY(cudaGetLastError());
     return PBT_OK;
@@ -1863,6 +1924,7 @@ int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, in
     K2MainArgs A;
     A.recs = S.recs;
     A.fovs = S.fovs;
+    A.rlo = S.rlo;
     A.seg_rec = seg_rec;
     A.item_pre = item_pre;
     A.nseg = 2 * no;
@@ -1882,6 +1944,7 @@ int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, in
     if (plan.variant == 1) {
         K2PkArgs B;
         B.pairs = S.pairs;
+        B.rlo = S.rlo;
         B.fovs = S.fovs;
         B.perm = cull ? g.fast_perm.as<int>() : nullptr;
         B.cones = cull ? g.fast_cone.as<K2Cone>() : nullptr;

@@ -253,6 +253,45 @@ def test_fp32_poles_and_bodge_row_hemispheres(ctx, plan, theta_deg):
     assert mueller_rel_err(_mueller(afb, afe), _mueller(rfb, rfe)) <= TOL_MU
 
 
+@pytest.mark.parametrize("plan", [(-1, 1, 2048), (0, 1, 2048)], ids=["packed", "one-record"])
+def test_fp32_clamp_lanes(ctx, plan):
+    """Bins on the reference's clamp |ky| <= 0.999999 (src/diff_mod.f90:151):
+    a triangle in the z = 0 plane with beams along (0, +-1, -1)/sqrt(2) has its
+    aperture frame's y axis along +-x (x lies along the beam's projection on the
+    plane), so the 15 bins within 0.08 deg of theta = 90 deg, phi = 0 or 180 deg
+    have |ky| above the clamp (the kernels' rare branch, with kx^2 + kz^2 on its
+    floor), next to bins just outside it.  There the reference divides kx and kz
+    (below 1.4e-3) by s = 1.4e-3; formed from the bin direction in FP32 they
+    carried an absolute error near 1e-7, and each clamp bin's Mueller elements
+    were off by up to 5.8 times its M11 (1.9e-4 over the bins above 1e-6 of the
+    peak).  The kernels form them from v = u - sigma R_1 instead: every bin within
+    1e-4 of its M11, and the amplitudes normwise within 1e-4."""
+    rng = np.random.default_rng(31)
+    th = abt_b200.make_angles([89.8, 90.2], [0.05])
+    ph = np.radians(np.concatenate([np.arange(0.0, 0.31, 0.05), np.arange(179.7, 180.31, 0.05)]))
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    on_clamp = (np.abs(np.sin(T) * np.cos(P)) > 0.999999).T  # (phi, theta)
+    assert on_clamp.sum() == 15
+    geo = one_triangle(scale=2.0)
+    beam = outbeams(4, rng, 1)
+    s = 1.0 / np.sqrt(2.0)
+    beam["prop_out"] = [(0, s, -s), (0, -s, -s), (0, s, -s), (0, -s, -s)]
+    beam["vk7"] = [(1, 0, 0), (1, 0, 0), (-1, 0, 0), (-1, 0, 0)]
+    ext = beam[:0]
+    ctx.set_plan(*plan)
+    try:
+        afb, afe = ctx.diff_main(beam, ext, geo, th, ph, LAM, precision="fp32")
+    finally:
+        ctx.set_plan()
+    rfb, rfe = ctx.diff_main(beam, ext, geo, th, ph, LAM, precision="fp64")
+    assert np.isfinite(afb).all()
+    assert rel_err(afb, rfb) <= 1e-4
+    m32, m64 = _mueller(afb, afe), _mueller(rfb, rfe)
+    assert mueller_rel_err(m32, m64) <= TOL_MU
+    per_bin = np.abs(m32 - m64).max(axis=-1) / m64[..., 0]
+    assert per_bin[on_clamp].max() <= TOL_MU
+
+
 def test_fp32_precision_study_grid_100k_facets(ctx):
     """The precision-study grid at full size (721 theta x 360 phi, 259,560 bins)
     with half of its list (100,000 synthetic facets in a 100 um cube, phases up to
