@@ -371,32 +371,34 @@ __device__ __forceinline__ void k4_main(const K4Rec &r, const Bin4 &B, const Dir
     float2 g, dlo, dhi;
     dd_grad_main(t[0], t[1], t[2], g, dlo, dhi);
     const float rs = rsqrt4(tt), s = tt * rs;
-    const float kyrs = ky * rs;
     const float e = rs * r.hicf, kxky = kx * ky;
     const float dd = fmaf(r.kw1, s, -kz * e);
     const float ee = fmaf(r.kw2, s, -kxky * e);
     const float hr[3] = {fmaf(r.inc[1], kz, -r.inc[2] * ky), fmaf(r.inc[2], kx, -r.inc[0] * kz),
                          fmaf(r.inc[0], ky, -r.inc[1] * kx)};
     const float hn = rsqrt4(fmaf(hr[2], hr[2], fmaf(hr[1], hr[1], hr[0] * hr[0])));
-    const float T1 = fmaf(hr[0], kx, hr[2] * kz);
-    const float P0 = fmaf(hr[1], s, -kyrs * T1);
+    // hr is normal to k and |k| = 1 to third order in |c|/R, so the general
+    // p = hn (hr1 s - (ky/s) hr . (kx, 0, kz)) is hn hr1 / s, the forward kernel's
+    // form; rr = hn (hr2 kx - hr0 kz) / s.
+    const float f = hn * rs;
     const float R0 = fmaf(hr[2], kx, -hr[0] * kz);
-    const float pp = hn * P0, rr = hn * rs * R0;
+    const float pp = f * hr[1], rr = f * R0;
     const float A = fmaf(pp, dd, rr * ee), Bm = fmaf(pp, ee, -rr * dd);
     float2 gb;
     float Ab, Bb;
     w_back(r, B, g, A, Bm, accA, gb, Ab, Bb);
     const float ppb = fmaf(Ab, dd, Bb * ee), rrb = fmaf(Ab, ee, -Bb * dd);
     const float ddb = fmaf(Ab, pp, -Bb * rr), eeb = fmaf(Ab, rr, Bb * pp);
-    const float Pb = ppb * hn, Rb = rrb * hn * rs;
-    const float hn3 = -fmaf(ppb, P0, rrb * rs * R0) * hn * hn * hn;
-    const float T1b = -Pb * kyrs;
-    const float hrb[3] = {fmaf(T1b, kx, fmaf(-Rb, kz, hn3 * hr[0])), fmaf(Pb, s, hn3 * hr[1]),
-                          fmaf(T1b, kz, fmaf(Rb, kx, hn3 * hr[2]))};
-    float kxb = fmaf(T1b, hr[0], Rb * hr[2]);
-    float kzb = fmaf(T1b, hr[2], -Rb * hr[0]);
-    float kyb = -Pb * rs * T1;
-    const float sbm = fmaf(Pb, fmaf(ky * T1, rs * rs, hr[1]), -Rb * R0 * rs);
+    // f = hn rs: f_bar = pp_bar hr1 + rr_bar R0; hn_bar = f_bar rs, rs_bar = f_bar hn
+    const float fb = fmaf(ppb, hr[1], rrb * R0);
+    const float R0b = rrb * f;
+    const float hn3 = -(fb * rs) * (hn * hn * hn);  // d hn / d hr_i = -hn^3 hr_i
+    const float hrb[3] = {fmaf(-R0b, kz, hn3 * hr[0]), fmaf(ppb, f, hn3 * hr[1]),
+                          fmaf(R0b, kx, hn3 * hr[2])};
+    float kxb = R0b * hr[2];
+    float kzb = -R0b * hr[0];
+    float kyb = 0.0f;
+    const float sbm = -(fb * hn) * (rs * rs);  // rs = 1/s
     // h = inc x k
     kxb += hrb[1] * r.inc[2] - hrb[2] * r.inc[1];
     kyb += hrb[2] * r.inc[0] - hrb[0] * r.inc[2];
