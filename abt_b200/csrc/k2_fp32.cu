@@ -1673,6 +1673,7 @@ K2Plan k2_plan_for(const pbt_ctx *ctx) {
         p.variant = ctx->plan_variant;
         p.bpt = ctx->plan_bpt;
         p.rpi = ctx->plan_rpi;
+        p.auto_rpi = false;
         return p;
     }
     if (const char *e = getenv("PBT_K2_PLAN")) {
@@ -1683,6 +1684,7 @@ K2Plan k2_plan_for(const pbt_ctx *ctx) {
             p.variant = v;
             p.bpt = b;
             p.rpi = r;
+            p.auto_rpi = false;
         }
     }
     return p;
@@ -1900,9 +1902,22 @@ int k2_fast_tiles(pbt_ctx *ctx, cudaStream_t st, int64_t tile) {
     return PBT_OK;
 }
 
+// Records per work item of the default plan: about eight items per resident CTA
+// (four per SM) for the call's records and bin tiles, in multiples of 64, between
+// 256 and 2,048.  Fewer, larger items cost less per item on large lists; on small
+// grids larger items leave the SMs short of work at the end of the launch (a
+// 31,000-outbeam orientation on 16,290 bins: 2.95 ms at 1,024 records per item,
+// 3.56 ms at 4,096).
+int64_t k2_auto_rpi(int64_t nrec, int64_t ntiles, int nsm) {
+    const int64_t want = (int64_t)8 * 4 * std::max(nsm, 1);
+    int64_t r = nrec * ntiles / want;
+    r = (r / 64) * 64;
+    return std::min<int64_t>(2048, std::max<int64_t>(256, r));
+}
+
 int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, int64_t no,
-                 double lambda, int fast_diff, const K2Plan &plan, double *ws, int64_t *seg_rec,
-                 int64_t *item_pre, unsigned long long *counter) {
+                 int64_t nrefs, double lambda, int fast_diff, K2Plan plan, double *ws,
+                 int64_t *seg_rec, int64_t *item_pre, unsigned long long *counter) {
     pbt::NvtxRange nvtx_("pbt: far-field sum (FP32)");
     const GridCache &g = ctx->grid;
     const int64_t tile = (int64_t)K2_THREADS * plan.bpt;
@@ -1912,6 +1927,7 @@ int k2_run_chunk(pbt_ctx *ctx, cudaStream_t st, const K2Setup &S, int64_t o0, in
         PBT_TRY(k2_fast_tiles(ctx, st, tile));
         ntiles = g.fast_ntiles;
     }
+    if (plan.auto_rpi) plan.rpi = k2_auto_rpi(nrefs, ntiles, ctx->sm_count);
     k2_plan_kernel<<<1, 32, 0, st>>>(S.start, S.refbase, S.beam_off, o0, no, plan.rpi, ntiles,
                                      seg_rec, item_pre, counter);
     ctx->launches++;
@@ -2100,7 +2116,9 @@ int k2_batch_add(pbt_ctx *ctx, cudaStream_t st, K2Batch &B, int64_t o0, int64_t 
     const unsigned egrid = (unsigned)((nb + eb - 1) / eb);
     for (int64_t l0 = 0; l0 < no; l0 += B.wchunk) {
         const int64_t n = std::min(B.wchunk, no - l0);
-        PBT_TRY(k2_run_chunk(ctx, st, S, l0, n, lambda, fast_diff, B.plan, B.ws, B.seg_rec,
+        const int64_t nrefs =
+            (h_beam_off[l0 + n] - h_beam_off[l0]) + (h_ext_off[l0 + n] - h_ext_off[l0]);
+        PBT_TRY(k2_run_chunk(ctx, st, S, l0, n, nrefs, lambda, fast_diff, B.plan, B.ws, B.seg_rec,
                              B.item_pre, B.counter));
         const int64_t og = o0 + l0;  // global orientation of the workspace's first slot
         pbt::NvtxRange nvtx_epi("pbt: epilogue (Mueller, orientation sums)");
@@ -2181,8 +2199,9 @@ int k2_diff_main_impl(pbt_ctx *ctx, cudaStream_t st, const pbt_outbeam *d_beam, 
     PBT_TRY(ctx->d_ws.ensure(o_end));
     char *base = ctx->d_ws.as<char>();
     double *ws = (double *)(base + o_ws);
-    PBT_TRY(k2_run_chunk(ctx, st, S, 0, 1, lambda, fast_diff, plan, ws, (int64_t *)(base + o_seg),
-                         (int64_t *)(base + o_it), (unsigned long long *)(base + o_cnt)));
+    PBT_TRY(k2_run_chunk(ctx, st, S, 0, 1, nbeam + next, lambda, fast_diff, plan, ws,
+                         (int64_t *)(base + o_seg), (int64_t *)(base + o_it),
+                         (unsigned long long *)(base + o_cnt)));
     const double waveno = 2.0 * kPiRef / lambda;
     k2_ampl_out_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, st>>>(
         ws, nb, (int64_t)g.phi.size(), g.phitab.as<double>(), g.xyz.as<double>(), waveno, d_afb,

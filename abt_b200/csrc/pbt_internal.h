@@ -203,6 +203,7 @@ struct K2Plan {
     int variant = 1;   // 0: one record per step, 1: two records packed (FP32x2)
     int bpt = 1;       // bins per thread
     int64_t rpi = 2048;  // facet records per work item
+    bool auto_rpi = true;  // default plan: rpi sized per call from the records and bin tiles
 };
 struct K2Batch {
     int64_t norient = 0, wchunk = 1;

@@ -906,6 +906,9 @@ def main():
     e2e = {"value": world * work / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3,
            "api": "pbt_diff_batch_list_c (host pointers; inputs and Mueller outputs pinned)"}
+    # the tuned plan is the step's; the further workloads (other facet counts and
+    # grids) use the library's default, which sizes the work items per call
+    ctx.set_plan()
 
     # reference-exact FP64 drop-in rate on a facet sample
     if args.fp64_facets > 0 and solo:

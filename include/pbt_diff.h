@@ -273,7 +273,9 @@ int pbt_set_kernel_timing(pbt_ctx *ctx, int32_t enable);
 /* Launch plan of the FP32 far-field kernel on this context: variant 1 = packed
  * two-facet kernel, 0 = one facet per step; bins_per_thread 1 or 2;
  * records_per_item = facet records per work item (32 .. 2^22).  variant < 0
- * restores the default.  Chosen by the tuner (abt_b200/tune.py). */
+ * restores the default: the packed kernel, one bin per thread, and work items
+ * sized per call (about eight per resident CTA for the call's records and bin
+ * tiles, 256 to 2,048 records).  Chosen by the tuner (abt_b200/tune.py). */
 int pbt_set_plan(pbt_ctx *ctx, int32_t variant, int32_t bins_per_thread, int64_t records_per_item);
 
 /* Sum of the device durations (ms) of the far-field kernel launches timed
