@@ -66,6 +66,7 @@ constexpr double kLit1_1 = (double)1.1f;    // stretch factors, src/beam_loop_mo
 constexpr double kLit1em5 = (double)1e-5f;  // near-normal refraction, src/beam_loop_mod.f90:1040
 constexpr double kBeamZ = 1000.0;           // incident plane, src/input_mod.f90:2169
 constexpr int kBB = 4;                      // bucket grid 4 x 4, src/beam_loop_mod.f90:2679-2680
+constexpr int64_t kGridFaces = 4096;          // meshes from this size use the cell grid of find_vis
 constexpr int64_t kMaxBeams = 20000000;     // guard against a runaway tree
 
 // ------------------------------------------------------------------ complex
@@ -441,12 +442,10 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
     // reference so that the threads of the loops below share this instance)
     thread_local std::vector<int> f3_tl, vb_tl;
     thread_local std::vector<Blocker> bl_tl;
-    thread_local std::vector<int64_t> members_tl[kBB * kBB];
     thread_local std::vector<char> is_vis_tl;
     thread_local std::vector<int64_t> map_tl;
     std::vector<int> &f3 = f3_tl, &vb = vb_tl;
     std::vector<Blocker> &bl = bl_tl;
-    std::vector<int64_t>(&members)[kBB * kBB] = members_tl;
     std::vector<char> &is_vis = is_vis_tl;
     std::vector<int64_t> &map = map_tl;  // face -> index in the beam's field list
     f3.resize(nf);
@@ -474,11 +473,72 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
         B.z = R.mid[3 * f + 2];
         B.up = R.n[3 * f + 2] >= kLit0_01;
     }
-    for (int b = 0; b < kBB * kBB; b++) members[b].clear();
+    // bucket membership of every face (bit b: a vertex in bucket b), and on small
+    // meshes the members of every bucket in face order
+    thread_local std::vector<int64_t> members_tl[kBB * kBB];
+    std::vector<int64_t>(&members)[kBB * kBB] = members_tl;
+    const bool use_grid = nf >= kGridFaces;
+    if (!use_grid)
+        for (int b = 0; b < kBB * kBB; b++) members[b].clear();
+    thread_local std::vector<uint16_t> memb_tl;
+    std::vector<uint16_t> &memb = memb_tl;
+    memb.resize(nf);
     for (int64_t f = 0; f < nf; f++) {
         unsigned m = 0;
         for (int k = 0; k < 3; k++) m |= 1u << vb[g.vi[g.off[f] + k]];
-        for (; m; m &= m - 1) members[__builtin_ctz(m)].push_back(f);
+        memb[f] = (uint16_t)m;
+        if (!use_grid)
+            for (; m; m &= m - 1) members[__builtin_ctz(m)].push_back(f);
+    }
+    // On large meshes, a finer grid of the faces' outlines: cell c lists, in face order, the faces
+    // whose bounding box (padded by 1e-12 of the extent, far beyond the rounding
+    // of the inside test) meets it.  The blockers of a centroid are the members
+    // of its bucket whose outline contains it, all in the centroid's cell: the
+    // loop below visits the same faces in the same order as a walk over the
+    // bucket's members, less the ones whose inside test would fail.
+    const int G = (int)std::min<int64_t>(128, std::max<int64_t>(4, (int64_t)sqrt((double)nf / 2.0)));
+    const double ex = std::max(mxx - mnx, mxy - mny), pad = 1e-12 * ex;
+    const double gx0 = mnx - pad, gy0 = mny - pad;
+    const double csx = (mxx - mnx + 2 * pad) / G, csy = (mxy - mny + 2 * pad) / G;
+    auto cell_x = [&](double x) {
+        const int c = (int)floor((x - gx0) / csx);
+        return c < 0 ? 0 : (c >= G ? G - 1 : c);
+    };
+    auto cell_y = [&](double y) {
+        const int c = (int)floor((y - gy0) / csy);
+        return c < 0 ? 0 : (c >= G ? G - 1 : c);
+    };
+    thread_local std::vector<int> c_off_tl, c_rng_tl;
+    thread_local std::vector<int64_t> c_item_tl;
+    std::vector<int> &c_off = c_off_tl, &c_rng = c_rng_tl;
+    std::vector<int64_t> &c_item = c_item_tl;
+    c_off.assign(use_grid ? (size_t)G * G + 1 : 1, 0);
+    c_rng.resize(use_grid ? 4 * nf : 0);
+    for (int64_t f = 0; use_grid && f < nf; f++) {
+        const Blocker &B = bl[f];
+        const double x0 = std::min(std::min(B.x[0], B.x[1]), B.x[2]) - pad;
+        const double x1 = std::max(std::max(B.x[0], B.x[1]), B.x[2]) + pad;
+        const double y0 = std::min(std::min(B.y[0], B.y[1]), B.y[2]) - pad;
+        const double y1 = std::max(std::max(B.y[0], B.y[1]), B.y[2]) + pad;
+        int *r = &c_rng[4 * f];
+        r[0] = cell_x(x0);
+        r[1] = cell_x(x1);
+        r[2] = cell_y(y0);
+        r[3] = cell_y(y1);
+        for (int i = r[0]; i <= r[1]; i++)
+            for (int j = r[2]; j <= r[3]; j++) c_off[i * G + j + 1]++;
+    }
+    if (use_grid) {
+        for (int c = 0; c < G * G; c++) c_off[c + 1] += c_off[c];
+        c_item.resize(c_off[G * G]);
+        thread_local std::vector<int> fill_tl;
+        std::vector<int> &fill = fill_tl;
+        fill.assign(c_off.begin(), c_off.end() - 1);
+        for (int64_t f = 0; f < nf; f++) {
+            const int *r = &c_rng[4 * f];
+            for (int i = r[0]; i <= r[1]; i++)
+                for (int j = r[2]; j <= r[3]; j++) c_item[fill[i * G + j]++] = f;
+        }
     }
     out.in_beam.assign(nf, kind == VIS_INC ? 1 : 0);
     out.is_shad.assign(nf, 0);
@@ -520,8 +580,13 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
             continue;
         }
         const double mx = R.mid[3 * m], my = R.mid[3 * m + 1], mz = R.mid[3 * m + 2];
-        for (const int64_t j : members[f3[m]]) {
-            if (j == m) continue;
+        const unsigned bit = 1u << f3[m];
+        const int cm = use_grid ? cell_x(mx) * G + cell_y(my) : 0;
+        const int64_t nq = use_grid ? c_off[cm + 1] - c_off[cm] : (int64_t)members[f3[m]].size();
+        const int64_t *cand = use_grid ? &c_item[c_off[cm]] : members[f3[m]].data();
+        for (int64_t q = 0; q < nq; q++) {
+            const int64_t j = cand[q];
+            if (!(memb[j] & bit) || j == m) continue;  // not in m's bucket
             const Blocker &B = bl[j];
             if (kind == VIS_INC && !B.up) continue;  // down-facing blocker
             const double jz = B.z;
