@@ -66,7 +66,7 @@ constexpr double kLit1_1 = (double)1.1f;    // stretch factors, src/beam_loop_mo
 constexpr double kLit1em5 = (double)1e-5f;  // near-normal refraction, src/beam_loop_mod.f90:1040
 constexpr double kBeamZ = 1000.0;           // incident plane, src/input_mod.f90:2169
 constexpr int kBB = 4;                      // bucket grid 4 x 4, src/beam_loop_mod.f90:2679-2680
-constexpr int64_t kGridFaces = 4096;          // meshes from this size use the cell grid of find_vis
+constexpr int64_t kGridFaces = 256;  // find_vis: candidate sets from this size use the cell grid
 constexpr int64_t kMaxBeams = 20000000;     // guard against a runaway tree
 
 // ------------------------------------------------------------------ complex
@@ -440,112 +440,37 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
     };
     // scratch of the calling thread, reused from beam to beam (bound by
     // reference so that the threads of the loops below share this instance)
-    thread_local std::vector<int> f3_tl, vb_tl;
+    thread_local std::vector<int> vb_tl;
     thread_local std::vector<Blocker> bl_tl;
     thread_local std::vector<char> is_vis_tl;
-    thread_local std::vector<int64_t> map_tl;
-    std::vector<int> &f3 = f3_tl, &vb = vb_tl;
+    thread_local std::vector<int64_t> map_tl, rel_tl;
+    thread_local std::vector<uint16_t> memb_tl;
+    thread_local std::vector<int64_t> members_tl[kBB * kBB];
+    std::vector<int> &vb = vb_tl;
     std::vector<Blocker> &bl = bl_tl;
     std::vector<char> &is_vis = is_vis_tl;
     std::vector<int64_t> &map = map_tl;  // face -> index in the beam's field list
-    f3.resize(nf);
+    std::vector<int64_t> &rel = rel_tl;
+    std::vector<uint16_t> &memb = memb_tl;
+    std::vector<int64_t>(&members)[kBB * kBB] = members_tl;
     vb.resize(g.nv);
     bl.resize(nf);
-    // bucket of every vertex (a face's vertices are tested one by one in the
-    // reference; the answer depends on the coordinates only)
-#pragma omp parallel for schedule(static) if (par && g.nv > 4096)
-    for (int64_t q = 0; q < g.nv; q++) vb[q] = nearest(R.v[3 * q], R.v[3 * q + 1]);
-#pragma omp parallel for schedule(static) if (par && nf > 4096)
-    for (int64_t f = 0; f < nf; f++) {
-        f3[f] = nearest(R.mid[3 * f], R.mid[3 * f + 1]);
-        // the face as a blocker: its corners and edge normals in x, y
-        Blocker &B = bl[f];
-        for (int k = 0; k < 3; k++) {
-            const double *v = &R.v[3 * g.vi[g.off[f] + k]];
-            B.x[k] = v[0];
-            B.y[k] = v[1];
-        }
-        for (int k = 0; k < 3; k++) {
-            const int kn = k == 2 ? 0 : k + 1;
-            B.en2[k] = -B.x[kn] + B.x[k];
-            B.en1[k] = B.y[kn] - B.y[k];
-        }
-        B.z = R.mid[3 * f + 2];
-        B.up = R.n[3 * f + 2] >= kLit0_01;
-    }
-    // bucket membership of every face (bit b: a vertex in bucket b), and on small
-    // meshes the members of every bucket in face order
-    thread_local std::vector<int64_t> members_tl[kBB * kBB];
-    std::vector<int64_t>(&members)[kBB * kBB] = members_tl;
-    const bool use_grid = nf >= kGridFaces;
-    if (!use_grid)
-        for (int b = 0; b < kBB * kBB; b++) members[b].clear();
-    thread_local std::vector<uint16_t> memb_tl;
-    std::vector<uint16_t> &memb = memb_tl;
     memb.resize(nf);
-    for (int64_t f = 0; f < nf; f++) {
-        unsigned m = 0;
-        for (int k = 0; k < 3; k++) m |= 1u << vb[g.vi[g.off[f] + k]];
-        memb[f] = (uint16_t)m;
-        if (!use_grid)
-            for (; m; m &= m - 1) members[__builtin_ctz(m)].push_back(f);
-    }
-    // On large meshes, a finer grid of the faces' outlines: cell c lists, in face order, the faces
-    // whose bounding box (padded by 1e-12 of the extent, far beyond the rounding
-    // of the inside test) meets it.  The blockers of a centroid are the members
-    // of its bucket whose outline contains it, all in the centroid's cell: the
-    // loop below visits the same faces in the same order as a walk over the
-    // bucket's members, less the ones whose inside test would fail.
-    const int G = (int)std::min<int64_t>(128, std::max<int64_t>(4, (int64_t)sqrt((double)nf / 2.0)));
-    const double ex = std::max(mxx - mnx, mxy - mny), pad = 1e-12 * ex;
-    const double gx0 = mnx - pad, gy0 = mny - pad;
-    const double csx = (mxx - mnx + 2 * pad) / G, csy = (mxy - mny + 2 * pad) / G;
-    auto cell_x = [&](double x) {
-        const int c = (int)floor((x - gx0) / csx);
-        return c < 0 ? 0 : (c >= G ? G - 1 : c);
-    };
-    auto cell_y = [&](double y) {
-        const int c = (int)floor((y - gy0) / csy);
-        return c < 0 ? 0 : (c >= G ? G - 1 : c);
-    };
-    thread_local std::vector<int> c_off_tl, c_rng_tl;
-    thread_local std::vector<int64_t> c_item_tl;
-    std::vector<int> &c_off = c_off_tl, &c_rng = c_rng_tl;
-    std::vector<int64_t> &c_item = c_item_tl;
-    c_off.assign(use_grid ? (size_t)G * G + 1 : 1, 0);
-    c_rng.resize(use_grid ? 4 * nf : 0);
-    for (int64_t f = 0; use_grid && f < nf; f++) {
-        const Blocker &B = bl[f];
-        const double x0 = std::min(std::min(B.x[0], B.x[1]), B.x[2]) - pad;
-        const double x1 = std::max(std::max(B.x[0], B.x[1]), B.x[2]) + pad;
-        const double y0 = std::min(std::min(B.y[0], B.y[1]), B.y[2]) - pad;
-        const double y1 = std::max(std::max(B.y[0], B.y[1]), B.y[2]) + pad;
-        int *r = &c_rng[4 * f];
-        r[0] = cell_x(x0);
-        r[1] = cell_x(x1);
-        r[2] = cell_y(y0);
-        r[3] = cell_y(y1);
-        for (int i = r[0]; i <= r[1]; i++)
-            for (int j = r[2]; j <= r[3]; j++) c_off[i * G + j + 1]++;
-    }
-    if (use_grid) {
-        for (int c = 0; c < G * G; c++) c_off[c + 1] += c_off[c];
-        c_item.resize(c_off[G * G]);
-        thread_local std::vector<int> fill_tl;
-        std::vector<int> &fill = fill_tl;
-        fill.assign(c_off.begin(), c_off.end() - 1);
-        for (int64_t f = 0; f < nf; f++) {
-            const int *r = &c_rng[4 * f];
-            for (int i = r[0]; i <= r[1]; i++)
-                for (int j = r[2]; j <= r[3]; j++) c_item[fill[i * G + j]++] = f;
-        }
-    }
     out.in_beam.assign(nf, kind == VIS_INC ? 1 : 0);
     out.is_shad.assign(nf, 0);
     out.id_beam.assign(nf, -1);
     out.dist.assign(nf, 0.0);
     is_vis.assign(nf, 1);
     map.assign(nf, -1);
+    const double ex = std::max(mxx - mnx, mxy - mny), pad = 1e-12 * ex;
+    // The faces that can be lit or block.  For the incident beam, every face.  For
+    // a beam leaving the particle's faces, a lit centroid lies in the beam's extent
+    // in x, y, and a blocker contains it: the faces whose outline (padded by 1e-12
+    // of the particle's extent, far beyond the rounding of the inside test) meets
+    // that extent -- about a tenth of a rough column's faces.  Their buckets,
+    // outlines and bucket lists are formed, in face order; the others' would not
+    // be read.
+    rel.clear();
     if (kind != VIS_INC) {
         for (size_t i = 0; i < beam.in.size(); i++) map[beam.in[i].fi] = (int64_t)i;
         // beam extent in x, y (:2126-2160)
@@ -562,6 +487,124 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
         for (int64_t f = 0; f < nf; f++) {
             const double x = R.mid[3 * f], y = R.mid[3 * f + 1];
             if (x < bxmin || x > bxmax || y < bymin || y > bymax) is_vis[f] = 0;
+        }
+        const double ax0 = bxmin - pad, ax1 = bxmax + pad, ay0 = bymin - pad, ay1 = bymax + pad;
+        for (int64_t f = 0; f < nf; f++) {
+            const int64_t q0 = 3 * g.vi[g.off[f]], q1 = 3 * g.vi[g.off[f] + 1],
+                          q2 = 3 * g.vi[g.off[f] + 2];
+            const double x0 = std::min(std::min(R.v[q0], R.v[q1]), R.v[q2]);
+            const double x1 = std::max(std::max(R.v[q0], R.v[q1]), R.v[q2]);
+            const double y0 = std::min(std::min(R.v[q0 + 1], R.v[q1 + 1]), R.v[q2 + 1]);
+            const double y1 = std::max(std::max(R.v[q0 + 1], R.v[q1 + 1]), R.v[q2 + 1]);
+            if (!(x1 < ax0 || x0 > ax1 || y1 < ay0 || y0 > ay1)) rel.push_back(f);
+        }
+    }
+    const bool all = kind == VIS_INC;
+    const int64_t nrel = all ? nf : (int64_t)rel.size();
+    auto rel_face = [&](int64_t i) { return all ? i : rel[i]; };
+    // bucket of every vertex of those faces (a face's vertices are tested one by
+    // one in the reference; the answer depends on the coordinates only)
+    if (all) {
+#pragma omp parallel for schedule(static) if (par && g.nv > 4096)
+        for (int64_t q = 0; q < g.nv; q++) vb[q] = nearest(R.v[3 * q], R.v[3 * q + 1]);
+    } else {
+        // each shared vertex once: stamp[q] marks the calls that formed vb[q]
+        thread_local std::vector<uint32_t> stamp_tl;
+        thread_local uint32_t call_tl = 0;
+        std::vector<uint32_t> &stamp = stamp_tl;
+        if (stamp.size() != (size_t)g.nv || ++call_tl == 0) {
+            stamp.assign(g.nv, 0);
+            call_tl = 1;
+        }
+        const uint32_t call = call_tl;
+        for (int64_t i = 0; i < nrel; i++)
+            for (int k = 0; k < 3; k++) {
+                const int64_t q = g.vi[g.off[rel[i]] + k];
+                if (stamp[q] != call) {
+                    stamp[q] = call;
+                    vb[q] = nearest(R.v[3 * q], R.v[3 * q + 1]);
+                }
+            }
+    }
+#pragma omp parallel for schedule(static) if (par && nrel > 4096)
+    for (int64_t i = 0; i < nrel; i++) {
+        const int64_t f = rel_face(i);
+        // the face as a blocker: its corners and edge normals in x, y
+        Blocker &B = bl[f];
+        for (int k = 0; k < 3; k++) {
+            const double *v = &R.v[3 * g.vi[g.off[f] + k]];
+            B.x[k] = v[0];
+            B.y[k] = v[1];
+        }
+        for (int k = 0; k < 3; k++) {
+            const int kn = k == 2 ? 0 : k + 1;
+            B.en2[k] = -B.x[kn] + B.x[k];
+            B.en1[k] = B.y[kn] - B.y[k];
+        }
+        B.z = R.mid[3 * f + 2];
+        B.up = R.n[3 * f + 2] >= kLit0_01;
+    }
+    // bucket membership of those faces (bit b: a vertex in bucket b), and on small
+    // meshes the members of every bucket in face order
+    const bool use_grid = nrel >= kGridFaces;
+    if (!use_grid)
+        for (int b = 0; b < kBB * kBB; b++) members[b].clear();
+    for (int64_t i = 0; i < nrel; i++) {
+        const int64_t f = rel_face(i);
+        unsigned m = 0;
+        for (int k = 0; k < 3; k++) m |= 1u << vb[g.vi[g.off[f] + k]];
+        memb[f] = (uint16_t)m;
+        if (!use_grid)
+            for (; m; m &= m - 1) members[__builtin_ctz(m)].push_back(f);
+    }
+    // On large sets, a finer grid of the faces' outlines: cell c lists, in face
+    // order, the faces whose bounding box (padded as above) meets it.  The
+    // blockers of a centroid are the members of its bucket whose outline contains
+    // it, all in the centroid's cell: the loop below visits the same faces in the
+    // same order as a walk over the bucket's members, less the ones whose inside
+    // test would fail.
+    const int G = (int)std::min<int64_t>(128, std::max<int64_t>(4, (int64_t)sqrt((double)nrel / 2.0)));
+    const double gx0 = mnx - pad, gy0 = mny - pad;
+    const double csx = (mxx - mnx + 2 * pad) / G, csy = (mxy - mny + 2 * pad) / G;
+    // (coordinates are at or above the padded origin, so truncation is the floor)
+    auto cell_x = [&](double x) {
+        const int c = (int)((x - gx0) / csx);
+        return c < 0 ? 0 : (c >= G ? G - 1 : c);
+    };
+    auto cell_y = [&](double y) {
+        const int c = (int)((y - gy0) / csy);
+        return c < 0 ? 0 : (c >= G ? G - 1 : c);
+    };
+    thread_local std::vector<int> c_off_tl, c_rng_tl;
+    thread_local std::vector<int64_t> c_item_tl;
+    std::vector<int> &c_off = c_off_tl, &c_rng = c_rng_tl;
+    std::vector<int64_t> &c_item = c_item_tl;
+    if (use_grid) {
+        c_off.assign((size_t)G * G + 1, 0);
+        c_rng.resize(4 * nrel);
+        for (int64_t i = 0; i < nrel; i++) {
+            const Blocker &B = bl[rel_face(i)];
+            const double x0 = std::min(std::min(B.x[0], B.x[1]), B.x[2]) - pad;
+            const double x1 = std::max(std::max(B.x[0], B.x[1]), B.x[2]) + pad;
+            const double y0 = std::min(std::min(B.y[0], B.y[1]), B.y[2]) - pad;
+            const double y1 = std::max(std::max(B.y[0], B.y[1]), B.y[2]) + pad;
+            int *r = &c_rng[4 * i];
+            r[0] = cell_x(x0);
+            r[1] = cell_x(x1);
+            r[2] = cell_y(y0);
+            r[3] = cell_y(y1);
+            for (int a = r[0]; a <= r[1]; a++)
+                for (int b = r[2]; b <= r[3]; b++) c_off[a * G + b + 1]++;
+        }
+        for (int c = 0; c < G * G; c++) c_off[c + 1] += c_off[c];
+        c_item.resize(c_off[G * G]);
+        thread_local std::vector<int> fill_tl;
+        std::vector<int> &fill = fill_tl;
+        fill.assign(c_off.begin(), c_off.end() - 1);
+        for (int64_t i = 0; i < nrel; i++) {
+            const int *r = &c_rng[4 * i];
+            for (int a = r[0]; a <= r[1]; a++)
+                for (int b = r[2]; b <= r[3]; b++) c_item[fill[a * G + b]++] = rel_face(i);
         }
     }
     for (int64_t f = 0; f < nf; f++) {
@@ -580,10 +623,11 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
             continue;
         }
         const double mx = R.mid[3 * m], my = R.mid[3 * m + 1], mz = R.mid[3 * m + 2];
-        const unsigned bit = 1u << f3[m];
+        const int fb = nearest(mx, my);  // the centroid's bucket
+        const unsigned bit = 1u << fb;
         const int cm = use_grid ? cell_x(mx) * G + cell_y(my) : 0;
-        const int64_t nq = use_grid ? c_off[cm + 1] - c_off[cm] : (int64_t)members[f3[m]].size();
-        const int64_t *cand = use_grid ? &c_item[c_off[cm]] : members[f3[m]].data();
+        const int64_t nq = use_grid ? c_off[cm + 1] - c_off[cm] : (int64_t)members[fb].size();
+        const int64_t *cand = use_grid ? &c_item[c_off[cm]] : members[fb].data();
         for (int64_t q = 0; q < nq; q++) {
             const int64_t j = cand[q];
             if (!(memb[j] & bit) || j == m) continue;  // not in m's bucket
