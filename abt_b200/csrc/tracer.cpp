@@ -42,6 +42,7 @@
 #include <math.h>
 #include <omp.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -67,6 +68,17 @@ constexpr double kLit1em5 = (double)1e-5f;  // near-normal refraction, src/beam_
 constexpr double kBeamZ = 1000.0;           // incident plane, src/input_mod.f90:2169
 constexpr int kBB = 4;                      // bucket grid 4 x 4, src/beam_loop_mod.f90:2679-2680
 constexpr int64_t kGridFaces = 256;  // find_vis: candidate sets from this size use the cell grid
+
+// The cell-grid threshold; PBT_TRACER_GRID_MIN overrides it (a test compares the
+// lists of both walks).
+int64_t grid_min_faces() {
+    static const int64_t v = [] {
+        const char *e = getenv("PBT_TRACER_GRID_MIN");
+        const long long x = e ? atoll(e) : -1;
+        return x >= 0 ? (int64_t)x : kGridFaces;
+    }();
+    return v;
+}
 constexpr int64_t kMaxBeams = 20000000;     // guard against a runaway tree
 
 // ------------------------------------------------------------------ complex
@@ -546,7 +558,7 @@ void find_vis(const Shape &g, const Rotated &R, const Beam &beam, VisKind kind, 
     }
     // bucket membership of those faces (bit b: a vertex in bucket b), and on small
     // meshes the members of every bucket in face order
-    const bool use_grid = nrel >= kGridFaces;
+    const bool use_grid = nrel >= grid_min_faces();
     if (!use_grid)
         for (int b = 0; b < kBB * kBB; b++) members[b].clear();
     for (int64_t i = 0; i < nrel; i++) {

@@ -455,3 +455,42 @@ def test_c_caller(tmp_path):
                                   LAM, RBI)
     assert tag == "ok" and int(nbeam) == len(beam) and int(next_) == len(ext)
     assert float(ratio) == pytest.approx(en["beam_energy_out"] / en["geo_cross_sec"], rel=1e-9)
+
+
+_DIGEST = (
+    "import hashlib, sys\n"
+    "import numpy as np\n"
+    "sys.path.insert(0, %r)\n"
+    "from abt_b200 import tracer as T, workloads as W\n"
+    "h = hashlib.sha256()\n"
+    "for geo, ibi in ((W.hex_prism(10.0, 20.0, n_side=6, n_len=12, roughness=0.1, seed=3), 0.0),\n"
+    "                 (W.hex_prism(30.0, 60.0, n_side=14, n_len=30, roughness=0.0, seed=5), 0.01)):\n"
+    "    P = T.Particle(geo, geo['apertures'])\n"
+    "    eul = W.uniform_euler(np.random.default_rng(41), 3)\n"
+    "    Vs, beams, exts, pins, en = T.trace_batch(P, eul, 0.532, 1.31, ibi=ibi)\n"
+    "    for a in list(Vs) + list(beams) + list(exts) + [pins]:\n"
+    "        h.update(np.ascontiguousarray(a).tobytes())\n"
+    "print(h.hexdigest())\n")
+
+
+def test_visibility_walks_give_the_same_lists():
+    """The visibility test walks the candidate blockers of a centroid either over
+    its bucket's member list or, from 256 candidate faces, over the faces whose
+    outline box meets the centroid's cell of a finer grid (in face order, filtered
+    by bucket membership): the same faces in the same order, less those whose
+    inside test fails.  Traced with only the member walk and with the grid from
+    the first face on, a rough column and a 7,392-triangle column give the same
+    lists bit for bit."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = _DIGEST % root
+    out = []
+    for grid_min in ("1000000000", "0"):
+        env = dict(os.environ, PBT_TRACER_GRID_MIN=grid_min, OMP_NUM_THREADS="4")
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr
+        out.append(r.stdout.strip())
+    assert out[0] == out[1] and len(out[0]) == 64
