@@ -824,9 +824,14 @@ __device__ __forceinline__ float2 sinc_series(float2 h) {
 // rsqrt(hn2 tt^2) the normalisation of the polarisation block.  With the half
 // phases sorted (lo <= mid <= hi) the edge midpoints of the full phases are
 // lo + mid and mid + hi and the half gaps mid - lo and hi - mid, each one
-// operation.
-__device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float2 hn2, float2 tt,
-                                          float2 &gx, float2 &gy) {
+// operation.  Formed in two halves: tri_front from the three half phases alone,
+// tri_back with the polarisation block's |h|^2 and tt (for the shared reciprocal
+// square root below).
+struct TriF {
+    float2 lo, mid, hi, Dh, h1, h2, s1, k1, s2, k2, p12, S1, S2;
+};
+__device__ __forceinline__ TriF tri_front(float2 t1, float2 t2, float2 t3) {
+    TriF F;
     float2 lo, hi, mid;
     lo.x = fminf(t1.x, t2.x);
     hi.x = fmaxf(t1.x, t2.x);
@@ -855,11 +860,20 @@ __device__ __forceinline__ void tri_dd_pk(float2 t1, float2 t2, float2 t3, float
     const float2 a1 = make_float2(fmaxf(h1.x, 0.5f), fmaxf(h1.y, 0.5f));
     const float2 a2 = make_float2(fmaxf(h2.x, 0.5f), fmaxf(h2.y, 0.5f));
     const float2 p12 = mul2(a1, a2);
+    F.lo = lo; F.mid = mid; F.hi = hi; F.Dh = Dh; F.h1 = h1; F.h2 = h2;
+    F.s1 = s1; F.k1 = k1; F.s2 = s2; F.k2 = k2; F.p12 = p12;
+    F.S1 = mul2(make_float2(sin_fz(h1.x), sin_fz(h1.y)), a2);
+    F.S2 = mul2(make_float2(sin_fz(h2.x), sin_fz(h2.y)), a1);
+    return F;
+}
+
+__device__ __forceinline__ void tri_back(const TriF &F, float2 hn2, float2 tt, float2 &gx, float2 &gy) {
+    const float2 lo = F.lo, mid = F.mid, hi = F.hi, Dh = F.Dh, h1 = F.h1, h2 = F.h2;
+    const float2 s1 = F.s1, k1 = F.k1, s2 = F.s2, k2 = F.k2, p12 = F.p12;
     const float2 q = mul2(mul2(p12, Dh), tt);
     const float2 hq = mul2(hn2, mul2(q, q));
     const float2 scr = make_float2(rsqrt_fz(hq.x), rsqrt_fz(hq.y));
-    float2 S1 = mul2(make_float2(sin_fz(h1.x), sin_fz(h1.y)), a2);
-    float2 S2 = mul2(make_float2(sin_fz(h2.x), sin_fz(h2.y)), a1);
+    float2 S1 = F.S1, S2 = F.S2;
     // below h = 0.5 sinc(h) from its series, evaluated only when a lane of the
     // warp needs it (small gaps occur near a facet's specular and forward
     // directions), one vote for both
@@ -982,6 +996,20 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
         kxx = fma2(nkh, kx, kp0);
         kyy = fma2(nkh, ky, kp1);
     }
+    // the divided difference's phases, sort, sines and cosines: independent of
+    // the polarisation block and its rare branch, so formed ahead of the branch
+    // (one basic block with the direction arithmetic for the scheduler)
+    TriF tf;
+    {
+        float2 vx0, vx1, vx2, vy0, vy1, vy2;
+        ld22(&P.vx[0], vx0, vx1);
+        ld22(&P.vx[2], vx2, vy0);
+        ld22(&P.vy[1], vy1, vy2);
+        const float2 t1 = fma2(kyy, vy0, fma2(kxx, vx0, ph));
+        const float2 t2 = fma2(kyy, vy1, fma2(kxx, vx1, ph));
+        const float2 t3 = fma2(kyy, vy2, fma2(kxx, vx2, ph));
+        tf = tri_front(t1, t2, t3);
+    }
     // Polarisation matrix [[d, e], [-e, d]] (see k2_record for the forms) and
     // the rotation into the scattering plane, with their normalisations folded
     // into one factor: with s = sqrt(tt) and hc = h / |h|,
@@ -1096,19 +1124,10 @@ __device__ __forceinline__ void k2_pair(const K2Pair &P, const K2Fov *fv, const 
     const float2 hn2 = fma2(hz, hz, fma2(hy, hy, mul2(hx, hx)));
     const float2 A = fma2(P1, d1, mul2(R1, e1));
     const float2 Bc = fma2(P1, e1, neg2(mul2(R1, d1)));
-    // aperture integral on the half phases (after the polarisation block, so
-    // that only A and B stay live across it): 2 sc g
+    // aperture integral on the half phases, its second half (the normalisation
+    // sc needs the polarisation block's |h| and tt): 2 sc g
     float2 gx, gy;
-    {
-        float2 vx0, vx1, vx2, vy0, vy1, vy2;
-        ld22(&P.vx[0], vx0, vx1);
-        ld22(&P.vx[2], vx2, vy0);
-        ld22(&P.vy[1], vy1, vy2);
-        const float2 t1 = fma2(kyy, vy0, fma2(kxx, vx0, ph));
-        const float2 t2 = fma2(kyy, vy1, fma2(kxx, vx1, ph));
-        const float2 t3 = fma2(kyy, vy2, fma2(kxx, vx2, ph));
-        tri_dd_pk(t1, t2, t3, hn2, tt, gx, gy);
-    }
+    tri_back(tf, hn2, tt, gx, gy);
     // [[A, B], [-B, A]] is diagonal in the circular basis: with z = A - iB the
     // columns' u+ take z, their u- take conj(z).  q+ = g z, q- = g conj(z).
     const float2 gyB = mul2(gy, Bc), gxB = mul2(gx, Bc);
