@@ -88,6 +88,38 @@ def test_batch_fp32_vs_fp64(ctx, scaling):
     np.testing.assert_allclose(f[3]["back_scatt"], r[3]["back_scatt"], rtol=1e-4)
 
 
+@pytest.mark.parametrize("fast", [False, True])
+def test_batch_fp32_uneven_grid(ctx, fast):
+    """The batched FP32 average against the FP64 path on a theta grid of three
+    spacings (fine near the forward direction, src/input_mod.f90:114-196) and a
+    phi range short of 360 degrees (the reference's phi integral then covers
+    [0, phi_max] only), with and without the -fast_diff field-of-view cull."""
+    rng = np.random.default_rng(21)
+    th = abt_b200.make_angles([0, 2, 20, 180], [0.25, 1, 4])
+    ph = abt_b200.make_angles([0, 270], [3])
+    geo = W.hex_prism(3.0, 6.0, n_side=2, n_len=3, roughness=0.05, seed=4)
+    beams, exts, Vs, pins = [], [], [], []
+    for k in range(4):
+        R = W.euler_rotation(*rng.uniform(0, 2 * np.pi, size=3))
+        V, beam, ext, gcs = W.standin_orientation(geo, R, rng, n_internal=(0, 2))
+        beams.append(beam)
+        exts.append(ext)
+        Vs.append(V)
+        pins.append(abt_b200.params(abs=0.0, geo_cross_sec=gcs, beam_energy_out=0.9 * gcs,
+                                    ext_energy_out=gcs))
+    pins = np.array(pins)
+    r = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pins, is_fast_diff=fast, precision="fp64")
+    f = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pins, is_fast_diff=fast, precision="fp32")
+    assert mueller_rel_err(f[0], r[0]) <= TOL_MU
+    assert rel_err(f[1], r[1]) <= TOL_MU
+    for n in ("scatt", "ext", "asymmetry", "scatt_beam", "scatt_ext_diff", "albedo"):
+        assert abs(f[2][n] - r[2][n]) <= TOL_PARAM * abs(r[2][n]), n
+    if fast:
+        # the cull changes the result (it is not the full sum)
+        full = ctx.diff_batch(beams, exts, Vs, geo, th, ph, LAM, pins, precision="fp64")
+        assert rel_err(full[0], r[0]) > 1e-6
+
+
 @pytest.mark.gpu
 def test_fp32_fast_diff_tile_cull(ctx):
     """is_fast_diff on beam lists with small fields of view: the FP32 kernel
