@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(HERE, "libpbt_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "pbt_diff.h")
 
 PBT_OK, PBT_EINVAL, PBT_ENOMEM, PBT_ECUDA, PBT_ETIMEOUT, PBT_ENODEV, PBT_ESTATE = range(7)
+PBT_DEVICE_LOCAL_RANK = -1  # pbt_ctx_create: the node-local rank modulo the visible devices
 PBT_PREC_FP64, PBT_PREC_FP32 = 0, 1
 STATUS_NAMES = {0: "PBT_OK", 1: "PBT_EINVAL", 2: "PBT_ENOMEM", 3: "PBT_ECUDA",
                 4: "PBT_ETIMEOUT", 5: "PBT_ENODEV", 6: "PBT_ESTATE"}
@@ -31,7 +32,7 @@ PARAMS_DTYPE = np.dtype([(n, "<f8") for n in PARAM_NAMES])
 assert PARAMS_DTYPE.itemsize == 144
 
 # every function declared in include/pbt_diff.h
-EXPORTS = ("pbt_ctx_create", "pbt_ctx_destroy", "pbt_last_error_string", "pbt_version",
+EXPORTS = ("pbt_ctx_create", "pbt_ctx_device", "pbt_ctx_destroy", "pbt_last_error_string", "pbt_version",
            "pbt_diff_main_c", "pbt_diffraction_c", "pbt_finalise_c", "pbt_summation_c",
            "pbt_divide_by_num_orientations_c", "pbt_totals_reset_c", "pbt_diff_batch_c",
            "pbt_diff_batch_dev_c", "pbt_last_launch_count", "pbt_set_kernel_timing",
@@ -76,6 +77,7 @@ def lib():
     sig = {
         "pbt_ctx_create": (C, [C, ctypes.POINTER(P)]),
         "pbt_ctx_destroy": (C, [P]),
+        "pbt_ctx_device": (C, [P, ctypes.POINTER(C)]),
         "pbt_last_error_string": (ctypes.c_char_p, []),
         "pbt_version": (C, []),
         "pbt_diff_main_c": (C, [P, P, I64, P, I64, P, I64, P, P, I64, P, I64, P, I64, D, I32, I32,

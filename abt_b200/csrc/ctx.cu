@@ -1,6 +1,7 @@
 // ctx.cu -- context lifecycle, error reporting and buffer management.
 #include <stdarg.h>
 #include <stdio.h>
+#include <stdlib.h>
 
 #include <atomic>
 
@@ -160,6 +161,22 @@ extern "C" int pbt_version(void) { return 10000; }
 
 extern "C" const char *pbt_last_error_string(void) { return last_error(); }
 
+// The node-local rank that an MPI or torchrun launcher exports (the first of
+// these variables set to a non-negative integer), or 0.
+static int local_rank_from_env() {
+    static const char *const vars[] = {"LOCAL_RANK",      "OMPI_COMM_WORLD_LOCAL_RANK",
+                                       "MV2_COMM_WORLD_LOCAL_RANK", "MPI_LOCALRANKID",
+                                       "SLURM_LOCALID",   "PMI_LOCAL_RANK"};
+    for (const char *v : vars) {
+        const char *s = getenv(v);
+        if (!s || !*s) continue;
+        char *end = nullptr;
+        const long r = strtol(s, &end, 10);
+        if (*end == '\0' && r >= 0 && r <= 1000000) return (int)r;
+    }
+    return 0;
+}
+
 extern "C" int pbt_ctx_create(int device, pbt_ctx **out) {
     clear_error();
     if (!out) {
@@ -174,6 +191,7 @@ extern "C" int pbt_ctx_create(int device, pbt_ctx **out) {
         set_error("no CUDA device: %s", e != cudaSuccess ? cudaGetErrorString(e) : "count is 0");
         return PBT_ENODEV;
     }
+    if (device == PBT_DEVICE_LOCAL_RANK) device = local_rank_from_env() % ndev;
     if (device < 0 || device >= ndev) {
         set_error("device %d out of range (have %d)", device, ndev);
         return PBT_EINVAL;
@@ -197,6 +215,16 @@ extern "C" int pbt_ctx_create(int device, pbt_ctx **out) {
         return PBT_ECUDA;
     }
     *out = c;
+    return PBT_OK;
+}
+
+extern "C" int pbt_ctx_device(const pbt_ctx *ctx, int *device) {
+    clear_error();
+    if (!ctx || !device) {
+        set_error("ctx and device must not be NULL");
+        return PBT_EINVAL;
+    }
+    *device = ctx->device;
     return PBT_OK;
 }
 

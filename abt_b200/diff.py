@@ -94,14 +94,18 @@ def _ob(a):
 
 
 class Context:
-    """A library context on one CUDA device (pbt_ctx_create / pbt_ctx_destroy)."""
+    """A library context on one CUDA device (pbt_ctx_create / pbt_ctx_destroy).
+    device=-1 (PBT_DEVICE_LOCAL_RANK) takes the launcher's node-local rank
+    modulo the visible devices; `device` holds the device the context is on."""
 
     def __init__(self, device=0):
         L = _lib.lib()
         h = ctypes.c_void_p()
         check(L.pbt_ctx_create(int(device), ctypes.byref(h)))
         self._h = h
-        self.device = device
+        d = ctypes.c_int(-1)
+        check(L.pbt_ctx_device(h, ctypes.byref(d)))
+        self.device = d.value
 
     @property
     def handle(self):

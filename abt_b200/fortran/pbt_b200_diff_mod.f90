@@ -39,6 +39,10 @@ module pbt_b200_diff_mod
 
     type(c_ptr), save :: pbt_ctx = c_null_ptr
     integer(c_int), save :: pbt_precision = PBT_PREC_FP64
+    ! device of the context: -1 (PBT_DEVICE_LOCAL_RANK) takes the node-local rank of
+    ! an MPI launcher modulo the visible devices, so that the reference's MPI build
+    ! spreads its ranks over a node's GPUs; set it before the first call to pin one
+    integer(c_int), save :: pbt_device = -1_c_int
 
     interface
         integer(c_int) function pbt_ctx_create(device, ctx) bind(C, name="pbt_ctx_create")
@@ -142,7 +146,7 @@ module pbt_b200_diff_mod
     end subroutine
 
     subroutine pbt_init()
-        if (.not. c_associated(pbt_ctx)) call pbt_check(pbt_ctx_create(0_c_int, pbt_ctx), 'pbt_ctx_create')
+        if (.not. c_associated(pbt_ctx)) call pbt_check(pbt_ctx_create(pbt_device, pbt_ctx), 'pbt_ctx_create')
     end subroutine
 
     ! facet vertex CSR of the geometry (geometry%f(:)%vi), 0-based offsets

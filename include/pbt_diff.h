@@ -66,8 +66,17 @@ typedef struct pbt_ctx pbt_ctx;
 
 /* Create a context bound to CUDA device `device`.  The context owns device
  * buffers reused across calls; it is safe to share between host threads
- * (calls are serialised on an internal mutex). */
+ * (calls are serialised on an internal mutex).  PBT_DEVICE_LOCAL_RANK picks the
+ * device from the process's node-local rank, as an MPI launcher (the
+ * reference's MPI build, src/pbt_mpi_mod.f90) or torchrun exports it
+ * (LOCAL_RANK, OMPI_COMM_WORLD_LOCAL_RANK, MV2_COMM_WORLD_LOCAL_RANK,
+ * MPI_LOCALRANKID, SLURM_LOCALID or PMI_LOCAL_RANK, the first one set; 0 when
+ * none is) modulo the number of visible devices, so that the ranks of one node
+ * spread over its GPUs. */
+#define PBT_DEVICE_LOCAL_RANK (-1)
 int pbt_ctx_create(int device, pbt_ctx **out);
+/* The CUDA device the context is bound to. */
+int pbt_ctx_device(const pbt_ctx *ctx, int *device);
 int pbt_ctx_destroy(pbt_ctx *ctx);
 /* Message of the last failed call made by this thread ("" if none). */
 const char *pbt_last_error_string(void);

@@ -45,9 +45,10 @@ def test_no_device_reports_enodev():
         has_gpu = False
     if has_gpu:
         pytest.skip("a GPU is present")
-    with pytest.raises(_lib.PbtError) as e:
-        abt_b200.Context(0)
-    assert e.value.status == _lib.PBT_ENODEV
+    for dev in (0, _lib.PBT_DEVICE_LOCAL_RANK):
+        with pytest.raises(_lib.PbtError) as e:
+            abt_b200.Context(dev)
+        assert e.value.status == _lib.PBT_ENODEV
     # a NULL context is rejected with a status, not a crash
     assert _lib.lib().pbt_diff_main_c(None, None, 0, None, 0, None, 0, None, None, 0, None, 0,
                                       None, 0, 0.5, 0, 0, None, None) == _lib.PBT_EINVAL

@@ -185,3 +185,30 @@ def test_injected_allocation_failure_reports_enomem(precision):
         assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
         mu = c.finalise(got[0], got[1], th, ph, LAM, abt_b200.params(geo_cross_sec=1.0))[0]
         assert np.isfinite(mu).all()
+
+
+def test_device_from_local_rank(monkeypatch):
+    """PBT_DEVICE_LOCAL_RANK takes the launcher's node-local rank modulo the
+    visible devices (the reference's MPI ranks spread over a node's GPUs); an
+    unset or malformed rank gives device 0, and an explicit device is kept."""
+    import torch
+    from abt_b200._lib import PBT_DEVICE_LOCAL_RANK
+    ndev = torch.cuda.device_count()
+    names = ("LOCAL_RANK", "OMPI_COMM_WORLD_LOCAL_RANK", "MV2_COMM_WORLD_LOCAL_RANK",
+             "MPI_LOCALRANKID", "SLURM_LOCALID", "PMI_LOCAL_RANK")
+    for n in names:
+        monkeypatch.delenv(n, raising=False)
+    for env, want in (({}, 0), ({"OMPI_COMM_WORLD_LOCAL_RANK": "5"}, 5 % ndev),
+                      ({"LOCAL_RANK": "x7", "SLURM_LOCALID": "3"}, 3 % ndev),
+                      ({"PMI_LOCAL_RANK": "-2"}, 0)):
+        for n in names:
+            monkeypatch.delenv(n, raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        with abt_b200.Context(PBT_DEVICE_LOCAL_RANK) as c:
+            assert c.device == want, env
+    with abt_b200.Context(0) as c:
+        assert c.device == 0
+    with pytest.raises(PbtError) as e:
+        abt_b200.Context(ndev)
+    assert e.value.status == PBT_EINVAL
