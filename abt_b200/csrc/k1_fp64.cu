@@ -11,6 +11,7 @@
 // host (host_setup.cpp); the bin grid and cos/sin(phi) are libm values.
 #include <float.h>
 #include <math.h>
+#include <string.h>
 
 #include <algorithm>
 #include <mutex>
@@ -355,6 +356,18 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
 
 static std::mutex g_na_mu;
 static double g_na_host[3 * kNaMaxBins + 2 * kNaMaxPhi];  // host staging of the bin grid
+// The grid in g_na_host was built from these theta / phi values (g_na_nt < 0: none
+// yet); g_na_gen counts the grids built.  A device's scratch holds that grid when
+// the 64-bit tag at kNaOffTag (in the facet slot's unused tail) reads
+// kNaTagBase ^ g_na_gen, so a call with the same theta and phi as the last one
+// builds and uploads nothing; a reset device, or one whose scratch last held
+// another grid, gets the grid again.
+static double g_na_theta[kNaMaxBins], g_na_phi[kNaMaxPhi];
+static int64_t g_na_nt = -1, g_na_np = -1;
+static uint64_t g_na_gen = 0;
+constexpr uint64_t kNaTagBase = 0x6e61677269645f31ull;
+constexpr size_t kNaOffTag = kNaOffFacet + 504;
+static_assert(sizeof(K1Facet) <= 504, "the grid tag follows the facet record in its slot");
 
 int na_fail(int status, const char *msg) {
     set_error("%s", msg);
@@ -411,19 +424,30 @@ extern "C" int pbt_diffraction_noalloc_c(const pbt_outbeam *outbeam, const doubl
     }
     unsigned char *base = static_cast<unsigned char *>(sym);
 
-    // bin grid (make_far_field_bins, phi fastest) and cos/sin(phi), libm values
+    // bin grid (make_far_field_bins, phi fastest) and cos/sin(phi), libm values;
+    // kept from the last call when theta and phi are the same, bit for bit
     const int64_t nb = ntheta * nphi;
     double *hx = g_na_host, *hp = g_na_host + 3 * nb;
-    for (int64_t j = 0; j < ntheta; j++)
+    const bool same_grid = ntheta == g_na_nt && nphi == g_na_np &&
+                           memcmp(theta, g_na_theta, (size_t)ntheta * sizeof(double)) == 0 &&
+                           memcmp(phi, g_na_phi, (size_t)nphi * sizeof(double)) == 0;
+    if (!same_grid) {
+        for (int64_t j = 0; j < ntheta; j++)
+            for (int64_t i = 0; i < nphi; i++) {
+                const int64_t o = i + nphi * j;
+                hx[o] = kFarR * sin(theta[j]) * cos(phi[i]);
+                hx[nb + o] = kFarR * sin(theta[j]) * sin(phi[i]);
+                hx[2 * nb + o] = -(kFarR * cos(theta[j]));
+            }
         for (int64_t i = 0; i < nphi; i++) {
-            const int64_t o = i + nphi * j;
-            hx[o] = kFarR * sin(theta[j]) * cos(phi[i]);
-            hx[nb + o] = kFarR * sin(theta[j]) * sin(phi[i]);
-            hx[2 * nb + o] = -(kFarR * cos(theta[j]));
+            hp[i] = cos(phi[i]);
+            hp[nphi + i] = sin(phi[i]);
         }
-    for (int64_t i = 0; i < nphi; i++) {
-        hp[i] = cos(phi[i]);
-        hp[nphi + i] = sin(phi[i]);
+        memcpy(g_na_theta, theta, (size_t)ntheta * sizeof(double));
+        memcpy(g_na_phi, phi, (size_t)nphi * sizeof(double));
+        g_na_nt = ntheta;
+        g_na_np = nphi;
+        g_na_gen++;
     }
 
     // the facet record and its edges (src/diff_mod.f90:515-574, :334-393), on the stack
@@ -483,8 +507,17 @@ extern "C" int pbt_diffraction_noalloc_c(const pbt_outbeam *outbeam, const doubl
     K1Facet *d_fac = reinterpret_cast<K1Facet *>(base + kNaOffFacet);
     K1Edge *d_edges = reinterpret_cast<K1Edge *>(base + kNaOffEdges);
     double *d_out = reinterpret_cast<double *>(base + kNaOffOut);
-    PBT_CUDA_TRY(cudaMemcpyAsync(d_xyz, hx, 3 * nb * sizeof(double), cudaMemcpyHostToDevice, st));
-    PBT_CUDA_TRY(cudaMemcpyAsync(d_phi, hp, 2 * nphi * sizeof(double), cudaMemcpyHostToDevice, st));
+    uint64_t *d_tag = reinterpret_cast<uint64_t *>(base + kNaOffTag);
+    const uint64_t tag = kNaTagBase ^ g_na_gen;
+    uint64_t have = 0;
+    PBT_CUDA_TRY(cudaMemcpyAsync(&have, d_tag, sizeof(have), cudaMemcpyDeviceToHost, st));
+    PBT_CUDA_TRY(cudaStreamSynchronize(st));
+    if (have != tag) {
+        // the grid, then its tag (stream order: the tag lands after the grid)
+        PBT_CUDA_TRY(cudaMemcpyAsync(d_xyz, hx, 3 * nb * sizeof(double), cudaMemcpyHostToDevice, st));
+        PBT_CUDA_TRY(cudaMemcpyAsync(d_phi, hp, 2 * nphi * sizeof(double), cudaMemcpyHostToDevice, st));
+        PBT_CUDA_TRY(cudaMemcpyAsync(d_tag, &tag, sizeof(tag), cudaMemcpyHostToDevice, st));
+    }
     PBT_CUDA_TRY(cudaMemcpyAsync(d_fac, &F, sizeof(K1Facet), cudaMemcpyHostToDevice, st));
     PBT_CUDA_TRY(cudaMemcpyAsync(d_edges, E, nv * sizeof(K1Edge), cudaMemcpyHostToDevice, st));
     const int threads = 128;

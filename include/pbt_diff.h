@@ -131,7 +131,10 @@ int pbt_make_far_field_bins_c(const double *theta, int64_t ntheta, const double 
  * the array's address on the current device and runs on the calling thread's
  * per-thread default stream (cudaStreamPerThread), waiting for its work.  All
  * calls on a device share the array; calls in one process are serialised and
- * complete before returning, and calls that overlapped on the GPU would race. */
+ * complete before returning, and calls that overlapped on the GPU would race.
+ * The bin grid stays in the array: a call whose theta and phi are the same,
+ * bit for bit, as the previous call's builds and uploads no grid (a tag stored
+ * beside the grid, read back each call, tells whether this device holds it). */
 #define PBT_NOALLOC_MAX_BINS 65536
 #define PBT_NOALLOC_MAX_PHI 4096
 #define PBT_NOALLOC_MAX_VERTS 64

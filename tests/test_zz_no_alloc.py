@@ -54,6 +54,28 @@ def test_no_alloc_matches_the_allocating_entry_point():
             assert rel_err(out, ref) <= 1e-10
 
 
+def test_no_alloc_reuses_the_grid_only_when_it_is_the_same():
+    """Calls alternate between two grids (A, B, A) and repeat a grid with other
+    facets: the grid kept in the fixed array from the previous call is reused
+    only when theta and phi are unchanged, and every result still equals the
+    allocating entry point's."""
+    rng = np.random.default_rng(79)
+    geo = mixed_polygon_geometry(rng)
+    nf = len(geo["face_off"]) - 1
+    A = (abt_b200.make_angles([0, 180], [3]), abt_b200.make_angles([0, 354], [6]))
+    B = (abt_b200.make_angles([0, 180], [2]), abt_b200.make_angles([0, 354], [6]))
+    C = (A[0], abt_b200.make_angles([1, 355], [6]))  # A's shape, other phi values
+    assert len(C[1]) == len(A[1])
+    with abt_b200.Context(0) as ctx:
+        for (th, ph), fi in ((A, 1), (B, 2), (A, 3), (A, 4), (C, 4), (A, 2), (B, 1)):
+            ob = outbeams(1, rng, nf)
+            ob["fi"] = fi
+            ref = ctx.diffraction(ob, geo, th, ph, LAM)
+            st, out = noalloc(ob, geo, th, ph, False)
+            assert st == _lib.PBT_OK, _lib.lib().pbt_last_error_string()
+            assert rel_err(out, ref) <= 1e-10
+
+
 def test_no_alloc_rejects_grids_beyond_its_scratch():
     rng = np.random.default_rng(78)
     geo = mixed_polygon_geometry(rng)
