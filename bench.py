@@ -90,6 +90,9 @@ def parse():
     ap.add_argument("--fd-coords", type=int, default=200,
                     help="vertex coordinates checked by FP64 central differences on each of the "
                          "first two orientations of the differentiation workload (0: skip)")
+    ap.add_argument("--diffraction-calls", type=int, default=200,
+                    help="per-call time of pbt_diffraction_c / pbt_diffraction_noalloc_c "
+                         "(one outbeam, 181 x 180 bins; 0 = skip)")
     ap.add_argument("--adjoint-facets", type=int, default=20000,
                     help="facet sample for the adjoint / forward kernel-time ratio (0: skip)")
     return ap.parse_args()
@@ -710,6 +713,52 @@ def workload_config(nf, nb):
                   "region; CPU arm: each step streams the facet list through the whole grid"}
 
 
+def diffraction_call(ncalls):
+    """The reference's -memory path calls diffraction once per outbeam
+    (src/beam_loop_mod.f90:1935-1967) and adds each call's grid into its totals:
+    the wall time of one call of pbt_diffraction_c and of pbt_diffraction_noalloc_c
+    (FP64, one outbeam of the plain-method column, r 5 um, L 10 um, at Euler
+    30, 40, 10 degrees, on its grid 181 x 180; host arrays in and out, the output
+    arrays reused), over ncalls calls each."""
+    import ctypes
+    from abt_b200 import _lib
+    from abt_b200 import workloads as W
+    from abt_b200.diff import _geo
+    L = _lib.lib()
+    th, ph = W.grid_small()
+    geo = W.hex_prism(5.0, 10.0, n_side=6, n_len=12)
+    V, bl, _, _ = W.standin_orientation(geo, W.euler_rotation(*np.radians([30, 40, 10])),
+                                        np.random.default_rng(1), n_internal=(0, 1))
+    ob = np.ascontiguousarray(bl[:1])
+    v, fo, fv = _geo(dict(geo, verts=V))
+    out = np.zeros((len(ph), len(th), 2, 2), dtype=np.complex128, order="F")
+    h = ctypes.c_void_p()
+    _lib.check(L.pbt_ctx_create(0, ctypes.byref(h)))
+    try:
+        calls = {
+            "pbt_diffraction_c": lambda: L.pbt_diffraction_c(
+                h, ob.ctypes.data, v.ctypes.data, v.shape[0], fo.ctypes.data, fv.ctypes.data,
+                len(fo) - 1, th.ctypes.data, len(th), ph.ctypes.data, len(ph), LAM, 0, out.ctypes.data),
+            "pbt_diffraction_noalloc_c": lambda: L.pbt_diffraction_noalloc_c(
+                ob.ctypes.data, v.ctypes.data, v.shape[0], fo.ctypes.data, fv.ctypes.data,
+                len(fo) - 1, th.ctypes.data, len(th), ph.ctypes.data, len(ph), LAM, 0, out.ctypes.data),
+        }
+        res = {"grid": "181 theta x 180 phi (%d bins)" % (len(th) * len(ph)), "calls": ncalls,
+               "particle": "hexagonal column r 5 um, L 10 um (%d triangles), one outbeam"
+                           % (len(fo) - 1),
+               "api": "host arrays in and out; the amplitude grid (%d bytes) copied back each call"
+                      % out.nbytes}
+        for name, f in calls.items():
+            _lib.check(f())
+            t = time.perf_counter()
+            for _ in range(ncalls):
+                _lib.check(f())
+            res[name + "_ms"] = (time.perf_counter() - t) / ncalls * 1e3
+        return res
+    finally:
+        L.pbt_ctx_destroy(h)
+
+
 def fast_diff_kept_fraction(beam, geo, th, ph, sample=20000, tile_theta=8, tile_phi=16):
     """Fraction of (record, bin tile) pairs that the -fast_diff tile cull keeps,
     estimated on the host on the first `sample` records with the kernel's test:
@@ -995,6 +1044,9 @@ def main():
                               "cull": "records whose field of view misses a 8x16 (theta x phi) "
                                       "bin tile are skipped for that tile"}
 
+    if args.diffraction_calls > 0 and solo:
+        extra["diffraction_call"] = diffraction_call(args.diffraction_calls)
+
     # FP32 error against the FP64 drop-in on the full workload
     if not args.no_error_check and solo:
         from tests.helpers import mueller_rel_err
@@ -1062,6 +1114,10 @@ def main():
         cpu = cpu_baseline(geo, beam, th, ph, args.cpu_seconds, os.cpu_count() or 1)
         # the single-thread path (the reference's seq build at -mt 0)
         cpu["single_thread"] = cpu_baseline(geo, beam, th, ph, args.cpu_seconds / 2, 1)
+        if "diffraction_call" in extra:
+            # the same call's work on one host core at the single-thread baseline's rate
+            extra["diffraction_call"]["cpu_1thread_ms_from_cpu_baseline"] = \
+                181 * 180 / cpu["single_thread"]["value"] * 1e3
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
