@@ -34,7 +34,7 @@ HOST_UNITS = {"host_setup.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math", "
                                  "-I" + os.path.join(CUDA_HOME, "include")],
               "beamlist.cpp": ["-O2", "-fPIC", "-std=c++17", "-I" + CSRC, "-I" + INCLUDE,
                                "-I" + os.path.join(CUDA_HOME, "include")],
-              "tracer.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
+              "tracer.cpp": ["-O3", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
                              "-std=c++17", "-I" + CSRC, "-I" + INCLUDE,
                              "-I" + os.path.join(CUDA_HOME, "include")]}
 
@@ -45,8 +45,16 @@ def _headers():
     return hs
 
 
-def _stale(obj, src):
+def _stale(obj, src, cmd):
+    """An object is rebuilt when it is missing, older than its source or a header,
+    or was compiled with another command line (kept beside it in <obj>.cmd)."""
     if not os.path.exists(obj):
+        return True
+    try:
+        with open(obj + ".cmd") as f:
+            if f.read() != " ".join(cmd):
+                return True
+    except OSError:
         return True
     t = os.path.getmtime(obj)
     return any(os.path.getmtime(d) > t for d in [src] + _headers())
@@ -55,12 +63,12 @@ def _stale(obj, src):
 def _compile(unit, flags, host, verbose):
     src = os.path.join(CSRC, unit)
     obj = os.path.join(BUILD, unit + ".o")
-    if not _stale(obj, src):
-        return obj
     if host:
         cmd = ["g++", "-c", src, "-o", obj] + flags
     else:
         cmd = [NVCC, "-c", src, "-o", obj] + NVCC_COMMON + flags
+    if not _stale(obj, src, cmd):
+        return obj
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -68,6 +76,8 @@ def _compile(unit, flags, host, verbose):
         raise RuntimeError("compile of %s failed:\n%s\n%s" % (unit, r.stdout, r.stderr))
     if verbose and r.stderr.strip():
         print(r.stderr, flush=True)
+    with open(obj + ".cmd", "w") as f:
+        f.write(" ".join(cmd))
     return obj
 
 
