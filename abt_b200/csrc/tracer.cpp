@@ -983,12 +983,19 @@ void spawn(const Shape &g, const Params &P, const Beam &beam, bool parent_int,
     for (int64_t a = 0; a < g.na; a++)
         create[a] = parent_int ? (ap_area[a] > P.thresh_area && ap_energy[a] > P.thresh_energy)
                                : (ap_area[a] > P.thresh_area);
-    std::vector<int64_t> slot(g.na, -1);
+    std::vector<int64_t> slot(g.na, -1), nface(g.na, 0);
+    for (const FieldOut &o : fo)
+        if (create[o.ap]) nface[o.ap]++;
     for (int64_t a = 0; a < g.na; a++) {
         if (!create[a]) continue;
         slot[a] = (int64_t)tree.size();
+        // each child's field list gets its final length at once (one allocation)
         tree.push_back(new_beam(beam, true));
-        if (!parent_int || !tir[a]) tree.push_back(new_beam(beam, false));
+        tree.back().in.reserve(nface[a]);
+        if (!parent_int || !tir[a]) {
+            tree.push_back(new_beam(beam, false));
+            tree.back().in.reserve(nface[a]);
+        }
     }
     for (const FieldOut &o : fo) {
         if (!create[o.ap]) continue;
